@@ -1,0 +1,1414 @@
+// afc_api.cu -- host side of apollofft_b200: integer layer, GPU planner, plan
+// cache and the C ABI declared in include/apollofft_cuda.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/apollofft_cuda.h"
+#include "afc_internal.h"
+
+namespace afc {
+
+// ───────────────────────────── errors / counters ─────────────────────────────
+
+static thread_local std::string g_last_error;
+static std::atomic<uint64_t> g_launches{0};
+void count_launch(int k) { g_launches.fetch_add((uint64_t)k, std::memory_order_relaxed); }
+
+static afc_status fail(afc_status s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return s;
+}
+static afc_status cuda_fail(cudaError_t e, const char* what) {
+  if (e == cudaErrorMemoryAllocation) return fail(AFC_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+  return fail(AFC_ERR_DEVICE, "%s: %s", what, cudaGetErrorString(e));
+}
+#define AFC_CUDA(call, what)                    \
+  do {                                          \
+    cudaError_t e_ = (call);                    \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+// Test hook: fail the next N device allocations with AFC_ERR_OUT_OF_MEMORY.
+static std::atomic<int> g_fail_allocs{0};
+static cudaError_t dev_alloc(void** p, size_t bytes) {
+  if (g_fail_allocs.load() > 0) {
+    g_fail_allocs.fetch_sub(1);
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  if (bytes == 0) bytes = 16;
+  return cudaMalloc(p, bytes);
+}
+
+// ───────────────────────────── integer layer ─────────────────────────────
+// The library's own statement of the reference's integer maps; results are
+// bit-exact with crates/apollo-fft (tests compare against the oracle and the
+// reference's known-answer tests).
+
+using u64 = uint64_t;
+
+static u64 mulmod(u64 a, u64 b, u64 m) { return (u64)((unsigned __int128)a * b % m); }
+static u64 powmod(u64 b, u64 e, u64 m) {
+  u64 r = 1 % m;
+  b %= m;
+  while (e) {
+    if (e & 1) r = mulmod(r, b, m);
+    b = mulmod(b, b, m);
+    e >>= 1;
+  }
+  return r;
+}
+static std::vector<u64> prime_factors(u64 n) {  // ascending, with multiplicity
+  std::vector<u64> f;
+  while (n > 0 && n % 2 == 0) { f.push_back(2); n /= 2; }
+  for (u64 d = 3; d * d <= n; d += 2)
+    while (n % d == 0) { f.push_back(d); n /= d; }
+  if (n > 1) f.push_back(n);
+  return f;
+}
+static bool is_prime_u(u64 n) {  // radix_shape.rs:172-190
+  if (n <= 1) return false;
+  if (n <= 3) return true;
+  if (n % 2 == 0 || n % 3 == 0) return false;
+  for (u64 i = 5; i * i <= n; i += 6)
+    if (n % i == 0 || n % (i + 2) == 0) return false;
+  return true;
+}
+// radix_shape.rs:60-170: odd primes of {3..23} innermost (largest first), 2s outermost;
+// None for other primes or pure powers of two.
+static bool factorize23(u64 n, std::vector<u64>& out) {
+  out.clear();
+  if (n <= 1) return true;
+  const u64 pr[8] = {23, 17, 13, 11, 7, 5, 3, 2};
+  u64 cnt[8] = {0}, m = n;
+  for (int i = 7; i >= 0; --i)
+    while (m % pr[i] == 0) { m /= pr[i]; cnt[i]++; }
+  if (m != 1) return false;
+  bool odd = false;
+  for (int i = 0; i < 7; ++i) odd |= cnt[i] > 0;
+  if (!odd) return false;
+  for (int i = 0; i < 8; ++i)
+    for (u64 k = 0; k < cnt[i]; ++k) out.push_back(pr[i]);
+  return true;
+}
+static std::vector<u64> lower_pairs(const std::vector<u64>& r) {  // radix_shape.rs:221-234
+  std::vector<u64> o;
+  for (size_t i = 0; i < r.size();) {
+    if (i + 1 < r.size() && r[i] == 2 && r[i + 1] == 2) { o.push_back(4); i += 2; }
+    else o.push_back(r[i++]);
+  }
+  return o;
+}
+// radix_shape.rs:192-219: n1 = power of the largest prime factor, n2 = rest.
+static bool coprime_split(u64 n, u64& n1, u64& n2) {
+  auto f = prime_factors(n);
+  if (f.empty()) return false;
+  std::vector<u64> pp;
+  for (size_t i = 0; i < f.size();) {
+    u64 p = f[i], pw = 1;
+    while (i < f.size() && f[i] == p) { pw *= p; ++i; }
+    pp.push_back(pw);
+  }
+  if (pp.size() < 2) return false;
+  n1 = pp.back();
+  n2 = n / n1;
+  return true;
+}
+static bool short_winograd(u64 n) {  // mixed_radix/traits.rs:172-176
+  if (n >= 2 && n <= 56) return true;
+  return n == 58 || n == 60 || n == 62 || n == 63 || n == 64 || n == 81 || n == 128;
+}
+// good_thomas/mod.rs:29-31 with three_by_prime.rs:1-11 and the fixed.rs:31-45
+// generator rule (apollo-fft-macros/src/good_thomas.rs:244-325).
+static bool static_coprime_codelet(u64 n1, u64 n2) {
+  static const u64 tbp[] = {5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
+  if (n2 == 3)
+    for (u64 p : tbp) if (p == n1) return true;
+  static const u64 ss[] = {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17,
+                           18, 19, 23, 24, 25, 27, 29, 31, 32, 36, 37, 41, 43, 47, 53};
+  auto in_ss = [&](u64 v) { for (u64 s : ss) if (s == v) return true; return false; };
+  const u64 n = n1 * n2;
+  if (!in_ss(n1) || !in_ss(n2) || n1 < 2 || n2 < 2 || n > 200 || in_ss(n)) return false;
+  u64 a = n1, b = n2;
+  while (b) { u64 t = a % b; a = b; b = t; }
+  if (a != 1) return false;
+  u64 c1, c2;
+  if (!coprime_split(n, c1, c2) || c1 != n1 || c2 != n2) return false;
+  const u64 lo = std::min(n1, n2), hi = std::max(n1, n2);
+  static const u64 dpp[] = {5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
+  if (lo == 2 || lo == 3)
+    for (u64 p : dpp)
+      if (p == hi) return false;
+  return true;
+}
+// rader/generator.rs:18-94: fixed table, then the smallest generator.
+static u64 primitive_root_u(u64 p) {
+  static const std::pair<u64, u64> tab[] = {
+      {2, 1},   {3, 2},   {5, 2},   {7, 3},    {11, 2},  {13, 2},  {17, 3},  {19, 2},
+      {23, 5},  {29, 2},  {31, 3},  {37, 2},   {41, 6},  {43, 3},  {47, 5},  {53, 2},
+      {59, 2},  {61, 2},  {67, 2},  {71, 7},   {73, 5},  {79, 3},  {83, 2},  {89, 3},
+      {97, 5},  {101, 2}, {109, 6}, {113, 3},  {127, 3}, {131, 2}, {151, 6}, {167, 5},
+      {173, 2}, {179, 2}, {181, 2}, {193, 5},  {197, 2}, {199, 3}, {10007, 5}};
+  for (auto& e : tab) if (e.first == p) return e.second;
+  if (p == 2) return 1;
+  auto f = prime_factors(p - 1);
+  f.erase(std::unique(f.begin(), f.end()), f.end());
+  for (u64 g = 2; g < p; ++g) {
+    bool ok = true;
+    for (u64 q : f) if (powmod(g, (p - 1) / q, p) == 1) { ok = false; break; }
+    if (ok) return g;
+  }
+  return 0;
+}
+static u64 inv_mod(u64 a, u64 m) {  // rader/generator.rs:96-120 (a in [1, m))
+  if (m == 1) return 0;
+  int64_t r0 = (int64_t)m, r1 = (int64_t)(a % m), s0 = 0, s1 = 1;
+  while (r1 != 0) {
+    int64_t q = r0 / r1, t = r0 - q * r1;
+    r0 = r1; r1 = t;
+    t = s0 - q * s1; s0 = s1; s1 = t;
+  }
+  if (s0 < 0) s0 += (int64_t)m;
+  return (u64)s0;
+}
+static int strategy_of(u64 n) {  // mixed_radix/dispatch.rs:26-132
+  if (n <= 1) return 0;
+  if ((n & (n - 1)) == 0 && n >= 64) return (n >= 4096 && (__builtin_ctzll(n) % 2 == 0)) ? 2 : 1;
+  if (short_winograd(n)) return 3;
+  u64 n1 = 0, n2 = 0;
+  bool cop = coprime_split(n, n1, n2);
+  if (cop && static_coprime_codelet(n1, n2)) return 4;
+  std::vector<u64> r;
+  if (factorize23(n, r)) return 5;
+  if (cop) return 6;
+  if (is_prime_u(n)) return (n - 1 >= 1024) ? 8 : 7;
+  return 9;
+}
+
+// ───────────────────────────── GPU planning ─────────────────────────────
+
+enum Algo { ALGO_SMEM = 0, ALGO_FOURSTEP = 1, ALGO_RADER = 2, ALGO_BLUESTEIN = 3, ALGO_NOOP = 4 };
+static const size_t kSmemMax = 220 * 1024;
+static const int64_t kRaderMax = 1024;  // Rader below, Bluestein above (primes)
+
+// Radices the engine executes for n: odd primes <= 13 (innermost, largest
+// first, as the reference orders its factors) then the power of two as 16s and
+// one 8/4/2.  False when n has another prime factor (Rader / Bluestein).
+static bool gpu_radices(int64_t n, std::vector<int>& rad) {
+  rad.clear();
+  if (n <= 1) return false;
+  int64_t m = n;
+  static const int odd[] = {13, 11, 7, 5, 3};
+  for (int p : odd)
+    while (m % p == 0) { rad.push_back(p); m /= p; }
+  int k = 0;
+  while (m % 2 == 0) { m /= 2; ++k; }
+  if (m != 1) return false;
+  while (k >= 4) { rad.push_back(16); k -= 4; }
+  if (k == 3) rad.push_back(8);
+  else if (k == 2) rad.push_back(4);
+  else if (k == 1) rad.push_back(2);
+  return (int)rad.size() <= kMaxStages;
+}
+
+struct LenPlan {
+  StageList sl{};
+  void* tw = nullptr;
+  int P = 0, ld = 0;
+  int64_t n = 0;
+};
+
+static int ld_for(int64_t n) {
+  int64_t ld = n + (n - 1) / 16 + 1;
+  if ((ld & 1) == 0) ld += 1;
+  return (int)ld;
+}
+
+// Threads per lane: one butterfly of the largest radix per thread and stage
+// (smaller radices loop), at most 512 threads.
+static int choose_threads(int64_t n, const std::vector<int>& rad) {
+  int rmax = 2;
+  for (int r : rad) rmax = std::max(rmax, r);
+  int64_t p = (n + rmax - 1) / rmax;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(512, p));
+}
+
+// A single-CTA plan needs two shared buffers of ld elements for one lane.
+static bool plannable(int64_t n, size_t csz, std::vector<int>* rad_out = nullptr) {
+  std::vector<int> rad;
+  if (!gpu_radices(n, rad)) return false;
+  if (2 * (size_t)ld_for(n) * csz + 64 > kSmemMax) return false;
+  if (rad_out) *rad_out = rad;
+  return true;
+}
+
+static afc_status build_lenplan(int64_t n, bool dbl, LenPlan& lp, cudaStream_t st) {
+  const size_t csz = dbl ? 16 : 8;
+  std::vector<int> rad;
+  if (!plannable(n, csz, &rad)) return fail(AFC_ERR_UNSUPPORTED, "length %lld has no shared-memory plan", (long long)n);
+  lp.n = n;
+  lp.P = choose_threads(n, rad);
+  lp.ld = ld_for(n);
+  lp.sl.n = (int)n;
+  lp.sl.nst = (int)rad.size();
+  int Ns = 1, off = 0;
+  for (size_t s = 0; s < rad.size(); ++s) {
+    lp.sl.st[s].R = rad[s];
+    lp.sl.st[s].Ns = Ns;
+    lp.sl.st[s].twoff = off;
+    if (Ns > 1) off += Ns * (rad[s] - 1);
+    Ns *= rad[s];
+  }
+  AFC_CUDA(dev_alloc(&lp.tw, (size_t)std::max(off, 1) * csz), "twiddle table");
+  if (off > 0) AFC_CUDA(gen_stage_twiddles_dev(lp.tw, lp.sl, dbl, st), "twiddle generation");
+  return AFC_OK;
+}
+
+struct AxisPlan {
+  int64_t n = 0;
+  int algo = ALGO_NOOP;
+  LenPlan lp;                        // SMEM: n; RADER / BLUESTEIN in smem: M
+  LenPlan lp1, lp2;                  // FOURSTEP: N1 and N2
+  int64_t N1 = 0, N2 = 0, twB = 1;
+  void* tw_hi = nullptr;
+  void* tw_lo = nullptr;
+  int64_t M = 0;                     // convolution length
+  bool conv_smem = true;
+  void* chirp = nullptr;
+  void* spec_f = nullptr;
+  void* spec_i = nullptr;
+  int* gather = nullptr;
+  int* scatter = nullptr;
+  std::unique_ptr<AxisPlan> sub;     // four-step plan of length M (large Bluestein)
+  ~AxisPlan() {
+    void* ptrs[] = {lp.tw, lp1.tw, lp2.tw, tw_hi, tw_lo, chirp, spec_f, spec_i, gather, scatter};
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+  }
+};
+
+static afc_status build_axis(int64_t n, bool dbl, AxisPlan& ap, cudaStream_t st);
+
+static afc_status build_fourstep(int64_t n, bool dbl, AxisPlan& ap, cudaStream_t st) {
+  const size_t csz = dbl ? 16 : 8;
+  // N1 = divisor nearest sqrt(n) with both factors plannable.
+  int64_t best = 0;
+  double target = std::sqrt((double)n);
+  for (int64_t d = 2; d * d <= n * 4 && d < n; ++d) {
+    if (n % d) continue;
+    if (!plannable(d, csz) || !plannable(n / d, csz)) continue;
+    if (best == 0 || std::fabs(std::log((double)d / target)) < std::fabs(std::log((double)best / target))) best = d;
+  }
+  if (best == 0) return fail(AFC_ERR_UNSUPPORTED, "length %lld has no two-pass split", (long long)n);
+  ap.algo = ALGO_FOURSTEP;
+  ap.N1 = best;
+  ap.N2 = n / best;
+  afc_status s = build_lenplan(ap.N1, dbl, ap.lp1, st);
+  if (s != AFC_OK) return s;
+  s = build_lenplan(ap.N2, dbl, ap.lp2, st);
+  if (s != AFC_OK) return s;
+  int64_t B = (int64_t)std::ceil(std::sqrt((double)n));
+  ap.twB = B;
+  int64_t nhi = (n + B - 1) / B;
+  AFC_CUDA(dev_alloc(&ap.tw_lo, (size_t)B * csz), "four-step twiddles");
+  AFC_CUDA(dev_alloc(&ap.tw_hi, (size_t)nhi * csz), "four-step twiddles");
+  AFC_CUDA(gen_roots_dev(ap.tw_lo, B, 1, n, dbl, st), "four-step twiddles");
+  AFC_CUDA(gen_roots_dev(ap.tw_hi, nhi, B, n, dbl, st), "four-step twiddles");
+  return AFC_OK;
+}
+
+struct AxisIO {
+  const void* in = nullptr;
+  void* out = nullptr;
+  long long lanes = 0;
+  LaneMap im{}, om{};
+  int in_op = IN_C, out_op = OUT_C;
+  double scale = 1.0;
+  long long nlen = 0;    // OUT_TRUNC bins kept
+  long long herm_n = 0;  // full length for IN_HERM / OUT_TRUNC pairing
+  double pair_w = 1.0;
+};
+
+// Lanes per CTA: about 256 threads, at least 8 (f64) / 16 (f32) adjacent lanes
+// when a side is staged (full 128-byte rows), shared memory per CTA kept
+// moderate so several CTAs share an SM.
+static int choose_L(const LenPlan& lp, long long lanes, bool stage_in, bool stage_out, size_t csz,
+                    size_t extra_per_lane = 0, int nbuf_override = 0) {
+  const int nbuf = nbuf_override ? nbuf_override : engine_buffers(lp.sl.nst, stage_in, stage_out);
+  const size_t per_lane = (size_t)nbuf * lp.ld * csz + extra_per_lane + 3 * sizeof(long long);
+  int L = std::max(1, 256 / lp.P);
+  const bool staged = stage_in || stage_out;
+  const int Lmin = staged ? (csz == 16 ? 8 : 16) : 1;
+  L = std::max(L, Lmin);
+  while (L > 1 && ((size_t)L * lp.P > 512 || (size_t)L * per_lane > kSmemMax)) --L;
+  while (L > Lmin && (size_t)L * per_lane > 100 * 1024) --L;
+  if ((long long)L > lanes) L = (int)std::max(1LL, lanes);
+  return L;
+}
+
+// The engine reads/writes global memory directly only for plain complex or
+// real data along contiguous lanes; everything else is staged.
+static bool plain_in(int op) { return op == IN_C || op == IN_R; }
+static bool plain_out(int op) { return op == OUT_C || op == OUT_RE; }
+
+static void fill_common(LaunchDesc& d, const LenPlan& lp) {
+  d.sl = lp.sl;
+  d.tw = lp.tw;
+  d.P = lp.P;
+  d.ld = lp.ld;
+}
+
+static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisIO& io, void* ws, cudaStream_t st);
+
+// Four-step execution of one axis: pass A (N1-point columns, twiddle) into the
+// workspace, pass B (N2-point rows) into the output with the transposed store.
+static cudaError_t exec_fourstep(const AxisPlan& ap, bool dbl, bool inv, const AxisIO& io, void* ws,
+                                 cudaStream_t st, int in_op_B = IN_C) {
+  const size_t csz = dbl ? 16 : 8;
+  const long long n = ap.n, N1 = ap.N1, N2 = ap.N2;
+  const long long d2 = io.im.d2;
+  LaunchDesc a;
+  fill_common(a, ap.lp1);
+  a.lanes = io.lanes * N2;
+  a.im = io.im.off ? LaneMap{1, N2, 0, 0, io.im.es, N2 * io.im.es, io.im.off}
+                   : LaneMap{N2, d2, io.im.s0, io.im.es, io.im.s2, N2 * io.im.es, nullptr};
+  a.om = LaneMap{N2, d2, d2 * n, 1, n, N2, nullptr};
+  a.in = io.in;
+  a.out = ws;
+  a.in_op = io.in_op;
+  a.out_op = OUT_TW;
+  a.jmul = N2;
+  a.col_div = d2;
+  a.col_mod = N2;
+  a.twN = n;
+  a.twB = ap.twB;
+  a.tw_hi = ap.tw_hi;
+  a.tw_lo = ap.tw_lo;
+  a.tw_conj = inv ? 1 : 0;
+  a.stage_in = a.im.es != 1 || !plain_in(a.in_op);
+  a.stage_out = true;
+  a.L = choose_L(ap.lp1, a.lanes, a.stage_in, a.stage_out, csz);
+  cudaError_t e = launch_lanes(a, dbl, inv, st);
+  if (e != cudaSuccess) return e;
+  LaunchDesc b;
+  fill_common(b, ap.lp2);
+  b.lanes = io.lanes * N1;
+  b.im = LaneMap{N1, d2, d2 * n, N2, n, 1, nullptr};
+  b.om = io.om.off ? LaneMap{1, N1, 0, 0, io.om.es, N1 * io.om.es, io.om.off}
+                   : LaneMap{N1, io.om.d2, io.om.s0, io.om.es, io.om.s2, N1 * io.om.es, nullptr};
+  b.in = ws;
+  b.out = io.out;
+  b.in_op = in_op_B;
+  b.out_op = io.out_op;
+  b.scale = io.scale;
+  b.jmul = N1;
+  b.col_div = d2;
+  b.col_mod = N1;
+  b.nlen = io.nlen;
+  b.herm_n = io.herm_n;
+  b.pair_w = io.pair_w;
+  b.stage_in = false;
+  b.stage_out = b.om.es != 1 || !plain_out(b.out_op);
+  if (ap.lp2.sl.nst <= 1) b.stage_out = true;
+  b.L = choose_L(ap.lp2, b.lanes, b.stage_in, b.stage_out, csz);
+  return launch_lanes(b, dbl, inv, st);
+}
+
+static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisIO& io, void* ws, cudaStream_t st) {
+  const size_t csz = dbl ? 16 : 8;
+  if (io.lanes <= 0) return cudaSuccess;
+  switch (ap.algo) {
+    case ALGO_SMEM: {
+      LaunchDesc d;
+      fill_common(d, ap.lp);
+      d.lanes = io.lanes;
+      d.im = io.im;
+      d.om = io.om;
+      d.in = io.in;
+      d.out = io.out;
+      d.in_op = io.in_op;
+      d.out_op = io.out_op;
+      d.scale = io.scale;
+      d.nlen = io.nlen;
+      d.herm_n = io.herm_n;
+      d.pair_w = io.pair_w;
+      d.stage_in = io.im.es != 1 || !plain_in(io.in_op);
+      d.stage_out = io.om.es != 1 || !plain_out(io.out_op) || ap.lp.sl.nst <= 1;
+      d.L = choose_L(ap.lp, io.lanes, d.stage_in, d.stage_out, csz);
+      return launch_lanes(d, dbl, inv, st);
+    }
+    case ALGO_FOURSTEP:
+      return exec_fourstep(ap, dbl, inv, io, ws, st);
+    case ALGO_RADER:
+    case ALGO_BLUESTEIN: {
+      const bool rader = ap.algo == ALGO_RADER;
+      const bool real_in = io.in_op == IN_R;
+      const bool real_out = io.out_op == OUT_RE;
+      if (ap.conv_smem) {
+        LaunchDesc d;
+        fill_common(d, ap.lp);
+        d.lanes = io.lanes;
+        d.im = io.im;
+        d.om = io.om;
+        d.in = io.in;
+        d.out = io.out;
+        d.scale = io.scale;
+        if (rader) {
+          d.in_op = real_in ? IN_GATHER_R : IN_GATHER;
+          d.out_op = real_out ? OUT_SCATTER_RE : OUT_SCATTER;
+          d.nlen = ap.n;
+        } else {
+          d.in_op = real_in ? IN_CHIRP_R : IN_CHIRP;
+          d.out_op = real_out ? OUT_CHIRP_RE : OUT_CHIRP;
+          d.nlen = io.out_op == OUT_TRUNC ? io.nlen : ap.n;
+        }
+        d.spec = inv ? ap.spec_i : ap.spec_f;
+        d.chirp = ap.chirp;
+        d.chirp_conj = inv ? 1 : 0;
+        d.gather = ap.gather;
+        d.scatter = ap.scatter;
+        d.L = choose_L(ap.lp, io.lanes, true, true, csz, 2 * csz, 2);
+        return launch_conv(d, dbl, st);
+      }
+      // Bluestein with a four-step convolution: 4 passes over two workspaces.
+      const AxisPlan& mp = *ap.sub;
+      const long long M = ap.M, N1 = mp.N1, N2 = mp.N2, d2 = io.im.d2;
+      char* w1 = static_cast<char*>(ws);
+      char* w2 = w1 + (size_t)io.lanes * M * csz;
+      LaunchDesc a;
+      fill_common(a, mp.lp1);
+      a.lanes = io.lanes * N2;
+      a.im = io.im.off ? LaneMap{1, N2, 0, 0, io.im.es, N2 * io.im.es, io.im.off}
+                       : LaneMap{N2, d2, io.im.s0, io.im.es, io.im.s2, N2 * io.im.es, nullptr};
+      a.om = LaneMap{N2, d2, d2 * M, 1, M, N2, nullptr};
+      a.in = io.in;
+      a.out = w1;
+      a.in_op = real_in ? IN_CHIRP_R : IN_CHIRP;
+      a.out_op = OUT_TW;
+      a.jmul = N2;
+      a.col_div = d2;
+      a.col_mod = N2;
+      a.nlen = ap.n;
+      a.chirp = ap.chirp;
+      a.chirp_conj = inv ? 1 : 0;
+      a.twN = M;
+      a.twB = mp.twB;
+      a.tw_hi = mp.tw_hi;
+      a.tw_lo = mp.tw_lo;
+      a.stage_in = true;
+      a.stage_out = true;
+      a.L = choose_L(mp.lp1, a.lanes, a.stage_in, a.stage_out, csz);
+      cudaError_t e = launch_lanes(a, dbl, false, st);
+      if (e != cudaSuccess) return e;
+      LaunchDesc b;
+      fill_common(b, mp.lp2);
+      b.lanes = io.lanes * N1;
+      b.im = LaneMap{N1, d2, d2 * M, N2, M, 1, nullptr};
+      b.om = LaneMap{N1, d2, d2 * M, 1, M, N1, nullptr};
+      b.in = w1;
+      b.out = w2;
+      b.out_op = OUT_MUL;
+      b.spec = inv ? ap.spec_i : ap.spec_f;
+      b.jmul = N1;
+      b.col_div = d2;
+      b.col_mod = N1;
+      b.stage_out = true;
+      b.L = choose_L(mp.lp2, b.lanes, b.stage_in, b.stage_out, csz);
+      e = launch_lanes(b, dbl, false, st);
+      if (e != cudaSuccess) return e;
+      LaunchDesc c = a;
+      c.tw_conj = 1;
+      c.im = LaneMap{N2, d2, d2 * M, 1, M, N2, nullptr};
+      c.in = w2;
+      c.in_op = IN_C;
+      c.out = w1;
+      c.stage_in = true;
+      c.L = choose_L(mp.lp1, c.lanes, c.stage_in, c.stage_out, csz);
+      e = launch_lanes(c, dbl, true, st);
+      if (e != cudaSuccess) return e;
+      LaunchDesc f;
+      fill_common(f, mp.lp2);
+      f.lanes = io.lanes * N1;
+      f.im = LaneMap{N1, d2, d2 * M, N2, M, 1, nullptr};
+      f.om = io.om.off ? LaneMap{1, N1, 0, 0, io.om.es, N1 * io.om.es, io.om.off}
+                       : LaneMap{N1, io.om.d2, io.om.s0, io.om.es, io.om.s2, N1 * io.om.es, nullptr};
+      f.in = w1;
+      f.out = io.out;
+      f.out_op = real_out ? OUT_CHIRP_RE : OUT_CHIRP;
+      f.scale = io.scale;
+      f.jmul = N1;
+      f.col_div = d2;
+      f.col_mod = N1;
+      f.nlen = io.out_op == OUT_TRUNC ? io.nlen : ap.n;
+      f.chirp = ap.chirp;
+      f.chirp_conj = inv ? 1 : 0;
+      f.stage_out = true;
+      f.L = choose_L(mp.lp2, f.lanes, f.stage_in, f.stage_out, csz);
+      return launch_lanes(f, dbl, true, st);
+    }
+    default:
+      return cudaSuccess;
+  }
+}
+
+static size_t axis_ws_bytes(const AxisPlan& ap, long long lanes, size_t csz) {
+  if (ap.algo == ALGO_FOURSTEP) return (size_t)lanes * ap.n * csz;
+  if (ap.algo == ALGO_BLUESTEIN && !ap.conv_smem) return 2 * (size_t)lanes * ap.M * csz;
+  return 0;
+}
+
+// FFT of a single length-M table (plan build) through an axis plan.
+static afc_status fft_table(const AxisPlan& mp, bool dbl, void* buf, cudaStream_t st) {
+  const size_t csz = dbl ? 16 : 8;
+  AxisIO io;
+  io.in = buf;
+  io.out = buf;
+  io.lanes = 1;
+  io.im = LaneMap{1, 1, mp.n, 0, 0, 1, nullptr};
+  io.om = io.im;
+  void* ws = nullptr;
+  size_t wsb = axis_ws_bytes(mp, 1, csz);
+  if (wsb) AFC_CUDA(dev_alloc(&ws, wsb), "table workspace");
+  cudaError_t e = exec_axis(mp, dbl, false, io, ws, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (ws) cudaFree(ws);
+  if (e != cudaSuccess) return cuda_fail(e, "table FFT");
+  return AFC_OK;
+}
+
+static afc_status build_axis(int64_t n, bool dbl, AxisPlan& ap, cudaStream_t st) {
+  const size_t csz = dbl ? 16 : 8;
+  ap.n = n;
+  if (n <= 1) { ap.algo = ALGO_NOOP; return AFC_OK; }
+  std::vector<int> rad;
+  if (gpu_radices(n, rad)) {
+    if (plannable(n, csz)) { ap.algo = ALGO_SMEM; return build_lenplan(n, dbl, ap.lp, st); }
+    return build_fourstep(n, dbl, ap, st);
+  }
+  if (is_prime_u((u64)n) && n < kRaderMax) {
+    // Rader: generator order of the reference (rader/mod.rs:76-122), cyclic
+    // convolution of length p-1, exact or zero-padded to a power of two.
+    const int64_t L = n - 1;
+    int64_t M = L;
+    if (!plannable(L, csz)) {
+      M = 1;
+      while (M < 2 * L - 1) M <<= 1;
+    }
+    if (!plannable(M, csz))
+      return fail(AFC_ERR_UNSUPPORTED, "no Rader plan for %lld", (long long)n);
+    ap.algo = ALGO_RADER;
+    ap.M = M;
+    afc_status s = build_lenplan(M, dbl, ap.lp, st);
+    if (s != AFC_OK) return s;
+    const u64 g = primitive_root_u((u64)n);
+    std::vector<int> gat(L), sca(L);
+    u64 v = 1;
+    for (int64_t q = 0; q < L; ++q) { gat[q] = (int)v; v = mulmod(v, g, (u64)n); }
+    for (int64_t q = 0; q < L; ++q) sca[q] = q == 0 ? gat[0] : gat[L - q];
+    AFC_CUDA(dev_alloc((void**)&ap.gather, L * sizeof(int)), "Rader maps");
+    AFC_CUDA(dev_alloc((void**)&ap.scatter, L * sizeof(int)), "Rader maps");
+    AFC_CUDA(cudaMemcpyAsync(ap.gather, gat.data(), L * sizeof(int), cudaMemcpyHostToDevice, st), "Rader maps");
+    AFC_CUDA(cudaMemcpyAsync(ap.scatter, sca.data(), L * sizeof(int), cudaMemcpyHostToDevice, st), "Rader maps");
+    AFC_CUDA(dev_alloc(&ap.spec_f, (size_t)M * csz), "Rader spectrum");
+    AFC_CUDA(dev_alloc(&ap.spec_i, (size_t)M * csz), "Rader spectrum");
+    AFC_CUDA(gen_rader_b_dev(ap.spec_f, ap.scatter, n, M, false, dbl, st), "Rader kernel");
+    AFC_CUDA(gen_rader_b_dev(ap.spec_i, ap.scatter, n, M, true, dbl, st), "Rader kernel");
+    AxisPlan mp;
+    mp.n = M;
+    mp.algo = ALGO_SMEM;
+    mp.lp = ap.lp;
+    s = fft_table(mp, dbl, ap.spec_f, st);
+    if (s == AFC_OK) s = fft_table(mp, dbl, ap.spec_i, st);
+    mp.lp.tw = nullptr;  // owned by ap
+    return s;
+  }
+  // Bluestein chirp-z with a power-of-two convolution of length M >= 2n-1.
+  int64_t M = 1;
+  while (M < 2 * n - 1) M <<= 1;
+  ap.algo = ALGO_BLUESTEIN;
+  ap.M = M;
+  AFC_CUDA(dev_alloc(&ap.chirp, (size_t)n * csz), "chirp");
+  AFC_CUDA(gen_chirp_dev(ap.chirp, n, dbl, st), "chirp");
+  AFC_CUDA(dev_alloc(&ap.spec_f, (size_t)M * csz), "Bluestein spectrum");
+  AFC_CUDA(dev_alloc(&ap.spec_i, (size_t)M * csz), "Bluestein spectrum");
+  AFC_CUDA(gen_bluestein_b_dev(ap.spec_f, ap.chirp, n, M, false, dbl, st), "Bluestein kernel");
+  AFC_CUDA(gen_bluestein_b_dev(ap.spec_i, ap.chirp, n, M, true, dbl, st), "Bluestein kernel");
+  afc_status s;
+  if (plannable(M, csz)) {
+    ap.conv_smem = true;
+    s = build_lenplan(M, dbl, ap.lp, st);
+    if (s != AFC_OK) return s;
+    AxisPlan mp;
+    mp.n = M;
+    mp.algo = ALGO_SMEM;
+    mp.lp = ap.lp;
+    s = fft_table(mp, dbl, ap.spec_f, st);
+    if (s == AFC_OK) s = fft_table(mp, dbl, ap.spec_i, st);
+    mp.lp.tw = nullptr;
+    return s;
+  }
+  ap.conv_smem = false;
+  ap.sub.reset(new AxisPlan());
+  ap.sub->n = M;
+  s = build_fourstep(M, dbl, *ap.sub, st);
+  if (s != AFC_OK) return s;
+  s = fft_table(*ap.sub, dbl, ap.spec_f, st);
+  if (s == AFC_OK) s = fft_table(*ap.sub, dbl, ap.spec_i, st);
+  return s;
+}
+
+// ───────────────────────────── plans ─────────────────────────────
+
+struct PlanKey {
+  int rank;
+  int64_t d[3];
+  int prec, kind;
+  int64_t batch;
+  int device;
+  bool operator<(const PlanKey& o) const {
+    return std::tie(rank, d[0], d[1], d[2], prec, kind, batch, device) <
+           std::tie(o.rank, o.d[0], o.d[1], o.d[2], o.prec, o.kind, o.batch, o.device);
+  }
+};
+
+}  // namespace afc
+
+struct afc_plan_s {
+  int rank = 0;
+  int64_t dims[3] = {1, 1, 1};
+  afc_precision prec = AFC_PREC_F64;
+  afc_kind kind = AFC_KIND_C2C;
+  int64_t batch = 1;
+  int device = 0;
+  bool dbl = true;
+  std::unique_ptr<afc::AxisPlan> axes[3];
+  std::atomic<int> refs{1};
+  bool cached = false;
+  afc::PlanKey key{};
+  std::mutex ws_mu;
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  void* host_in = nullptr;   // staging for afc_execute_host
+  void* host_out = nullptr;
+  cudaStream_t host_stream = nullptr;
+  int64_t N() const { return dims[0] * dims[1] * dims[2]; }
+  ~afc_plan_s() {
+    if (ws) cudaFree(ws);
+    if (host_in) cudaFree(host_in);
+    if (host_out) cudaFree(host_out);
+    if (host_stream) cudaStreamDestroy(host_stream);
+  }
+};
+
+namespace afc {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+static int64_t last_len(const afc_plan_s& p) { return p.dims[p.rank - 1]; }
+static int64_t half_len(const afc_plan_s& p) { return last_len(p) / 2 + 1; }
+
+// Element counts of the arrays one execution touches.
+static void io_elems(const afc_plan_s& p, bool inv, int64_t& in_e, int64_t& out_e) {
+  const int64_t N = p.N() * p.batch;
+  const int64_t Nh = N / last_len(p) * half_len(p);
+  switch (p.kind) {
+    case AFC_KIND_C2C: in_e = out_e = N; break;
+    case AFC_KIND_R2C_FULL: in_e = out_e = N; break;
+    case AFC_KIND_R2C_HALF:
+      in_e = inv ? Nh : N;
+      out_e = inv ? N : Nh;
+      break;
+  }
+}
+
+// Lane map of axis a in the (batch, d0..d_{r-1}) array whose last dim is `last`.
+static LaneMap axis_map(const afc_plan_s& p, int a, int64_t last, long long& lanes) {
+  int64_t shp[3] = {p.dims[0], p.dims[1], p.dims[2]};
+  shp[p.rank - 1] = last;
+  int64_t es = 1;
+  for (int b = a + 1; b < p.rank; ++b) es *= shp[b];
+  int64_t total = p.batch;
+  for (int b = 0; b < p.rank; ++b) total *= shp[b];
+  lanes = total / shp[a];
+  if (es == 1) return LaneMap{1, 1, shp[a], 0, 0, 1, nullptr};
+  return LaneMap{1, es, shp[a] * es, 0, 1, es, nullptr};
+}
+
+static size_t plan_ws_bytes(const afc_plan_s& p) {
+  const size_t csz = p.dbl ? 16 : 8;
+  size_t need = 0;
+  for (int a = 0; a < p.rank; ++a) {
+    long long lanes;
+    int64_t last = (p.kind == AFC_KIND_R2C_HALF && a != p.rank - 1) ? half_len(p) : last_len(p);
+    axis_map(p, a, last, lanes);
+    need = std::max(need, axis_ws_bytes(*p.axes[a], lanes, csz));
+  }
+  // C2R forms keep their complex intermediate in the workspace.
+  size_t inter = 0;
+  if (p.rank > 1 && p.kind == AFC_KIND_R2C_FULL) inter = (size_t)p.N() * p.batch * csz;
+  if (p.rank > 1 && p.kind == AFC_KIND_R2C_HALF) inter = (size_t)(p.N() / last_len(p) * half_len(p)) * p.batch * csz;
+  inter = (inter + 255) / 256 * 256;
+  return inter + need;
+}
+
+// Runs one transform of the plan.  scale is applied on the last pass;
+// pair_w is the Hermitian weight used by the R2C_HALF adjoints.
+static cudaError_t run_plan(const afc_plan_s& p, const void* in, void* out, bool inv, double scale, double pair_w,
+                            void* ws, cudaStream_t st) {
+  const size_t csz = p.dbl ? 16 : 8;
+  const int r = p.rank;
+  const int64_t n_last = last_len(p), h = half_len(p);
+  size_t inter_b = 0;
+  if (r > 1 && p.kind == AFC_KIND_R2C_FULL) inter_b = (size_t)p.N() * p.batch * csz;
+  if (r > 1 && p.kind == AFC_KIND_R2C_HALF) inter_b = (size_t)(p.N() / n_last * h) * p.batch * csz;
+  inter_b = (inter_b + 255) / 256 * 256;
+  void* inter = ws;
+  void* axis_ws = static_cast<char*>(ws) + inter_b;
+
+  // Pass order: forward last axis first (plan/fft/dimension_3d.rs:148-157,
+  // dimension_2d.rs forward rows then columns); inverse first axis first.
+  std::vector<int> order;
+  if (!inv) for (int a = r - 1; a >= 0; --a) order.push_back(a);
+  else for (int a = 0; a < r; ++a) order.push_back(a);
+  // Skip length-1 axes (no-op passes) unless they carry a dtype change.
+  const void* src = in;
+  void* dst = out;
+  bool first = true;
+  for (size_t k = 0; k < order.size(); ++k) {
+    const int a = order[k];
+    const bool lastpass = k + 1 == order.size();
+    const AxisPlan& ap = *p.axes[a];
+    AxisIO io;
+    io.scale = lastpass ? scale : 1.0;
+    io.pair_w = 1.0;
+    long long lanes = 0;
+    if (p.kind == AFC_KIND_C2C) {
+      io.im = io.om = axis_map(p, a, n_last, lanes);
+      io.in = first ? src : dst;
+      io.out = dst;
+    } else if (p.kind == AFC_KIND_R2C_FULL) {
+      io.im = io.om = axis_map(p, a, n_last, lanes);
+      if (!inv) {
+        io.in = first ? src : dst;
+        io.out = dst;
+        if (first) io.in_op = IN_R;
+      } else {
+        void* cbuf = (r > 1) ? inter : nullptr;
+        io.in = first ? src : cbuf;
+        io.out = lastpass ? dst : cbuf;
+        if (lastpass) io.out_op = OUT_RE;
+      }
+    } else {  // R2C_HALF
+      if (!inv) {
+        if (first) {  // a == r-1: real rows of n -> half rows of h
+          long long l2;
+          io.im = axis_map(p, a, n_last, lanes);
+          io.om = axis_map(p, a, h, l2);
+          io.in = src;
+          io.out = dst;
+          io.in_op = IN_R;
+          io.out_op = OUT_TRUNC;
+          io.nlen = h;
+          io.herm_n = n_last;
+          io.pair_w = pair_w;
+        } else {
+          io.im = io.om = axis_map(p, a, h, lanes);
+          io.in = dst;
+          io.out = dst;
+        }
+      } else {
+        if (!lastpass) {  // leading axes on the half array, into the intermediate
+          io.im = io.om = axis_map(p, a, h, lanes);
+          io.in = first ? src : inter;
+          io.out = inter;
+        } else {  // a == r-1: half rows -> real rows
+          long long l2;
+          io.im = axis_map(p, a, h, lanes);
+          io.om = axis_map(p, a, n_last, l2);
+          io.in = (r > 1) ? inter : src;
+          io.out = dst;
+          io.in_op = IN_HERM;
+          io.out_op = OUT_RE;
+          io.herm_n = n_last;
+          io.pair_w = pair_w;
+        }
+      }
+    }
+    io.lanes = lanes;
+    // A length-1 axis is the identity, but it may still have to move or convert data.
+    if (ap.algo == ALGO_NOOP) {
+      AxisPlan one;
+      one.n = 1;
+      if (io.in == io.out && io.in_op == IN_C && io.out_op == OUT_C && io.scale == 1.0) {
+        first = false;
+        continue;
+      }
+      // route through a radix-free copy: a length-1 "transform" is a scaled copy
+      LaunchDesc d;
+      d.sl.n = 1;
+      d.sl.nst = 0;
+      d.P = 1;
+      d.ld = 3;
+      d.lanes = io.lanes;
+      d.im = io.im;
+      d.om = io.om;
+      d.in = io.in;
+      d.out = io.out;
+      d.in_op = io.in_op;
+      d.out_op = io.out_op;
+      d.scale = io.scale;
+      d.nlen = io.nlen ? io.nlen : 1;
+      d.herm_n = io.herm_n ? io.herm_n : 1;
+      d.pair_w = io.pair_w;
+      d.stage_in = d.stage_out = true;
+      d.L = (int)std::min<long long>(256, std::max(1LL, io.lanes));
+      cudaError_t e = launch_lanes(d, p.dbl, inv, st);
+      if (e != cudaSuccess) return e;
+      first = false;
+      continue;
+    }
+    cudaError_t e = exec_axis(ap, p.dbl, inv, io, axis_ws, st);
+    if (e != cudaSuccess) return e;
+    first = false;
+  }
+  return cudaSuccess;
+}
+
+static std::mutex g_cache_mu;
+static std::map<PlanKey, afc_plan_s*> g_cache;
+
+static afc_status create_plan(afc_plan* out, int rank, const int64_t* dims, afc_precision prec, afc_kind kind,
+                              int64_t batch, int device) {
+  if (!out) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  *out = nullptr;
+  if (rank < 1 || rank > 3) return fail(AFC_ERR_VALIDATION, "validation failed for `rank`: `%d` violates `1..=3`", rank);
+  if (!dims) return fail(AFC_ERR_VALIDATION, "validation failed for `dims`: `null` violates `must be non-null`");
+  static const char* names[3][3] = {{"n", "", ""}, {"nx", "ny", ""}, {"nx", "ny", "nz"}};
+  for (int a = 0; a < rank; ++a)
+    if (dims[a] <= 0)
+      return fail(AFC_ERR_VALIDATION, "validation failed for `%s`: `%lld` violates `must be > 0`", names[rank - 1][a],
+                  (long long)dims[a]);
+  if (batch < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `batch`: `%lld` violates `must be > 0`", (long long)batch);
+  if (prec != AFC_PREC_F32 && prec != AFC_PREC_F64)
+    return fail(AFC_ERR_UNSUPPORTED, "precision %d needs the tensor-core plan (afc_tc_* entry points)", (int)prec);
+  if (kind != AFC_KIND_C2C && kind != AFC_KIND_R2C_FULL && kind != AFC_KIND_R2C_HALF)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `kind`: `%d` violates `C2C|R2C_FULL|R2C_HALF`", (int)kind);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(AFC_ERR_BACKEND_UNAVAILABLE, "backend unavailable: cuda (no device)");
+  if (device < 0 || device >= ndev)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `device`: `%d` violates `< %d`", device, ndev);
+  DeviceGuard g(device);
+  std::unique_ptr<afc_plan_s> p(new afc_plan_s());
+  p->rank = rank;
+  for (int a = 0; a < rank; ++a) p->dims[a] = dims[a];
+  p->prec = prec;
+  p->kind = kind;
+  p->batch = batch;
+  p->device = device;
+  p->dbl = prec == AFC_PREC_F64;
+  cudaStream_t st;
+  AFC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+  afc_status s = AFC_OK;
+  for (int a = 0; a < rank && s == AFC_OK; ++a) {
+    p->axes[a].reset(new AxisPlan());
+    s = build_axis(dims[a], p->dbl, *p->axes[a], st);
+  }
+  if (s == AFC_OK && kind == AFC_KIND_R2C_HALF) {
+    const AxisPlan& la = *p->axes[rank - 1];
+    if (la.algo != ALGO_SMEM && la.algo != ALGO_FOURSTEP && la.algo != ALGO_NOOP)
+      s = fail(AFC_ERR_UNSUPPORTED, "half-spectrum plans need a smooth last dimension (got %lld)", (long long)dims[rank - 1]);
+  }
+  cudaError_t e = cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  if (s != AFC_OK) return s;
+  if (e != cudaSuccess) return cuda_fail(e, "plan build");
+  p->ws_bytes = plan_ws_bytes(*p);
+  *out = p.release();
+  return AFC_OK;
+}
+
+static afc_status execute(afc_plan p, const void* in, void* out, afc_direction dir, double scale, bool use_scale,
+                          double pair_w, void* ws, size_t ws_bytes, bool own_ws, void* stream) {
+  if (!p) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (!in || !out) return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  if (dir != AFC_FORWARD && dir != AFC_INVERSE)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `direction`: `%d` violates `FORWARD|INVERSE`", (int)dir);
+  const bool inv = dir == AFC_INVERSE;
+  if (in == out && p->kind != AFC_KIND_C2C)
+    return fail(AFC_ERR_SHAPE_MISMATCH, "shape mismatch: expected distinct real and complex buffers, got in == out");
+  const double sc = use_scale ? scale : (inv ? 1.0 / (double)p->N() : 1.0);
+  DeviceGuard g(p->device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (own_ws) {
+    std::lock_guard<std::mutex> lk(p->ws_mu);
+    if (p->ws_bytes && !p->ws) AFC_CUDA(dev_alloc(&p->ws, p->ws_bytes), "workspace");
+    cudaError_t e = run_plan(*p, in, out, inv, sc, pair_w, p->ws, st);
+    if (e != cudaSuccess) return cuda_fail(e, "execute");
+    return AFC_OK;
+  }
+  if (ws_bytes < p->ws_bytes)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `workspace_bytes`: `%zu` violates `>= %zu`", ws_bytes, p->ws_bytes);
+  if (p->ws_bytes && !ws) return fail(AFC_ERR_VALIDATION, "validation failed for `workspace`: `null` violates `must be non-null`");
+  cudaError_t e = run_plan(*p, in, out, inv, sc, pair_w, ws, st);
+  if (e != cudaSuccess) return cuda_fail(e, "execute");
+  return AFC_OK;
+}
+
+// ───────────────────────────── uneven batches ─────────────────────────────
+
+struct BatchGroup {
+  int64_t n = 0;
+  long long lanes = 0;
+  std::unique_ptr<AxisPlan> ap;
+  long long* d_off = nullptr;  // device lane offsets (packed layout)
+  ~BatchGroup() {
+    if (d_off) cudaFree(d_off);
+  }
+};
+
+}  // namespace afc
+
+struct afc_batch_plan_s {
+  bool dbl = false;
+  int device = 0;
+  int64_t total = 0;
+  std::vector<int64_t> lengths;
+  std::vector<std::unique_ptr<afc::BatchGroup>> groups;
+  size_t ws_bytes = 0;
+  void* ws = nullptr;
+  std::mutex mu;
+  // CUDA graph of the per-length launches, keyed by (in, out, direction)
+  cudaGraphExec_t gexec = nullptr;
+  const void* g_in = nullptr;
+  void* g_out = nullptr;
+  int g_dir = -1;
+  ~afc_batch_plan_s() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (ws) cudaFree(ws);
+  }
+};
+
+namespace afc {
+
+static cudaError_t run_batch(afc_batch_plan_s& bp, const void* in, void* out, bool inv, cudaStream_t st) {
+  const size_t csz = bp.dbl ? 16 : 8;
+  (void)csz;
+  for (auto& g : bp.groups) {
+    AxisIO io;
+    io.in = in;
+    io.out = out;
+    io.lanes = g->lanes;
+    io.im = LaneMap{1, 1, 0, 0, 1, 1, g->d_off};
+    io.om = io.im;
+    io.scale = inv ? 1.0 / (double)g->n : 1.0;
+    cudaError_t e;
+    if (g->ap->algo == ALGO_NOOP) {
+      if (in == out) continue;
+      LaunchDesc d;
+      d.sl.n = 1;
+      d.sl.nst = 0;
+      d.P = 1;
+      d.ld = 3;
+      d.lanes = io.lanes;
+      d.im = io.im;
+      d.om = io.om;
+      d.in = in;
+      d.out = out;
+      d.stage_in = d.stage_out = true;
+      d.L = (int)std::min<long long>(256, std::max(1LL, io.lanes));
+      e = launch_lanes(d, bp.dbl, inv, st);
+    } else {
+      e = exec_axis(*g->ap, bp.dbl, inv, io, bp.ws, st);
+    }
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace afc
+
+using namespace afc;
+
+extern "C" {
+
+afc_status afc_plan_create(afc_plan* out, int rank, const int64_t* dims, afc_precision precision, afc_kind kind,
+                           int64_t batch, int device) {
+  return create_plan(out, rank, dims, precision, kind, batch, device);
+}
+
+afc_status afc_plan_get_cached(afc_plan* out, int rank, const int64_t* dims, afc_precision precision, afc_kind kind,
+                               int64_t batch, int device) {
+  if (!out) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (rank < 1 || rank > 3 || !dims) return create_plan(out, rank, dims, precision, kind, batch, device);
+  PlanKey k{};
+  k.rank = rank;
+  for (int a = 0; a < 3; ++a) k.d[a] = a < rank ? dims[a] : 1;
+  k.prec = precision;
+  k.kind = kind;
+  k.batch = batch;
+  k.device = device;
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  auto it = g_cache.find(k);
+  if (it != g_cache.end()) {
+    it->second->refs.fetch_add(1);
+    *out = it->second;
+    return AFC_OK;
+  }
+  afc_plan p = nullptr;
+  afc_status s = create_plan(&p, rank, dims, precision, kind, batch, device);
+  if (s != AFC_OK) return s;
+  p->cached = true;
+  p->key = k;
+  p->refs.store(2);  // one for the cache, one for the caller
+  g_cache[k] = p;
+  *out = p;
+  return AFC_OK;
+}
+
+afc_status afc_plan_destroy(afc_plan plan) {
+  if (!plan) return AFC_OK;
+  if (plan->cached) {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    if (plan->refs.fetch_sub(1) > 1) return AFC_OK;
+    g_cache.erase(plan->key);
+  } else if (plan->refs.fetch_sub(1) > 1) {
+    return AFC_OK;
+  }
+  DeviceGuard g(plan->device);
+  delete plan;
+  return AFC_OK;
+}
+
+afc_status afc_execute(afc_plan plan, const void* in, void* out, afc_direction direction, void* stream) {
+  return execute(plan, in, out, direction, 0.0, false, 1.0, nullptr, 0, true, stream);
+}
+
+afc_status afc_execute_scaled(afc_plan plan, const void* in, void* out, afc_direction direction, double scale,
+                              void* stream) {
+  return execute(plan, in, out, direction, scale, true, 1.0, nullptr, 0, true, stream);
+}
+
+afc_status afc_execute_adjoint(afc_plan plan, const void* in, void* out, afc_direction direction, void* stream) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  const double N = (double)plan->N();
+  // adjoint of forward = unnormalized inverse map; adjoint of inverse = forward / N
+  if (direction == AFC_FORWARD) {
+    double pw = plan->kind == AFC_KIND_R2C_HALF ? 0.5 : 1.0;
+    return execute(plan, in, out, AFC_INVERSE, 1.0, true, pw, nullptr, 0, true, stream);
+  }
+  if (direction == AFC_INVERSE) {
+    double pw = plan->kind == AFC_KIND_R2C_HALF ? 2.0 : 1.0;
+    return execute(plan, in, out, AFC_FORWARD, 1.0 / N, true, pw, nullptr, 0, true, stream);
+  }
+  return fail(AFC_ERR_VALIDATION, "validation failed for `direction`: `%d` violates `FORWARD|INVERSE`", (int)direction);
+}
+
+afc_status afc_workspace_size(afc_plan plan, size_t* bytes) {
+  if (!plan || !bytes) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  *bytes = plan->ws_bytes;
+  return AFC_OK;
+}
+
+afc_status afc_execute_ws(afc_plan plan, const void* in, void* out, afc_direction direction, double scale, int use_scale,
+                          void* workspace, size_t workspace_bytes, void* stream) {
+  return execute(plan, in, out, direction, scale, use_scale != 0, 1.0, workspace, workspace_bytes, false, stream);
+}
+
+afc_status afc_plan_io_elems(afc_plan plan, afc_direction direction, int64_t* in_elems, int64_t* out_elems) {
+  if (!plan || !in_elems || !out_elems)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  int64_t a, b;
+  io_elems(*plan, direction == AFC_INVERSE, a, b);
+  *in_elems = a;
+  *out_elems = b;
+  return AFC_OK;
+}
+
+afc_status afc_execute_host(afc_plan plan, const void* host_in, void* host_out, afc_direction direction) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (!host_in || !host_out) return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  const bool inv = direction == AFC_INVERSE;
+  int64_t ie, oe;
+  io_elems(*plan, inv, ie, oe);
+  const size_t csz = plan->dbl ? 16 : 8, rsz = plan->dbl ? 8 : 4;
+  bool real_in = plan->kind != AFC_KIND_C2C && !inv;
+  bool real_out = plan->kind != AFC_KIND_C2C && inv;
+  const size_t ib = (size_t)ie * (real_in ? rsz : csz), ob = (size_t)oe * (real_out ? rsz : csz);
+  const size_t maxb = (size_t)std::max(ie, oe) * csz;
+  DeviceGuard g(plan->device);
+  {
+    std::lock_guard<std::mutex> lk(plan->ws_mu);
+    if (!plan->host_stream) AFC_CUDA(cudaStreamCreateWithFlags(&plan->host_stream, cudaStreamNonBlocking), "stream");
+    if (!plan->host_in) AFC_CUDA(dev_alloc(&plan->host_in, maxb), "staging");
+    if (!plan->host_out) AFC_CUDA(dev_alloc(&plan->host_out, maxb), "staging");
+  }
+  cudaStream_t st = plan->host_stream;
+  AFC_CUDA(cudaMemcpyAsync(plan->host_in, host_in, ib, cudaMemcpyHostToDevice, st), "host to device");
+  afc_status s = afc_execute(plan, plan->host_in, plan->host_out, direction, st);
+  if (s != AFC_OK) return s;
+  AFC_CUDA(cudaMemcpyAsync(host_out, plan->host_out, ob, cudaMemcpyDeviceToHost, st), "device to host");
+  AFC_CUDA(cudaStreamSynchronize(st), "synchronize");
+  return AFC_OK;
+}
+
+afc_status afc_capabilities(afc_capabilities_t* caps) {
+  if (!caps) return fail(AFC_ERR_VALIDATION, "validation failed for `caps`: `null` violates `must be non-null`");
+  memset(caps, 0, sizeof(*caps));
+  caps->kind = 2;
+  caps->normalization = 0;
+  caps->supports_1d = caps->supports_2d = caps->supports_3d = 1;
+  caps->supports_real_to_complex = 1;
+  caps->supports_mixed_precision = 1;
+  caps->default_precision = AFC_PREC_F64;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+  caps->device_count = n;
+  if (n > 0) {
+    cudaDeviceProp pr;
+    if (cudaGetDeviceProperties(&pr, 0) == cudaSuccess) {
+      caps->sm_count = pr.multiProcessorCount;
+      caps->cc_major = pr.major;
+      caps->cc_minor = pr.minor;
+      caps->max_smem_per_block = pr.sharedMemPerBlockOptin;
+    }
+  }
+  return AFC_OK;
+}
+
+afc_status afc_length_info(uint64_t n, afc_length_info_t* info) {
+  if (!info) return fail(AFC_ERR_VALIDATION, "validation failed for `info`: `null` violates `must be non-null`");
+  memset(info, 0, sizeof(*info));
+  if (n == 0) return fail(AFC_ERR_VALIDATION, "validation failed for `n`: `0` violates `must be > 0`");
+  info->strategy = strategy_of(n);
+  std::vector<u64> f;
+  if (factorize23(n, f)) {
+    auto lo = lower_pairs(f);
+    info->n_radices = (int)lo.size();
+    for (size_t i = 0; i < lo.size() && i < 64; ++i) info->radices[i] = lo[i];
+  } else {
+    info->n_radices = -1;
+  }
+  u64 a, b;
+  if (coprime_split(n, a, b)) { info->coprime_n1 = a; info->coprime_n2 = b; }
+  if ((n & (n - 1)) == 0 && n > 1) {
+    unsigned k = __builtin_ctzll(n), k1 = k / 2;
+    info->four_step_n1 = 1ull << k1;
+    info->four_step_n2 = 1ull << (k - k1);
+  }
+  info->is_prime = is_prime_u(n);
+  if (info->is_prime) {
+    info->primitive_root = primitive_root_u(n);
+    info->primitive_root_inv = inv_mod(info->primitive_root, n);
+  }
+  info->is_short_winograd = short_winograd(n);
+  info->has_static_coprime_codelet = coprime_split(n, a, b) ? static_coprime_codelet(a, b) : 0;
+  // GPU choice (as build_axis would make it for f64)
+  std::vector<int> rad;
+  if (n <= 1) info->gpu_algo = ALGO_NOOP;
+  else if (gpu_radices((int64_t)n, rad)) {
+    if (plannable((int64_t)n, 16)) {
+      info->gpu_algo = ALGO_SMEM;
+      info->gpu_n_radices = (int)rad.size();
+      for (size_t i = 0; i < rad.size(); ++i) info->gpu_radices[i] = rad[i];
+    } else {
+      info->gpu_algo = ALGO_FOURSTEP;
+    }
+  } else if (is_prime_u(n) && (int64_t)n < kRaderMax) {
+    info->gpu_algo = ALGO_RADER;
+    int64_t L = (int64_t)n - 1, M = L;
+    if (!plannable(L, 16)) { M = 1; while (M < 2 * L - 1) M <<= 1; }
+    info->gpu_conv_len = (u64)M;
+  } else {
+    info->gpu_algo = ALGO_BLUESTEIN;
+    int64_t M = 1;
+    while (M < 2 * (int64_t)n - 1) M <<= 1;
+    info->gpu_conv_len = (u64)M;
+  }
+  return AFC_OK;
+}
+
+afc_status afc_rader_maps(uint64_t p, uint64_t* gather, uint64_t* scatter) {
+  if (!gather || !scatter) return fail(AFC_ERR_VALIDATION, "validation failed for `maps`: `null` violates `must be non-null`");
+  if (!is_prime_u(p)) return fail(AFC_ERR_VALIDATION, "validation failed for `p`: `%llu` violates `must be prime`", (unsigned long long)p);
+  const u64 g = primitive_root_u(p), L = p - 1;
+  u64 v = 1;
+  for (u64 q = 0; q < L; ++q) { gather[q] = v; v = mulmod(v, g, p); }
+  for (u64 q = 0; q < L; ++q) scatter[q] = q == 0 ? gather[0] : gather[L - q];
+  return AFC_OK;
+}
+
+afc_status afc_pfa_perm(uint64_t n1, uint64_t n2, uint64_t* in_perm, uint64_t* out_perm) {
+  if (!in_perm || !out_perm) return fail(AFC_ERR_VALIDATION, "validation failed for `perm`: `null` violates `must be non-null`");
+  u64 a = n1, b = n2;
+  while (b) { u64 t = a % b; a = b; b = t; }
+  if (n1 < 1 || n2 < 1 || a != 1)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `n1,n2`: `%llu,%llu` violates `coprime`", (unsigned long long)n1,
+                (unsigned long long)n2);
+  const u64 n = n1 * n2;
+  const u64 i21 = n1 > 1 ? inv_mod(n2 % n1, n1) : 0, i12 = n2 > 1 ? inv_mod(n1 % n2, n2) : 0;
+  for (u64 x = 0; x < n1; ++x)
+    for (u64 y = 0; y < n2; ++y) in_perm[x * n2 + y] = (x * n2 + y * n1) % n;
+  for (u64 k1 = 0; k1 < n1; ++k1)
+    for (u64 k2 = 0; k2 < n2; ++k2)
+      out_perm[k2 * n1 + k1] = (u64)(((unsigned __int128)k1 * n2 * i21 + (unsigned __int128)k2 * n1 * i12) % n);
+  return AFC_OK;
+}
+
+afc_status afc_plan_describe(afc_plan plan, int axis, afc_length_info_t* info) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (axis < 0 || axis >= plan->rank) return fail(AFC_ERR_VALIDATION, "validation failed for `axis`: `%d` violates `< rank`", axis);
+  afc_status s = afc_length_info((uint64_t)plan->dims[axis], info);
+  if (s != AFC_OK) return s;
+  const AxisPlan& ap = *plan->axes[axis];
+  info->gpu_algo = ap.algo;
+  info->gpu_conv_len = (u64)ap.M;
+  info->gpu_split_n1 = (u64)ap.N1;
+  info->gpu_split_n2 = (u64)ap.N2;
+  const LenPlan& lp = ap.algo == ALGO_FOURSTEP ? ap.lp1 : ap.lp;
+  info->gpu_n_radices = ap.algo == ALGO_FOURSTEP ? 0 : lp.sl.nst;
+  for (int s2 = 0; s2 < info->gpu_n_radices; ++s2) info->gpu_radices[s2] = lp.sl.st[s2].R;
+  return AFC_OK;
+}
+
+
+afc_status afc_batch_plan_create(afc_batch_plan* out, const int64_t* lengths, int64_t count, afc_precision precision,
+                                 int device) {
+  if (!out) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  *out = nullptr;
+  if (!lengths || count < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `count`: `%lld` violates `must be > 0`", (long long)count);
+  if (precision != AFC_PREC_F32 && precision != AFC_PREC_F64)
+    return fail(AFC_ERR_UNSUPPORTED, "batch plans support f32 and f64");
+  for (int64_t i = 0; i < count; ++i)
+    if (lengths[i] <= 0) return fail(AFC_ERR_VALIDATION, "validation failed for `lengths[%lld]`: `%lld` violates `must be > 0`", (long long)i, (long long)lengths[i]);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(AFC_ERR_BACKEND_UNAVAILABLE, "backend unavailable: cuda (no device)");
+  if (device < 0 || device >= ndev) return fail(AFC_ERR_VALIDATION, "validation failed for `device`: `%d` violates `< %d`", device, ndev);
+  DeviceGuard g(device);
+  std::unique_ptr<afc_batch_plan_s> bp(new afc_batch_plan_s());
+  bp->dbl = precision == AFC_PREC_F64;
+  bp->device = device;
+  bp->lengths.assign(lengths, lengths + count);
+  std::map<int64_t, std::vector<long long>> by_len;
+  long long off = 0;
+  for (int64_t i = 0; i < count; ++i) {
+    by_len[lengths[i]].push_back(off);
+    off += lengths[i];
+  }
+  bp->total = off;
+  cudaStream_t st;
+  AFC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+  const size_t csz = bp->dbl ? 16 : 8;
+  afc_status s = AFC_OK;
+  for (auto& kv : by_len) {
+    std::unique_ptr<BatchGroup> grp(new BatchGroup());
+    grp->n = kv.first;
+    grp->lanes = (long long)kv.second.size();
+    grp->ap.reset(new AxisPlan());
+    s = build_axis(kv.first, bp->dbl, *grp->ap, st);
+    if (s != AFC_OK) break;
+    cudaError_t e = dev_alloc((void**)&grp->d_off, kv.second.size() * sizeof(long long));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(grp->d_off, kv.second.data(), kv.second.size() * sizeof(long long), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) { s = cuda_fail(e, "batch offsets"); break; }
+    bp->ws_bytes = std::max(bp->ws_bytes, axis_ws_bytes(*grp->ap, grp->lanes, csz));
+    bp->groups.push_back(std::move(grp));
+  }
+  cudaError_t e = cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  if (s != AFC_OK) return s;
+  if (e != cudaSuccess) return cuda_fail(e, "batch plan build");
+  if (bp->ws_bytes) AFC_CUDA(dev_alloc(&bp->ws, bp->ws_bytes), "batch workspace");
+  *out = bp.release();
+  return AFC_OK;
+}
+
+afc_status afc_batch_plan_destroy(afc_batch_plan plan) {
+  if (!plan) return AFC_OK;
+  DeviceGuard g(plan->device);
+  delete plan;
+  return AFC_OK;
+}
+
+afc_status afc_batch_total_elems(afc_batch_plan plan, int64_t* elems) {
+  if (!plan || !elems) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  *elems = plan->total;
+  return AFC_OK;
+}
+
+afc_status afc_batch_execute(afc_batch_plan plan, const void* in, void* out, afc_direction direction, int mode,
+                             void* stream) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (!in || !out) return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  if (direction != AFC_FORWARD && direction != AFC_INVERSE)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `direction`: `%d` violates `FORWARD|INVERSE`", (int)direction);
+  const bool inv = direction == AFC_INVERSE;
+  DeviceGuard g(plan->device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::lock_guard<std::mutex> lk(plan->mu);
+  if (mode == 1) {
+    cudaError_t e = run_batch(*plan, in, out, inv, st);
+    if (e != cudaSuccess) return cuda_fail(e, "batch execute");
+    return AFC_OK;
+  }
+  // mode 0: the whole batch as one CUDA graph, captured once per (in, out, direction)
+  if (!plan->gexec || plan->g_in != in || plan->g_out != out || plan->g_dir != (int)direction) {
+    if (plan->gexec) { cudaGraphExecDestroy(plan->gexec); plan->gexec = nullptr; }
+    cudaStream_t cs;
+    AFC_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      cudaError_t e2 = run_batch(*plan, in, out, inv, cs);
+      e = cudaStreamEndCapture(cs, &graph);
+      if (e2 != cudaSuccess) e = e2;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&plan->gexec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) return cuda_fail(e, "batch graph capture");
+    plan->g_in = in;
+    plan->g_out = out;
+    plan->g_dir = (int)direction;
+  }
+  AFC_CUDA(cudaGraphLaunch(plan->gexec, st), "batch graph launch");
+  return AFC_OK;
+}
+
+const char* afc_last_error_message(void) { return g_last_error.c_str(); }
+
+uint64_t afc_kernel_launch_count(void) { return g_launches.load(); }
+
+// Test hook (not part of the public header): the next `count` device
+// allocations fail, so tests can check the AFC_ERR_OUT_OF_MEMORY path.
+AFC_API void afc_test_fail_next_allocs(int count) { g_fail_allocs.store(count); }
+
+}  // extern "C"

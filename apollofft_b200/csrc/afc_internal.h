@@ -1,0 +1,64 @@
+// afc_internal.h -- host <-> kernel interface inside libapollofft_cuda.so.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include "afc_engine.cuh"
+
+namespace afc {
+
+enum InOpKind { IN_C = 0, IN_R = 1, IN_HERM = 2, IN_CHIRP = 3, IN_CHIRP_R = 4, IN_GATHER = 5, IN_GATHER_R = 6 };
+enum OutOpKind {
+  OUT_C = 0, OUT_RE = 1, OUT_TRUNC = 2, OUT_TW = 3, OUT_MUL = 4, OUT_CHIRP = 5, OUT_CHIRP_RE = 6,
+  OUT_SCATTER = 7, OUT_SCATTER_RE = 8
+};
+
+// Everything one launch of the lanes / conv kernels needs (type-erased).
+struct LaunchDesc {
+  StageList sl;
+  const void* tw = nullptr;
+  long long lanes = 0;
+  int L = 1, P = 1, ld = 1;
+  LaneMap im{}, om{};
+  const void* in = nullptr;
+  void* out = nullptr;
+  double scale = 1.0;
+  int in_op = IN_C, out_op = OUT_C;
+  bool stage_in = false, stage_out = false;
+  long long jmul = 1, col_div = 1, col_mod = 1;
+  long long nlen = 0, herm_n = 0;
+  double pair_w = 1.0;
+  long long twN = 1, twB = 1;
+  int tw_conj = 0;
+  const void* tw_hi = nullptr;
+  const void* tw_lo = nullptr;
+  const void* spec = nullptr;
+  const void* chirp = nullptr;
+  int chirp_conj = 0;
+  const int* gather = nullptr;
+  const int* scatter = nullptr;
+};
+
+// dynamic shared memory of lanes_kernel: L lanes x buffers x ld + 3 L lane descriptors
+inline size_t lanes_smem_bytes(const LaunchDesc& d, size_t csz) {
+  const int nbuf = engine_buffers(d.sl.nst, d.stage_in, d.stage_out);
+  return (size_t)d.L * nbuf * (size_t)d.ld * csz + (size_t)d.L * 3 * sizeof(long long);
+}
+// conv_kernel: L lanes x 2 buffers x ld + 2 L extra complex + 2 L lane descriptors
+inline size_t conv_smem_bytes(const LaunchDesc& d, size_t csz) {
+  return (size_t)d.L * 2 * (size_t)d.ld * csz + (size_t)d.L * 2 * csz + (size_t)d.L * 2 * sizeof(long long);
+}
+
+cudaError_t launch_lanes(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st);
+cudaError_t launch_conv(const LaunchDesc& d, bool dbl, cudaStream_t st);
+
+cudaError_t gen_stage_twiddles_dev(void* tw, const StageList& sl, bool dbl, cudaStream_t st);
+cudaError_t gen_roots_dev(void* out, long long cnt, long long mult, long long N, bool dbl, cudaStream_t st);
+cudaError_t gen_chirp_dev(void* out, long long n, bool dbl, cudaStream_t st);
+cudaError_t gen_bluestein_b_dev(void* b, const void* chirp, long long n, long long M, bool inverse, bool dbl,
+                                cudaStream_t st);
+cudaError_t gen_rader_b_dev(void* b, const int* scatter, long long p, long long M, bool inverse, bool dbl,
+                            cudaStream_t st);
+
+void count_launch(int k);
+
+}  // namespace afc

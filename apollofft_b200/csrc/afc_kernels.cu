@@ -1,0 +1,493 @@
+// afc_kernels.cu -- sm_100a kernels of apollofft_b200 and their launchers.
+//
+// lanes_kernel     : L lanes per CTA through the Stockham engine; the global
+//                    load/store operator is chosen per launch (complex, real
+//                    widen, Hermitian expand, chirp premultiply / four-step
+//                    twiddle, pointwise spectrum, real part, truncation,
+//                    chirp postmultiply).
+// conv_kernel      : a whole Rader or Bluestein transform per lane in shared
+//                    memory: staged gather (generator order) or chirp
+//                    premultiply, forward FFT, kernel-spectrum multiply,
+//                    inverse FFT, staged scatter (+ x0, DC sum) or chirp
+//                    postmultiply.
+// table kernels    : FP64 generation of stage twiddles, two-level four-step
+//                    twiddles, Bluestein chirps and Rader kernels, narrowed once.
+#include <cuda_runtime.h>
+#include <cstring>
+#include "afc_engine.cuh"
+#include "afc_internal.h"
+
+namespace afc {
+
+// ───────────────────────────── kernel arguments ─────────────────────────────
+
+template <class T> struct KArgs {
+  using C = typename CT<T>::type;
+  StageList sl;
+  const C* tw;
+  long long lanes;
+  int L, P, ld;
+  int in_op, out_op;
+  int stage_in, stage_out;
+  LaneMap im, om;          // input / output lane maps
+  const void* in;
+  void* out;
+  T scale;
+  // element-index map of index-aware operators: j = i * jmul + col(q),
+  // col(q) = (q / col_div) % col_mod.
+  long long jmul, col_div, col_mod;
+  long long nlen;          // valid length (chirp / truncation) or p (Rader)
+  long long herm_n;        // full length behind a half spectrum
+  T pair_w;                // Hermitian weight of paired bins (adjoints); 1 otherwise
+  // four-step twiddle W_N^{(col * i) mod N} = hi[m / B] * lo[m % B], conj if tw_conj
+  long long twN, twB;
+  int tw_conj;
+  const C* tw_hi;
+  const C* tw_lo;
+  const C* spec;           // pointwise spectrum
+  const C* chirp;          // Bluestein chirp (forward sign; conj if chirp_conj)
+  int chirp_conj;
+  const int* gather;       // Rader: gather[q] = g^q mod p
+  const int* scatter;      // Rader: scatter[q] = g^{-q} mod p
+};
+
+template <class T>
+__device__ __forceinline__ typename CT<T>::type gload(const KArgs<T>& a, long long base, long long col, int i) {
+  using C = typename CT<T>::type;
+  const C zero = C{(T)0, (T)0};
+  switch (a.in_op) {
+    case IN_C:
+      return static_cast<const C*>(a.in)[base + (long long)i * a.im.es];
+    case IN_R:  // real input widened (reference RealFftData, real_storage.rs:186-303)
+      return C{static_cast<const T*>(a.in)[base + (long long)i * a.im.es], (T)0};
+    case IN_HERM: {  // half spectrum (n/2+1 bins) expanded by Hermitian symmetry
+      const C* p = static_cast<const C*>(a.in);
+      const long long n = a.herm_n;
+      C v;
+      if (2LL * i <= n) {
+        v = p[base + (long long)i * a.im.es];
+      } else {
+        v = p[base + (n - i) * a.im.es];
+        v.y = -v.y;
+      }
+      if (i > 0 && 2LL * i != n) v = cscale(v, a.pair_w);
+      return v;
+    }
+    case IN_CHIRP:
+    case IN_CHIRP_R: {  // Bluestein premultiply x[j] * chirp[j], zero for j >= nlen
+      const long long j = (long long)i * a.jmul + col;
+      if (j >= a.nlen) return zero;
+      const long long off = base + (long long)i * a.im.es;
+      C x = a.in_op == IN_CHIRP ? static_cast<const C*>(a.in)[off] : C{static_cast<const T*>(a.in)[off], (T)0};
+      const C c = a.chirp[j];
+      return a.chirp_conj ? cmulc(x, c) : cmul(x, c);
+    }
+    case IN_GATHER:
+    case IN_GATHER_R: {  // Rader: x[g^i] for i < p-1, zero padding beyond
+      if (i >= a.nlen - 1) return zero;
+      const long long off = base + (long long)a.gather[i] * a.im.es;
+      return a.in_op == IN_GATHER ? static_cast<const C*>(a.in)[off] : C{static_cast<const T*>(a.in)[off], (T)0};
+    }
+  }
+  return zero;
+}
+
+template <class T>
+__device__ __forceinline__ void gstore(const KArgs<T>& a, long long base, long long col, int i,
+                                       typename CT<T>::type v, typename CT<T>::type x0) {
+  using C = typename CT<T>::type;
+  const long long off = base + (long long)i * a.om.es;
+  switch (a.out_op) {
+    case OUT_C:
+      static_cast<C*>(a.out)[off] = cscale(v, a.scale);
+      return;
+    case OUT_RE:  // real part (reference C2R: full inverse then .re)
+      static_cast<T*>(a.out)[off] = v.x * a.scale;
+      return;
+    case OUT_TRUNC: {  // keep j < nlen (half spectrum); paired bins weighted by pair_w
+      const long long j = (long long)i * a.jmul + col;
+      if (j < a.nlen) {
+        const bool paired = (j > 0) && (2 * j != a.herm_n);
+        static_cast<C*>(a.out)[off] = cscale(v, paired ? a.scale * a.pair_w : a.scale);
+      }
+      return;
+    }
+    case OUT_TW: {  // four-step: multiply by W_N^{col * i}
+      const long long m = (col * (long long)i) % a.twN;
+      const C w = cmul(a.tw_hi[m / a.twB], a.tw_lo[m % a.twB]);
+      v = a.tw_conj ? cmulc(v, w) : cmul(v, w);
+      static_cast<C*>(a.out)[off] = cscale(v, a.scale);
+      return;
+    }
+    case OUT_MUL: {  // pointwise spectrum at natural index j
+      const long long j = (long long)i * a.jmul + col;
+      static_cast<C*>(a.out)[off] = cmul(v, a.spec[j]);
+      return;
+    }
+    case OUT_CHIRP:
+    case OUT_CHIRP_RE: {  // Bluestein post-multiply, keep j < nlen
+      const long long j = (long long)i * a.jmul + col;
+      if (j < a.nlen) {
+        const C c = a.chirp[j];
+        v = cscale(a.chirp_conj ? cmulc(v, c) : cmul(v, c), a.scale);
+        if (a.out_op == OUT_CHIRP) static_cast<C*>(a.out)[off] = v;
+        else static_cast<T*>(a.out)[off] = v.x;
+      }
+      return;
+    }
+    case OUT_SCATTER:
+    case OUT_SCATTER_RE: {  // Rader: X[g^{-i}] = x0 + conv[i]
+      if (i < a.nlen - 1) {
+        const long long o2 = base + (long long)a.scatter[i] * a.om.es;
+        const C y = cscale(cadd(x0, v), a.scale);
+        if (a.out_op == OUT_SCATTER) static_cast<C*>(a.out)[o2] = y;
+        else static_cast<T*>(a.out)[o2] = y.x;
+      }
+      return;
+    }
+  }
+}
+
+// Per-thread context the engine loads from / stores to.  Direct global access
+// is plain (complex or real-widened loads, complex or real-part stores with the
+// scale); every other operator goes through the staged copies below.
+template <class T> struct Ctx {
+  using C = typename CT<T>::type;
+  const KArgs<T>& a;
+  long long ib, ob;
+  bool valid;
+  __device__ __forceinline__ C gload(int i) const {
+    if (!valid) return C{(T)0, (T)0};
+    const long long off = ib + (long long)i * a.im.es;
+    if (a.in_op == IN_R) return C{static_cast<const T*>(a.in)[off], (T)0};
+    return static_cast<const C*>(a.in)[off];
+  }
+  __device__ __forceinline__ void gstore(int i, C v) const {
+    if (!valid) return;
+    const long long off = ob + (long long)i * a.om.es;
+    if (a.out_op == OUT_RE) static_cast<T*>(a.out)[off] = v.x * a.scale;
+    else static_cast<C*>(a.out)[off] = cscale(v, a.scale);
+  }
+};
+
+template <class T> __device__ __forceinline__ long long col_of(const KArgs<T>& a, long long q) {
+  return (q / a.col_div) % a.col_mod;
+}
+
+// ─────────────────────────────── lanes kernel ───────────────────────────────
+// Shared memory: L lanes x nbuf buffers x ld elements, then 3L lane descriptors.
+
+template <class T, bool INV>
+__global__ void __launch_bounds__(512) lanes_kernel(const __grid_constant__ KArgs<T> a) {
+  using C = typename CT<T>::type;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  const int P = a.P, L = a.L, n = a.sl.n, ld = a.ld;
+  const int nbuf = engine_buffers(a.sl.nst, a.stage_in, a.stage_out);
+  long long* lb = reinterpret_cast<long long*>(sm + (long long)L * nbuf * ld);  // in base, out base, col
+  const int tid = threadIdx.x;
+  const int l = tid / P, t = tid - l * P;
+  const long long q0 = (long long)blockIdx.x * L;
+  const int lanes_here = (int)((a.lanes - q0) < L ? (a.lanes - q0) : L);
+  if (tid < L) {
+    const long long qq = q0 + tid;
+    const bool v = tid < lanes_here;
+    lb[tid] = v ? a.im.base(qq) : 0;
+    lb[L + tid] = v ? a.om.base(qq) : 0;
+    lb[2 * L + tid] = v ? col_of(a, qq) : 0;
+  }
+  C* b0 = sm + (long long)l * nbuf * ld;
+  C* b1 = b0 + (nbuf > 1 ? ld : 0);
+  __syncthreads();
+  if (a.stage_in) {
+    const int total = lanes_here * n;
+    for (int e = tid; e < total; e += blockDim.x) {
+      const int l2 = e % lanes_here, i = e / lanes_here;
+      sm[(long long)l2 * nbuf * ld + spad(i)] = gload(a, lb[l2], lb[2 * L + l2], i);
+    }
+    __syncthreads();
+  }
+  const Ctx<T> cx{a, lb[l], lb[L + l], l < lanes_here};
+  C* res = run_stages<INV>(cx, a.sl, a.tw, t, P, b0, b1, a.stage_in != 0, a.stage_out != 0);
+  if (a.stage_out) {
+    // every lane ends in the same buffer slot: offset of res within its lane block
+    const long long off = res ? (long long)(res - b0) : 0;
+    const int total = lanes_here * n;
+    const C z = C{(T)0, (T)0};
+    for (int e = tid; e < total; e += blockDim.x) {
+      const int l2 = e % lanes_here, i = e / lanes_here;
+      gstore(a, lb[L + l2], lb[2 * L + l2], i, sm[(long long)l2 * nbuf * ld + off + spad(i)], z);
+    }
+  }
+}
+
+// ──────────────────────── convolution kernel (Rader / Bluestein) ────────────────────────
+// One lane = one transform of length p (Rader) or n (Bluestein); the cyclic
+// convolution of length M = sl.n runs in shared memory (two buffers per lane):
+// staged gather / chirp premultiply, forward FFT, spectrum multiply (spec
+// carries 1/M), inverse FFT, staged scatter (+ x0, DC) / chirp postmultiply.
+
+template <class T>
+__global__ void __launch_bounds__(512) conv_kernel(const __grid_constant__ KArgs<T> a) {
+  using C = typename CT<T>::type;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  const int P = a.P, L = a.L, M = a.sl.n, ld = a.ld;
+  const int tid = threadIdx.x;
+  const int l = tid / P, t = tid - l * P;
+  const long long q0 = (long long)blockIdx.x * L;
+  const bool rader = a.in_op == IN_GATHER || a.in_op == IN_GATHER_R;
+  C* extra = sm + (long long)L * 2 * ld;                         // [2L]: x0, DC per lane
+  long long* lb = reinterpret_cast<long long*>(extra + 2 * L);   // [2L]: in base, out base
+  const int lanes_here = (int)((a.lanes - q0) < L ? (a.lanes - q0) : L);
+  if (tid < L) {
+    const long long qq = q0 + tid;
+    const bool v = tid < lanes_here;
+    lb[tid] = v ? a.im.base(qq) : 0;
+    lb[L + tid] = v ? a.om.base(qq) : 0;
+    C x0 = C{(T)0, (T)0};
+    if (v && rader) x0 = a.in_op == IN_GATHER ? static_cast<const C*>(a.in)[lb[tid]] : C{static_cast<const T*>(a.in)[lb[tid]], (T)0};
+    extra[2 * tid] = x0;
+  }
+  __syncthreads();
+  for (int e = tid; e < lanes_here * M; e += blockDim.x) {
+    const int l2 = e % lanes_here, i = e / lanes_here;
+    sm[(long long)l2 * 2 * ld + spad(i)] = gload(a, lb[l2], 0, i);
+  }
+  __syncthreads();
+  C* b0 = sm + (long long)l * 2 * ld;
+  C* b1 = b0 + ld;
+  const Ctx<T> cx{a, 0, 0, false};
+  C* res = run_stages<false>(cx, a.sl, a.tw, t, P, b0, b1, true, true);
+  const long long off = (long long)(res - b0);
+  if (tid < lanes_here) extra[2 * tid + 1] = sm[(long long)tid * 2 * ld + off];  // DC = sum of the gathered values
+  __syncthreads();
+  for (int e = tid; e < lanes_here * M; e += blockDim.x) {
+    const int l2 = e % lanes_here, i = e / lanes_here;
+    C* p = sm + (long long)l2 * 2 * ld + off + spad(i);
+    *p = cmul(*p, a.spec[i]);
+  }
+  __syncthreads();
+  // the inverse FFT starts from the buffer holding the product
+  C* res2 = off == 0 ? run_stages<true>(cx, a.sl, a.tw, t, P, b0, b1, true, true)
+                     : run_stages<true>(cx, a.sl, a.tw, t, P, b1, b0, true, true);
+  const long long off2 = (long long)(res2 - b0);
+  for (int e = tid; e < lanes_here * M; e += blockDim.x) {
+    const int l2 = e % lanes_here, i = e / lanes_here;
+    gstore(a, lb[L + l2], 0, i, sm[(long long)l2 * 2 * ld + off2 + spad(i)], extra[2 * l2]);
+  }
+  if (rader && tid < lanes_here) {
+    const C dc = cscale(cadd(extra[2 * tid], extra[2 * tid + 1]), a.scale);
+    if (a.out_op == OUT_SCATTER) static_cast<C*>(a.out)[lb[L + tid]] = dc;
+    else static_cast<T*>(a.out)[lb[L + tid]] = dc.x;
+  }
+}
+
+// ────────────────────────────── table kernels ──────────────────────────────
+
+// Stage twiddles: tw[off + k(R-1) + r-1] = exp(-2 pi i (r k mod NsR) / (NsR)).
+template <class T>
+__global__ void gen_stage_twiddles(typename CT<T>::type* tw, StageList sl) {
+  using C = typename CT<T>::type;
+  for (int s = 0; s < sl.nst; ++s) {
+    const int R = sl.st[s].R, Ns = sl.st[s].Ns, off = sl.st[s].twoff;
+    if (Ns <= 1) continue;
+    const long long cnt = (long long)Ns * (R - 1);
+    const long long Lr = (long long)Ns * R;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < cnt; e += (long long)gridDim.x * blockDim.x) {
+      const long long k = e / (R - 1), r = e % (R - 1) + 1;
+      const long long m = (r * k) % Lr;
+      double sn, cs;
+      sincospi(-2.0 * (double)m / (double)Lr, &sn, &cs);
+      tw[off + e] = C{(T)cs, (T)sn};
+    }
+  }
+}
+
+// out[j] = exp(-2 pi i (j * mult mod N) / N) for j < cnt.
+template <class T>
+__global__ void gen_roots(typename CT<T>::type* out, long long cnt, long long mult, long long N) {
+  using C = typename CT<T>::type;
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < cnt; j += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long m = (unsigned long long)(((__int128)j * mult) % N);
+    double sn, cs;
+    sincospi(-2.0 * (double)m / (double)N, &sn, &cs);
+    out[j] = C{(T)cs, (T)sn};
+  }
+}
+
+// Bluestein chirp, forward sign: c[j] = exp(-i pi (j^2 mod 2n) / n); the phase
+// is reduced in exact 64-bit integer arithmetic before the FP64 sincospi.
+template <class T>
+__global__ void gen_chirp(typename CT<T>::type* out, long long n) {
+  using C = typename CT<T>::type;
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long m = (unsigned long long)(((__int128)j * j) % (2 * n));
+    double sn, cs;
+    sincospi(-(double)m / (double)n, &sn, &cs);
+    out[j] = C{(T)cs, (T)sn};
+  }
+}
+
+// Bluestein convolution kernel (length M): b[m] = conj(c_dir[|m|]) for |m| < n
+// placed cyclically, c_dir = c (forward) or conj(c) (inverse); scaled by 1/M.
+template <class T>
+__global__ void gen_bluestein_b(typename CT<T>::type* b, const typename CT<T>::type* chirp, long long n, long long M,
+                                int inverse) {
+  using C = typename CT<T>::type;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M; i += (long long)gridDim.x * blockDim.x) {
+    long long m = -1;
+    if (i < n) m = i;
+    else if (i > M - n) m = M - i;
+    C v = C{(T)0, (T)0};
+    if (m >= 0) {
+      const C c = chirp[m];
+      v = inverse ? c : C{c.x, -c.y};
+      v = cscale(v, (T)(1.0 / (double)M));
+    }
+    b[i] = v;
+  }
+}
+
+// Rader kernel b[q] = exp(sign 2 pi i (g^{-q} mod p) / p), q < p-1 (scalar/rader.rs:3-19
+// of the reference builds the same sequence); the length-(p-1) cyclic kernel is
+// embedded in M >= 2(p-1)-1 when M != p-1.  Scaled by 1/M.
+template <class T>
+__global__ void gen_rader_b(typename CT<T>::type* b, const int* scatter, long long p, long long M, int inverse) {
+  using C = typename CT<T>::type;
+  const long long L = p - 1;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M; i += (long long)gridDim.x * blockDim.x) {
+    long long qq = -1;
+    if (M == L || i < L) qq = i;
+    else if (i > M - L) qq = L - (M - i);
+    C v = C{(T)0, (T)0};
+    if (qq >= 0) {
+      double sn, cs;
+      sincospi((inverse ? 2.0 : -2.0) * (double)scatter[qq] / (double)p, &sn, &cs);
+      v = C{(T)(cs / (double)M), (T)(sn / (double)M)};
+    }
+    b[i] = v;
+  }
+}
+
+// ─────────────────────────────── launchers ────────────────────────────────
+
+template <class T> static KArgs<T> to_kargs(const LaunchDesc& d) {
+  using C = typename CT<T>::type;
+  KArgs<T> a;
+  memset(&a, 0, sizeof(a));
+  a.sl = d.sl;
+  a.tw = static_cast<const C*>(d.tw);
+  a.lanes = d.lanes;
+  a.L = d.L;
+  a.P = d.P;
+  a.ld = d.ld;
+  a.in_op = d.in_op;
+  a.out_op = d.out_op;
+  a.stage_in = d.stage_in;
+  a.stage_out = d.stage_out;
+  a.im = d.im;
+  a.om = d.om;
+  a.in = d.in;
+  a.out = d.out;
+  a.scale = (T)d.scale;
+  a.jmul = d.jmul ? d.jmul : 1;
+  a.col_div = d.col_div ? d.col_div : 1;
+  a.col_mod = d.col_mod ? d.col_mod : 1;
+  a.nlen = d.nlen;
+  a.herm_n = d.herm_n;
+  a.pair_w = (T)d.pair_w;
+  a.twN = d.twN ? d.twN : 1;
+  a.twB = d.twB ? d.twB : 1;
+  a.tw_conj = d.tw_conj;
+  a.tw_hi = static_cast<const C*>(d.tw_hi);
+  a.tw_lo = static_cast<const C*>(d.tw_lo);
+  a.spec = static_cast<const C*>(d.spec);
+  a.chirp = static_cast<const C*>(d.chirp);
+  a.chirp_conj = d.chirp_conj;
+  a.gather = d.gather;
+  a.scatter = d.scatter;
+  return a;
+}
+
+template <class K> static cudaError_t prep_smem(K kern, size_t smem) {
+  if (smem > 48 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return cudaSuccess;
+}
+
+template <class T, bool INV> static cudaError_t launch_lanes_t(const LaunchDesc& d, cudaStream_t st) {
+  auto k = lanes_kernel<T, INV>;
+  const size_t smem = lanes_smem_bytes(d, sizeof(typename CT<T>::type));
+  cudaError_t e = prep_smem(k, smem);
+  if (e != cudaSuccess) return e;
+  const long long grid = (d.lanes + d.L - 1) / d.L;
+  k<<<(unsigned)grid, d.L * d.P, smem, st>>>(to_kargs<T>(d));
+  count_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lanes(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st) {
+  if (d.lanes <= 0) return cudaSuccess;
+  if (dbl) return inv ? launch_lanes_t<double, true>(d, st) : launch_lanes_t<double, false>(d, st);
+  return inv ? launch_lanes_t<float, true>(d, st) : launch_lanes_t<float, false>(d, st);
+}
+
+template <class T> static cudaError_t launch_conv_t(const LaunchDesc& d, cudaStream_t st) {
+  auto k = conv_kernel<T>;
+  const size_t smem = conv_smem_bytes(d, sizeof(typename CT<T>::type));
+  cudaError_t e = prep_smem(k, smem);
+  if (e != cudaSuccess) return e;
+  const long long grid = (d.lanes + d.L - 1) / d.L;
+  k<<<(unsigned)grid, d.L * d.P, smem, st>>>(to_kargs<T>(d));
+  count_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_conv(const LaunchDesc& d, bool dbl, cudaStream_t st) {
+  if (d.lanes <= 0) return cudaSuccess;
+  return dbl ? launch_conv_t<double>(d, st) : launch_conv_t<float>(d, st);
+}
+
+static unsigned table_grid(long long n) {
+  long long g = (n + 255) / 256;
+  if (g < 1) g = 1;
+  if (g > 4096) g = 4096;
+  return (unsigned)g;
+}
+
+cudaError_t gen_stage_twiddles_dev(void* tw, const StageList& sl, bool dbl, cudaStream_t st) {
+  if (dbl) gen_stage_twiddles<double><<<table_grid(sl.n), 256, 0, st>>>(static_cast<double2*>(tw), sl);
+  else gen_stage_twiddles<float><<<table_grid(sl.n), 256, 0, st>>>(static_cast<float2*>(tw), sl);
+  count_launch(1);
+  return cudaGetLastError();
+}
+cudaError_t gen_roots_dev(void* out, long long cnt, long long mult, long long N, bool dbl, cudaStream_t st) {
+  if (dbl) gen_roots<double><<<table_grid(cnt), 256, 0, st>>>(static_cast<double2*>(out), cnt, mult, N);
+  else gen_roots<float><<<table_grid(cnt), 256, 0, st>>>(static_cast<float2*>(out), cnt, mult, N);
+  count_launch(1);
+  return cudaGetLastError();
+}
+cudaError_t gen_chirp_dev(void* out, long long n, bool dbl, cudaStream_t st) {
+  if (dbl) gen_chirp<double><<<table_grid(n), 256, 0, st>>>(static_cast<double2*>(out), n);
+  else gen_chirp<float><<<table_grid(n), 256, 0, st>>>(static_cast<float2*>(out), n);
+  count_launch(1);
+  return cudaGetLastError();
+}
+cudaError_t gen_bluestein_b_dev(void* b, const void* chirp, long long n, long long M, bool inverse, bool dbl,
+                                cudaStream_t st) {
+  if (dbl)
+    gen_bluestein_b<double><<<table_grid(M), 256, 0, st>>>(static_cast<double2*>(b), static_cast<const double2*>(chirp), n, M, inverse);
+  else
+    gen_bluestein_b<float><<<table_grid(M), 256, 0, st>>>(static_cast<float2*>(b), static_cast<const float2*>(chirp), n, M, inverse);
+  count_launch(1);
+  return cudaGetLastError();
+}
+cudaError_t gen_rader_b_dev(void* b, const int* scatter, long long p, long long M, bool inverse, bool dbl,
+                            cudaStream_t st) {
+  if (dbl) gen_rader_b<double><<<table_grid(M), 256, 0, st>>>(static_cast<double2*>(b), scatter, p, M, inverse);
+  else gen_rader_b<float><<<table_grid(M), 256, 0, st>>>(static_cast<float2*>(b), scatter, p, M, inverse);
+  count_launch(1);
+  return cudaGetLastError();
+}
+
+}  // namespace afc

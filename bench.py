@@ -1,0 +1,355 @@
+"""Benchmark: 3D complex-to-complex FFT, forward then inverse (1/N), on B200.
+
+Workload (the headline): 256 x 256 x 256 complex128 (f64 high_accuracy plan),
+entries i.i.d. standard normal re/im from a seed, forward then normalized
+inverse per step.  The other shapes/dtypes of the same configuration
+(243x250x343, complex64) are measured in the same run and reported under
+"also".  Inputs (268 MB) exceed the 126 MB L2, so no flush is needed between
+steps.
+
+value        : whole-job GFLOP/s, 5 N log2 N per transform, two transforms per step,
+               data already in HBM, CUDA events on the launching stream.
+e2e          : the same metric through afc_execute_host (the reference-facing slice
+               API) from pinned host buffers, copies inside the timed region.
+roofline     : the dominant kernel (lanes_kernel, every launch of the step): bytes a
+               launch moves algorithmically (read + write of the volume it
+               transforms) / its average duration, against MEASURED_PEAKS.json.
+cpu_baseline : the oracle's restatement of the reference CPU plan (FftPlan3D<f64>),
+               all host threads, one forward+inverse of the same volume.
+
+--impl reference times that CPU path alone on the same config.
+Multi-GPU: replicas only (one transform per rank, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE = (256, 256, 256)
+ALSO = [((243, 250, 343), "f64"), ((256, 256, 256), "f32"), ((243, 250, 343), "f32")]
+METRIC = "FFT GFLOP/s (5N log2N) and % HBM roofline vs plain FP32, at stated FP64-oracle error"
+
+
+def flops_per_transform(shape):
+    n = int(np.prod(shape))
+    return 5.0 * n * math.log2(n)
+
+
+def bytes_per_transform(shape, prec):
+    return 2.0 * int(np.prod(shape)) * (16 if prec == "f64" else 8)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl" if os.environ.get("AFC_BENCH_BACKEND", "nccl") == "nccl" else "gloo",
+                                timeout=timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(v: float, world: int, device) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_transform_gflops(shape, reps, threads=0, want_output=False):
+    """Oracle FftPlan3D<f64> forward + inverse on host cores; returns GFLOP/s."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    O.fft3d(np.zeros((4, 4, 4), dtype=np.complex128))  # load + warm caches
+    t0 = time.perf_counter()
+    y = None
+    for _ in range(reps):
+        y = O.fft3d(x, threads=threads)
+        O.fft3d(y, inverse=True, threads=threads)
+    dt = time.perf_counter() - t0
+    g = reps * 2 * flops_per_transform(shape) / dt / 1e9
+    return (g, dt, x, y) if want_output else (g, dt)
+
+
+def run_reference(args):
+    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    threads = O.max_threads()
+    vals = []
+    for _ in range(args.warmup):
+        cpu_transform_gflops(SHAPE, 1)
+    for _ in range(args.steps):
+        g, _ = cpu_transform_gflops(SHAPE, 1)
+        vals.append(g)
+    v = float(np.mean(vals))
+    step_s = 2 * flops_per_transform(SHAPE) / (v * 1e9)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "GFLOP/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_s * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1) re/im)",
+        "config": {"workload": "3D C2C 256x256x256 complex128 forward+inverse (1/N)", "shape": list(SHAPE),
+                   "precision": "f64 high_accuracy", "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": round(v, 3), "unit": "GFLOP/s", "cores": threads, "kind": "port",
+                         "sample": "one forward+inverse of the 256^3 complex128 volume per step (oracle FftPlan3D<f64>)"},
+        "e2e": {"value": round(v, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def time_device(plan, x, y, steps, warmup, torch):
+    """fwd (x->y) + inv (y->x) per step; returns seconds per step (CUDA events)."""
+    for _ in range(warmup):
+        plan.execute(x, out=y)
+        plan.execute(y, out=x, inverse=True)
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        plan.execute(x, out=y)
+        plan.execute(y, out=x, inverse=True)
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / steps
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import apollofft_b200 as afc
+
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    hbm_peak, peak_kind = load_peaks()
+
+    g = torch.Generator(device=dev).manual_seed(2 + rank)
+    x = torch.randn(SHAPE, dtype=torch.complex128, device=dev, generator=g)
+    x0 = x.clone()
+    y = torch.empty_like(x)
+    plan = afc.CudaPlan(list(SHAPE), precision="f64", device=local)
+    launches_per_transform = len(SHAPE)
+
+    barrier(world)
+    torch.cuda.synchronize()
+    n0 = afc.kernel_launch_count()
+    with ClockSampler(local) as clk:
+        for _ in range(args.warmup):
+            plan.execute(x, out=y)
+            plan.execute(y, out=x, inverse=True)
+        torch.cuda.synchronize()
+        barrier(world)
+        n1 = afc.kernel_launch_count()
+        st = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            plan.execute(x, out=y)
+            plan.execute(y, out=x, inverse=True)
+        e1.record(st)
+        torch.cuda.synchronize()
+        t_step = e0.elapsed_time(e1) / 1e3 / args.steps
+        n2 = afc.kernel_launch_count()
+    t_step_max = max_over_ranks(t_step, world, dev)
+    launches = n2 - n1
+    roundtrip_err = (torch.linalg.vector_norm(x - x0) / torch.linalg.vector_norm(x0)).item()
+
+    flops_step = 2 * flops_per_transform(SHAPE)
+    value = world * flops_step / t_step_max / 1e9
+    vol_bytes = bytes_per_transform(SHAPE, "f64")  # read + write of the volume
+    launches_per_step = 2 * launches_per_transform
+    t_launch = t_step / launches_per_step
+    achieved = vol_bytes / t_launch / 1e9
+    transform_frac = (2 * vol_bytes / t_step / 1e9) / hbm_peak
+
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "lanes_kernel_traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get("bytes_per_launch_256cube_f64")
+        except (ValueError, OSError):
+            traffic = None
+
+    # other shapes / dtypes of the configuration
+    also = []
+    del y
+    for shp, prec in ALSO:
+        dt = torch.complex128 if prec == "f64" else torch.complex64
+        xa = torch.randn(shp, dtype=dt, device=dev, generator=g)
+        ya = torch.empty_like(xa)
+        pa = afc.CudaPlan(list(shp), precision=prec, device=local)
+        ts = time_device(pa, xa, ya, max(3, args.steps // 2), args.warmup, torch)
+        err = None
+        if prec == "f32":
+            ref = afc.CudaPlan(list(shp), precision="f64", device=local).execute(xa.to(torch.complex128))
+            out = pa.execute(xa)
+            err = (torch.linalg.vector_norm(out.to(torch.complex128) - ref) / torch.linalg.vector_norm(ref)).item()
+            del ref, out
+        also.append({"shape": list(shp), "precision": prec, "ms_per_step": round(ts * 1e3, 4),
+                     "gflops": round(2 * flops_per_transform(shp) / ts / 1e9, 2),
+                     "transform_hbm_frac": round((2 * bytes_per_transform(shp, prec) / ts / 1e9) / hbm_peak, 4),
+                     "rel_l2_vs_f64_path": err})
+        del xa, ya, pa
+        torch.cuda.empty_cache()
+
+    # end to end through the host-pointer C-ABI call, pinned buffers
+    hx = torch.randn(SHAPE, dtype=torch.complex128, generator=torch.Generator().manual_seed(2)).pin_memory()
+    hy = torch.empty_like(hx).pin_memory()
+    hz = torch.empty_like(hx).pin_memory()
+    xn, yn, zn = hx.numpy(), hy.numpy(), hz.numpy()
+    import ctypes
+    L = afc._lib.lib()
+    for _ in range(2):
+        afc._lib.check(L.afc_execute_host(plan._h, xn.ctypes.data, yn.ctypes.data, 0))
+        afc._lib.check(L.afc_execute_host(plan._h, yn.ctypes.data, zn.ctypes.data, 1))
+    e2e_steps = max(3, args.steps // 4)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        afc._lib.check(L.afc_execute_host(plan._h, xn.ctypes.data, yn.ctypes.data, 0))
+        afc._lib.check(L.afc_execute_host(plan._h, yn.ctypes.data, zn.ctypes.data, 1))
+    t_e2e = (time.perf_counter() - t0) / e2e_steps
+    t_e2e = max_over_ranks(t_e2e, world, dev)
+    e2e_val = world * flops_step / t_e2e / 1e9
+
+    # CPU baseline (rank 0, N = 1 only) and the error against the f64 oracle
+    cpu = None
+    err_oracle = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        gcpu, dt, xin, yref = cpu_transform_gflops(SHAPE, 1, want_output=True)
+        cpu = {"value": round(gcpu, 3), "unit": "GFLOP/s", "cores": O.max_threads(), "kind": "port",
+               "sample": "one forward+inverse of the 256^3 complex128 volume (oracle FftPlan3D<f64>, all threads)"}
+        xt = torch.from_numpy(xin).to(dev)
+        yt = plan.execute(xt).cpu().numpy()
+        err_oracle = float(np.linalg.norm(yt - yref) / np.linalg.norm(yref))
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(t_step_max * 1e3, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1) re/im)",
+            "config": {"workload": "3D C2C 256x256x256 complex128 forward+inverse (1/N)", "shape": list(SHAPE),
+                       "precision": "f64 high_accuracy", "parallelism": f"replicas x{world}",
+                       "l2": "inputs (268 MB) larger than L2; no flush"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                         "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
+                         "kernel": "lanes_kernel<double> (all launches of the step)",
+                         "peak_source": peak_kind},
+            "transform_hbm_frac": round(transform_frac, 4),
+            "error_vs_oracle_rel_l2": err_oracle,
+            "roundtrip_rel_l2": roundtrip_err,
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_val, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": int(2 * 16 * np.prod(SHAPE)),
+                    "d2h_bytes_per_step": int(2 * 16 * np.prod(SHAPE))},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "also": also,
+        }
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

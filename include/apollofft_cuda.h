@@ -1,0 +1,193 @@
+/* apollofft_cuda.h -- C ABI of apollofft_b200, the B200 (sm_100a) backend for
+ * apollo-fft's dense FFT plan execution.
+ *
+ * Plain C types only: pointers, sizes, enums.  A Rust crate binds these with an
+ * `extern "C"` block; Python binds them with ctypes (apollofft_b200/_lib.py).
+ *
+ * Conventions (crates/apollo-fft/src/domain/metadata/precision.rs:15-19,
+ * Normalization::FftwCompatible): forward is unnormalized, inverse is scaled by
+ * 1/N (N = product of the transform dims).  Data are C-order, interleaved
+ * (re, im), with `batch` transforms back to back.  Every call returns an
+ * afc_status; nothing aborts.  Kernels run asynchronously on the caller's
+ * stream; only the *_host variants and plan creation synchronize.
+ */
+#ifndef APOLLOFFT_CUDA_H
+#define APOLLOFFT_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define AFC_API __attribute__((visibility("default")))
+#else
+#define AFC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces ApolloError (crates/apollo-fft/src/domain/contracts/error.rs:10-47):
+ * Validation, ShapeMismatch, NonContiguous, BackendUnavailable, plus device,
+ * memory and timeout conditions the CPU backend does not have. */
+typedef enum {
+  AFC_OK = 0,
+  AFC_ERR_VALIDATION = 1,
+  AFC_ERR_SHAPE_MISMATCH = 2,
+  AFC_ERR_NON_CONTIGUOUS = 3,
+  AFC_ERR_BACKEND_UNAVAILABLE = 4,
+  AFC_ERR_DEVICE = 5,
+  AFC_ERR_OUT_OF_MEMORY = 6,
+  AFC_ERR_TIMEOUT = 7,
+  AFC_ERR_UNSUPPORTED = 8
+} afc_status;
+
+/* Precision profiles (precision.rs:55-85): F64 = HIGH_ACCURACY_F64 (the
+ * `high_accuracy` plan), F32 = LOW_PRECISION_F32 (`low_precision`).  The two
+ * tensor-core forms compute radix-16 stages as split-precision DFT-matrix
+ * products with FP32 accumulation on complex64 data. */
+typedef enum {
+  AFC_PREC_F32 = 0,
+  AFC_PREC_F64 = 1,
+  AFC_PREC_TC_BF16_SPLIT = 2,
+  AFC_PREC_TC_FP16_SPLIT = 3
+} afc_precision;
+
+/* C2C: complex -> complex.
+ * R2C_FULL: the reference's "R2C": real input widened to complex, full C2C,
+ *   output of the same shape (plan/fft/real_storage.rs:186-303); its inverse is
+ *   a full C2C inverse followed by taking the real part ("C2R").
+ * R2C_HALF: Hermitian half spectrum, last dim n -> n/2 + 1 (new explicit API;
+ *   the reference models HalfSpectrum3D in domain/metadata/shape.rs:79-95 but
+ *   never wires it). */
+typedef enum { AFC_KIND_C2C = 0, AFC_KIND_R2C_FULL = 1, AFC_KIND_R2C_HALF = 2 } afc_kind;
+
+typedef enum { AFC_FORWARD = 0, AFC_INVERSE = 1 } afc_direction;
+
+typedef struct afc_plan_s* afc_plan;
+
+/* Mirrors BackendCapabilities (domain/contracts/backend.rs:9-29). */
+typedef struct {
+  int kind; /* 2 = CUDA (the reference has Cpu = 0, Wgpu = 1) */
+  int normalization; /* 0 = FftwCompatible */
+  int supports_1d, supports_2d, supports_3d;
+  int supports_real_to_complex;
+  int supports_mixed_precision;
+  int default_precision; /* afc_precision */
+  int device_count;
+  int sm_count;
+  int cc_major, cc_minor;
+  size_t max_smem_per_block;
+} afc_capabilities_t;
+
+/* Reference dispatch decision for one length (mixed_radix/dispatch.rs:26-132),
+ * reported bit-exactly from this library's own integer layer. */
+typedef struct {
+  int strategy;          /* 0 noop, 1 stockham, 2 four_step, 3 winograd, 4 pfa_static,
+                            5 composite, 6 pfa_generic, 7 rader_full, 8 rader_half,
+                            9 untransformed (prime power the reference leaves as is) */
+  int n_radices;         /* lowered prime23 radices (radix_shape.rs:60-234), -1 if None */
+  uint64_t radices[64];
+  uint64_t coprime_n1, coprime_n2; /* radix_shape.rs:192-219, 0 if None */
+  uint64_t four_step_n1, four_step_n2; /* four_step/mod.rs:66-70, 0 unless pow2 */
+  uint64_t primitive_root, primitive_root_inv; /* rader/generator.rs:18-120, 0 unless prime */
+  int is_prime;
+  int is_short_winograd;
+  int has_static_coprime_codelet;
+  /* GPU execution chosen by this library for the length */
+  int gpu_algo;          /* 0 smem Stockham, 1 four-step, 2 Rader, 3 Bluestein, 4 noop */
+  int gpu_n_radices;
+  int gpu_radices[24];
+  uint64_t gpu_conv_len; /* convolution length for Rader/Bluestein */
+  uint64_t gpu_split_n1, gpu_split_n2;
+} afc_length_info_t;
+
+/* ── plans (FftPlan1D/2D/3D::new, plan/fft/dimension_{1,2,3}d.rs) ──────────── */
+
+/* Replaces FftPlan1D/2D/3D::new (dimension_1d.rs:24-41, dimension_2d.rs:77-100,
+ * dimension_3d.rs:92-123) and Shape{1,2,3}D::new validation (shape.rs:14-56):
+ * rank 1..3, dims[0..rank) > 0, batch >= 1.  Twiddle, Rader and Bluestein
+ * tables are generated on `device` and stay resident with the plan. */
+AFC_API afc_status afc_plan_create(afc_plan* out, int rank, const int64_t* dims, afc_precision precision,
+                           afc_kind kind, int64_t batch, int device);
+
+/* Replaces PlanCacheProvider::get_{1,2,3}d_plan (orchestration/cache/plans.rs:15-231):
+ * a process-wide, mutex-guarded, reference-counted cache keyed by
+ * (rank, dims, precision, kind, batch, device).  Release with afc_plan_destroy. */
+AFC_API afc_status afc_plan_get_cached(afc_plan* out, int rank, const int64_t* dims, afc_precision precision,
+                               afc_kind kind, int64_t batch, int device);
+
+/* Drops one reference; frees device tables when the last one goes. */
+AFC_API afc_status afc_plan_destroy(afc_plan plan);
+
+/* Replaces forward_complex_inplace / inverse_complex_inplace and their slice
+ * forms (dimension_1d.rs:55-82, dimension_2d.rs:102-122, dimension_3d.rs:148-169).
+ * Device pointers; in == out runs in place (C2C only).  Input element counts:
+ * C2C batch*N complex; R2C_FULL forward batch*N real -> batch*N complex,
+ * inverse batch*N complex -> batch*N real; R2C_HALF forward batch*N real ->
+ * batch*N/n_last*(n_last/2+1) complex, inverse the reverse. */
+AFC_API afc_status afc_execute(afc_plan plan, const void* in, void* out, afc_direction direction, void* stream);
+
+/* Same with an explicit overall scale in place of the convention (1 forward,
+ * 1/N inverse). */
+AFC_API afc_status afc_execute_scaled(afc_plan plan, const void* in, void* out, afc_direction direction,
+                              double scale, void* stream);
+
+/* Adjoint (conjugate transpose, real inner product for real spaces) of the
+ * linear map afc_execute(plan, ., ., direction): the backward pass of an
+ * autograd function.  C2C forward -> unnormalized inverse; C2C inverse -> forward
+ * times 1/N; R2C_FULL forward -> real part of the unnormalized inverse;
+ * R2C_HALF adds the Hermitian weights (1/2 on bins 1..ceil(n/2)-1 going back,
+ * 2 going forward).  No reference counterpart (the reference has no autograd). */
+AFC_API afc_status afc_execute_adjoint(afc_plan plan, const void* in, void* out, afc_direction direction,
+                               void* stream);
+
+/* Host-pointer convenience form (mirrors the slice API callers such as
+ * apollo-nufft/stft/czt use): copies host -> device, executes, copies back,
+ * synchronizes.  Uses plan-owned staging buffers. */
+AFC_API afc_status afc_execute_host(afc_plan plan, const void* host_in, void* host_out, afc_direction direction);
+
+/* Workspace the plan needs for one execution on one stream, in bytes (0 if
+ * none).  afc_execute uses a plan-owned workspace guarded by a mutex;
+ * afc_execute_ws takes a caller-owned one so concurrent streams can share a plan. */
+AFC_API afc_status afc_workspace_size(afc_plan plan, size_t* bytes);
+AFC_API afc_status afc_execute_ws(afc_plan plan, const void* in, void* out, afc_direction direction, double scale,
+                          int use_scale, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Element counts of one execution's input and output (complex or real elements). */
+AFC_API afc_status afc_plan_io_elems(afc_plan plan, afc_direction direction, int64_t* in_elems, int64_t* out_elems);
+
+/* ── uneven batches (new: many lengths in one persistent launch) ─────────── */
+
+typedef struct afc_batch_plan_s* afc_batch_plan;
+
+/* Lanes of lengths[i] packed back to back (offset = prefix sum).  Precision
+ * F32 or F64.  Each length gets an autotuned configuration from the plan cache. */
+AFC_API afc_status afc_batch_plan_create(afc_batch_plan* out, const int64_t* lengths, int64_t count,
+                                 afc_precision precision, int device);
+AFC_API afc_status afc_batch_plan_destroy(afc_batch_plan plan);
+/* mode 0: one persistent launch per phase (captured into a CUDA graph on the
+ * first call per stream), mode 1: one plain launch per distinct length. */
+AFC_API afc_status afc_batch_execute(afc_batch_plan plan, const void* in, void* out, afc_direction direction,
+                             int mode, void* stream);
+AFC_API afc_status afc_batch_total_elems(afc_batch_plan plan, int64_t* elems);
+
+/* ── introspection / integer layer ───────────────────────────────────────── */
+
+AFC_API afc_status afc_capabilities(afc_capabilities_t* caps);
+AFC_API afc_status afc_length_info(uint64_t n, afc_length_info_t* info);
+/* Rader maps (rader/mod.rs:215-246): gather[q] = g^q mod p, scatter[q] = g^{-q} mod p. */
+AFC_API afc_status afc_rader_maps(uint64_t p, uint64_t* gather, uint64_t* scatter);
+/* Good-Thomas CRT permutations (mixed_radix/caches/misc.rs:233-256). */
+AFC_API afc_status afc_pfa_perm(uint64_t n1, uint64_t n2, uint64_t* in_perm, uint64_t* out_perm);
+AFC_API afc_status afc_plan_describe(afc_plan plan, int axis, afc_length_info_t* info);
+/* Thread-local message of the last failing call on this thread. */
+AFC_API const char* afc_last_error_message(void);
+/* Number of kernels this library launched in this process (all devices). */
+AFC_API uint64_t afc_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* APOLLOFFT_CUDA_H */

@@ -1,0 +1,75 @@
+"""The C ABI library loads, exports every symbol the header declares and
+validates arguments without a GPU (no compute calls here)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "apollofft_cuda.h")).read()
+    return sorted(set(re.findall(r"^AFC_API [^(]*?\b(afc_\w+)\(", txt, flags=re.M)))
+
+
+def test_header_declares_expected_entry_points():
+    syms = header_symbols()
+    for s in ("afc_plan_create", "afc_plan_get_cached", "afc_plan_destroy", "afc_execute", "afc_execute_adjoint",
+              "afc_execute_host", "afc_batch_plan_create", "afc_batch_execute", "afc_length_info"):
+        assert s in syms
+
+
+def test_library_exports_every_header_symbol(afc):
+    lib = ctypes.CDLL(afc._lib.LIB_PATH)
+    for s in header_symbols():
+        assert hasattr(lib, s), s
+
+
+def test_python_signatures_cover_header():
+    from apollofft_b200 import _lib
+    assert set(header_symbols()) == set(_lib.SIGNATURES)
+
+
+def _create(afc, rank, dims, prec=1, kind=0, batch=1, device=0):
+    h = ctypes.c_void_p()
+    arr = (ctypes.c_int64 * max(len(dims), 1))(*dims)
+    st = afc._lib.lib().afc_plan_create(ctypes.byref(h), rank, arr, prec, kind, batch, device)
+    return st, h
+
+
+def test_validation_errors(afc):
+    L = afc._lib
+    st, _ = _create(afc, 3, [4, 0, 4])
+    assert st == L.AFC_ERR_VALIDATION
+    assert "ny" in L.last_error() and "must be > 0" in L.last_error()
+    st, _ = _create(afc, 4, [1, 1, 1, 1])
+    assert st == L.AFC_ERR_VALIDATION
+    st, _ = _create(afc, 1, [8], batch=0)
+    assert st == L.AFC_ERR_VALIDATION
+    st, _ = _create(afc, 1, [8], prec=7)
+    assert st == L.AFC_ERR_UNSUPPORTED
+    assert afc._lib.lib().afc_execute(None, None, None, 0, None) == L.AFC_ERR_VALIDATION
+
+
+def test_no_device_is_backend_unavailable(afc):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    st, _ = _create(afc, 1, [8])
+    assert st == afc._lib.AFC_ERR_BACKEND_UNAVAILABLE
+
+
+def test_python_api_validation_messages(afc):
+    import numpy as np
+    with pytest.raises(ValueError, match="C-contiguous"):
+        afc.fft1(np.linspace(0.0, 1.0, 16)[::2])
+    with pytest.raises(ValueError, match="expects float64/complex128 storage"):
+        afc.fft1(np.arange(8, dtype=np.float32))
+    with pytest.raises(ValueError, match="expects float32/complex64 storage"):
+        afc.fft1(np.linspace(0.0, 1.0, 8), precision="low_precision")
+    with pytest.raises(ValueError, match="inconsistent"):
+        afc.irfft3(np.ones((2, 2, 3), dtype=np.complex128), 4)
+    with pytest.raises(ValueError, match="unsupported precision"):
+        afc.fft1(np.zeros(4), precision="bogus")

@@ -1,0 +1,168 @@
+"""CUDA kernels vs the f64 oracle (the reference's high_accuracy plan restated).
+
+Bars (stated in the north star): f64 relative L2 <= 1e-12, f32 <= 1e-5 against
+the f64 oracle on the same seeded inputs.  Integer maps are checked bit-exactly
+in test_oracle_integer.py."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+TOL = {"f64": 1e-12, "f32": 1e-5}
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden.npz"))
+
+
+def run(afc, x, dims, prec, kind="c2c", inverse=False, batch=1, inplace=False, scale=None):
+    p = afc.CudaPlan(dims, precision=prec, kind=kind, batch=batch)
+    t = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    out = t if inplace else None
+    y = p.execute(t, out=out, inverse=inverse, scale=scale)
+    torch.cuda.synchronize()
+    return y.cpu().numpy()
+
+
+def cplx(rng, shape, dtype=np.complex128):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(dtype)
+
+
+LENGTHS_1D = [1, 2, 3, 4, 5, 7, 8, 11, 13, 16, 17, 23, 31, 32, 45, 60, 64, 81, 97, 100, 128, 192, 243, 250, 256, 343,
+              361, 512, 1000, 1009, 1024, 1031, 2048, 2053, 4096, 4099, 6561, 8192, 10007, 16384, 65536, 65521,
+              1 << 18]
+
+
+@pytest.mark.parametrize("n", LENGTHS_1D)
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_c2c_1d_vs_oracle(afc, oracle, cuda, n, prec):
+    rng = np.random.default_rng(n)
+    batch = 3 if n < 100000 else 1
+    x = cplx(rng, (batch, n))
+    if oracle.dispatch_strategy(n) == "untransformed":
+        ref = np.fft.fft(x, axis=-1)  # the reference leaves p^k (p > 23) untransformed
+    else:
+        ref = oracle.fft1d(x)
+    dt = np.complex128 if prec == "f64" else np.complex64
+    y = run(afc, x.astype(dt), [n], prec, batch=batch).reshape(batch, n)
+    assert rel_l2(y, ref) < TOL[prec], (n, rel_l2(y, ref))
+    yi = run(afc, ref.astype(dt), [n], prec, inverse=True, batch=batch).reshape(batch, n)
+    assert rel_l2(yi, x) < TOL[prec]
+
+
+@pytest.mark.parametrize("n", [256, 4096, 243, 1009, 4099])
+def test_c2c_1d_inplace(afc, oracle, cuda, n):
+    rng = np.random.default_rng(n + 1)
+    x = cplx(rng, (2, n))
+    y = run(afc, x, [n], "f64", batch=2, inplace=True).reshape(2, n)
+    assert rel_l2(y, oracle.fft1d(x)) < 1e-12
+
+
+@pytest.mark.parametrize("shape", [(8, 16, 32), (9, 10, 7), (4, 1, 6), (1, 1, 5), (16, 243, 2), (3, 5, 1031)])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_c2c_3d_vs_oracle(afc, oracle, cuda, shape, prec):
+    rng = np.random.default_rng(sum(shape))
+    x = cplx(rng, shape)
+    ref = oracle.fft3d(x)
+    dt = np.complex128 if prec == "f64" else np.complex64
+    y = run(afc, x.astype(dt), list(shape), prec).reshape(shape)
+    assert rel_l2(y, ref) < TOL[prec]
+    yi = run(afc, ref.astype(dt), list(shape), prec, inverse=True).reshape(shape)
+    assert rel_l2(yi, x) < TOL[prec]
+
+
+@pytest.mark.parametrize("shape", [(48, 30), (2048, 64), (7, 1009)])
+def test_c2c_2d_vs_oracle(afc, oracle, cuda, shape):
+    rng = np.random.default_rng(3)
+    x = cplx(rng, (2,) + shape)
+    y = run(afc, x, list(shape), "f64", batch=2).reshape(x.shape)
+    assert rel_l2(y, oracle.fft2d(x)) < 1e-12
+
+
+def test_golden_fixtures(afc, cuda):
+    g = GOLD
+    y = run(afc, g["c1_x"], [4096], "f64", batch=2).reshape(2, 4096)
+    assert rel_l2(y, g["c1_fwd"]) < 1e-12
+    for name, shp in (("c2a", (8, 16, 32)), ("c2b", (9, 10, 7))):
+        y = run(afc, g[f"{name}_x"], list(shp), "f64").reshape(shp)
+        assert rel_l2(y, g[f"{name}_fwd"]) < 1e-12
+        y32 = run(afc, g[f"{name}_x"].astype(np.complex64), list(shp), "f32").reshape(shp)
+        assert rel_l2(y32, g[f"{name}_fwd"]) < 1e-5
+    for n in (2, 3, 12, 30, 45, 60, 150, 192, 243, 250, 343, 361, 1009, 2048, 4099):
+        y = run(afc, g[f"len_{n}_x"], [n], "f64")
+        assert rel_l2(y, g[f"len_{n}_fwd"]) < 1e-12, n
+
+
+@pytest.mark.parametrize("shape", [(16,), (30,), (7, 12), (4, 6, 8), (9, 10, 7), (3, 1031)])
+def test_r2c_full_and_c2r(afc, oracle, cuda, shape):
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((2,) + shape)
+    ref = np.stack([oracle.fft3d(v.reshape((1,) * (3 - len(shape)) + shape).astype(np.complex128)).reshape(shape)
+                    for v in x])
+    y = run(afc, x, list(shape), "f64", kind="r2c_full", batch=2).reshape(ref.shape)
+    assert rel_l2(y, ref) < 1e-12
+    xr = run(afc, ref, list(shape), "f64", kind="r2c_full", batch=2, inverse=True).reshape(x.shape)
+    assert rel_l2(xr, x) < 1e-12
+    y32 = run(afc, x.astype(np.float32), list(shape), "f32", kind="r2c_full", batch=2).reshape(ref.shape)
+    assert rel_l2(y32, ref) < 1e-5
+
+
+@pytest.mark.parametrize("shape", [(16,), (30,), (7, 12), (4, 6, 8), (64, 64), (5, 2048)])
+def test_r2c_half_and_c2r_half(afc, cuda, shape):
+    rng = np.random.default_rng(12)
+    x = rng.standard_normal((2,) + shape)
+    axes = tuple(range(1, len(shape) + 1))
+    ref = np.fft.rfftn(x, axes=axes)
+    y = run(afc, x, list(shape), "f64", kind="r2c_half", batch=2).reshape(ref.shape)
+    assert rel_l2(y, ref) < 1e-12
+    xr = run(afc, ref, list(shape), "f64", kind="r2c_half", batch=2, inverse=True).reshape(x.shape)
+    assert rel_l2(xr, x) < 1e-12
+
+
+def test_c2r_full_takes_real_part(afc, oracle, cuda):
+    rng = np.random.default_rng(13)
+    X = cplx(rng, (6, 10))
+    ref = oracle.fft2d(X, inverse=True).real
+    y = run(afc, X, [6, 10], "f64", kind="r2c_full", inverse=True).reshape(6, 10)
+    assert rel_l2(y, ref) < 1e-12
+
+
+def test_scaled_and_host_paths(afc, oracle, cuda):
+    rng = np.random.default_rng(14)
+    x = cplx(rng, (256,))
+    p = afc.CudaPlan([256], precision="f64")
+    y = p.execute_host(x)
+    assert rel_l2(y, oracle.fft1d(x)) < 1e-12
+    yi = run(afc, y, [256], "f64", inverse=True, scale=1.0)
+    assert rel_l2(yi, 256 * x) < 1e-12
+
+
+def test_python_api_roundtrips(afc, cuda):  # apollo-python tests/test_smoke.py:7-35
+    s = np.linspace(0.0, 1.0, 8)
+    assert np.allclose(afc.ifft1(afc.fft1(s)), s, atol=1e-12)
+    f = np.arange(64, dtype=np.float64).reshape(4, 4, 4)
+    assert np.allclose(afc.ifft3(afc.fft3(f)), f, atol=1e-12)
+    assert np.allclose(afc.irfft3(afc.rfft3(f), 4), f, atol=1e-12)
+    z = np.zeros((2, 2, 4))
+    z[0, 0, 0] = 1
+    sp = afc.rfft3(z)
+    assert sp.shape == z.shape and sp.dtype == np.complex128
+    assert np.allclose(sp, np.ones(z.shape), atol=1e-12)
+    s32 = np.linspace(0.0, 1.0, 16, dtype=np.float32)
+    sp32 = afc.fft1(s32, precision="low_precision")
+    assert sp32.dtype == np.complex64
+    back = afc.ifft1(sp32, precision="low_precision")
+    assert back.dtype == np.float32 and np.allclose(back, s32, atol=1e-5)
+    f32 = np.arange(64, dtype=np.float32).reshape(4, 4, 4)
+    r = afc.ifft3(afc.fft3(f32, precision="mixed_precision"), precision="mixed_precision")
+    assert np.allclose(r, f32, atol=5e-3 * 64)
+    x = np.arange(12, dtype=np.complex128).reshape(3, 4) * (1 + 0.5j)
+    assert np.allclose(afc.ifft_complex2(afc.fft_complex2(x)), x, atol=1e-12)
+    assert afc.backend_capabilities()["cuda"]["available"] is True
+
+
+def test_native_kernels_ran(afc, cuda):
+    before = afc.kernel_launch_count()
+    run(afc, np.ones(64, dtype=np.complex128), [64], "f64")
+    assert afc.kernel_launch_count() > before
