@@ -368,6 +368,22 @@ static int choose_L(const LenPlan& lp, long long lanes, bool stage_in, bool stag
 static bool plain_in(int op) { return op == IN_C || op == IN_R; }
 static bool plain_out(int op) { return op == OUT_C || op == OUT_RE; }
 
+// Tile-kernel configuration: threads per lane P ~ n/16 (each thread walks its
+// butterflies), lanes per CTA L (>= 8 complex128 / 16 complex64 lanes when
+// strided, so each row is a full 128-byte line), at most 256 threads, three
+// L x ld shared buffers kept under ~110 KB when possible (two CTAs per SM).
+static bool tile_config(const LenPlan& lp, long long lanes, bool lm, size_t csz, int& L, int& P) {
+  const int n = (int)lp.n;
+  const size_t per_lane = 3 * (size_t)lp.ld * csz + 4 * sizeof(long long);
+  const int Lmin = lm ? (csz == 16 ? 8 : 16) : 1;
+  if ((size_t)Lmin * per_lane > kSmemMax) return false;
+  P = std::max(1, std::min(256 / Lmin, (n + 15) / 16));
+  L = std::max(Lmin, 256 / P);
+  while (L > Lmin && ((size_t)L * per_lane > 110 * 1024 || L * P > 256)) L = lm ? L / 2 : L - 1;
+  if ((long long)L > lanes && !lm) L = (int)std::max(1LL, lanes);
+  return (size_t)L * per_lane <= kSmemMax && L * P <= 256;
+}
+
 static void fill_common(LaunchDesc& d, const LenPlan& lp) {
   d.sl = lp.sl;
   d.tw = lp.tw;
@@ -449,6 +465,16 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
       d.nlen = io.nlen;
       d.herm_n = io.herm_n;
       d.pair_w = io.pair_w;
+      if (io.in_op == IN_C && plain_out(io.out_op)) {
+        const bool lm = io.im.es != 1;
+        int L, P;
+        if (tile_config(ap.lp, io.lanes, lm, csz, L, P)) {
+          d.L = L;
+          d.P = P;
+          d.lane_minor = lm ? 1 : 0;
+          return launch_tile(d, dbl, inv, st);
+        }
+      }
       d.stage_in = io.im.es != 1 || !plain_in(io.in_op);
       d.stage_out = io.om.es != 1 || !plain_out(io.out_op) || ap.lp.sl.nst <= 1;
       d.L = choose_L(ap.lp, io.lanes, d.stage_in, d.stage_out, csz);

@@ -36,6 +36,7 @@ struct LaunchDesc {
   int chirp_conj = 0;
   const int* gather = nullptr;
   const int* scatter = nullptr;
+  int lane_minor = 0;
 };
 
 // dynamic shared memory of lanes_kernel: L lanes x buffers x ld + 3 L lane descriptors
@@ -48,7 +49,13 @@ inline size_t conv_smem_bytes(const LaunchDesc& d, size_t csz) {
   return (size_t)d.L * 2 * (size_t)d.ld * csz + (size_t)d.L * 2 * csz + (size_t)d.L * 2 * sizeof(long long);
 }
 
+// tile_kernel: 3 buffers of L x ld elements + 4 L lane bases
+inline size_t tile_smem_bytes(const LaunchDesc& d, size_t csz) {
+  return 3 * (size_t)d.L * (size_t)d.ld * csz + (size_t)d.L * 4 * sizeof(long long);
+}
+
 cudaError_t launch_lanes(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st);
+cudaError_t launch_tile(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st);
 cudaError_t launch_conv(const LaunchDesc& d, bool dbl, cudaStream_t st);
 
 cudaError_t gen_stage_twiddles_dev(void* tw, const StageList& sl, bool dbl, cudaStream_t st);

@@ -49,6 +49,7 @@ template <class T> struct KArgs {
   int chirp_conj;
   const int* gather;       // Rader: gather[q] = g^q mod p
   const int* scatter;      // Rader: scatter[q] = g^{-q} mod p
+  int lane_minor;          // tile kernel: consecutive threads take consecutive lanes
 };
 
 template <class T>
@@ -219,6 +220,176 @@ __global__ void __launch_bounds__(512) lanes_kernel(const __grid_constant__ KArg
       gstore(a, lb[L + l2], lb[2 * L + l2], i, sm[(long long)l2 * nbuf * ld + off + spad(i)], z);
     }
   }
+}
+
+
+// ─────────────────────────────── tile kernel ───────────────────────────────
+// Persistent CTAs walk tiles of L lanes.  The next tile is prefetched into
+// shared memory with cp.async while the current one is transformed, so HBM
+// reads overlap the butterflies and the stores.  Shared memory: two tile
+// buffers and one work buffer, each L x ld (padded) elements; the input tile is
+// first viewed linearly (lane-minor [i][l] for strided lanes, lane-major [l][i]
+// for contiguous ones) and, once stage 0 has consumed it, reused as a padded
+// work buffer.  Strided lanes run lane-minor (consecutive threads take
+// consecutive lanes: conflict-free shared accesses, coalesced rows of L
+// elements); contiguous lanes run lane-major.  The last stage stores straight
+// to global memory.  Plain complex input, complex or real-part output.
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// element i of lane l: p[l * ls + i * is + (pad ? i >> 4 : 0)]
+template <class C> struct SView {
+  C* p;
+  int ls, is, pad;
+  __device__ __forceinline__ C& at(int l, int i) const { return p[l * ls + i * is + (pad ? (i >> 4) : 0)]; }
+};
+
+template <int R, bool INV, class T>
+__device__ __forceinline__ void tstage(const KArgs<T>& a, SView<typename CT<T>::type> src, SView<typename CT<T>::type> dst,
+                                       bool to_global, long long ob, bool valid, int l, int n, int Ns,
+                                       const typename CT<T>::type* __restrict__ tw, int t, int P) {
+  using C = typename CT<T>::type;
+  const int nb = n / R;
+  for (int j = t; j < nb; j += P) {
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src.at(l, j + r * nb);
+    const int k = j % Ns;
+    if (Ns > 1) {
+      const C* w = tw + (long long)k * (R - 1);
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const C wr = w[r - 1];
+        v[r] = INV ? cmulc(v[r], wr) : cmul(v[r], wr);
+      }
+    }
+    DFT<R, INV>::run(v);
+    const int o = (j - k) * R + k;
+    if (to_global) {
+      if (valid) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const long long off = ob + (long long)(o + r * Ns) * a.om.es;
+          if (a.out_op == OUT_RE) static_cast<T*>(a.out)[off] = v[r].x * a.scale;
+          else static_cast<C*>(a.out)[off] = cscale(v[r], a.scale);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) dst.at(l, o + r * Ns) = v[r];
+    }
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void tile_issue(const KArgs<T>& a, typename CT<T>::type* buf, const long long* lbi, long long q0,
+                                           int L, int n, bool lm) {
+  using C = typename CT<T>::type;
+  const long long rem = a.lanes - q0;
+  const int lanes_here = (int)(rem < L ? rem : L);
+  const int total = lanes_here * n;
+  const C* in = static_cast<const C*>(a.in);
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    int l2, i;
+    if (lm) { l2 = e % lanes_here; i = e / lanes_here; }
+    else { l2 = e / n; i = e - l2 * n; }
+    const C* g = in + lbi[l2] + (long long)i * a.im.es;
+    C* s = lm ? buf + i * L + l2 : buf + l2 * n + i;
+    if (sizeof(C) == 16) cp_async16(s, g);
+    else cp_async8(s, g);
+  }
+}
+
+template <class T, bool INV>
+__global__ void __launch_bounds__(256) tile_kernel(const __grid_constant__ KArgs<T> a) {
+  using C = typename CT<T>::type;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int L = a.L, P = a.P, n = a.sl.n, ld = a.ld;
+  C* bufs[2];
+  bufs[0] = reinterpret_cast<C*>(smraw);
+  bufs[1] = bufs[0] + L * ld;
+  C* work = bufs[1] + L * ld;
+  long long* lbi = reinterpret_cast<long long*>(work + L * ld);  // [2][L] input lane bases
+  long long* lbo = lbi + 2 * L;                                     // [2][L] output lane bases
+  const bool lm = a.lane_minor != 0;
+  const int tid = threadIdx.x;
+  const int l = lm ? tid % L : tid / P;
+  const int t = lm ? tid / L : tid % P;
+  const long long ntiles = (a.lanes + L - 1) / L;
+  long long tile = blockIdx.x;
+  if (tile >= ntiles) return;
+  if (tid < L) {
+    const long long q = tile * L + tid;
+    lbi[tid] = q < a.lanes ? a.im.base(q) : 0;
+    lbo[tid] = q < a.lanes ? a.om.base(q) : 0;
+  }
+  __syncthreads();
+  tile_issue(a, bufs[0], lbi, tile * L, L, n, lm);
+  cp_async_commit();
+  const SView<C> wv{work, ld, 1, 1};
+  for (int it = 0;; ++it) {
+    const int cb = it & 1;
+    const long long nxt = tile + gridDim.x;
+    if (nxt < ntiles && tid < L) {
+      const long long q = nxt * L + tid;
+      lbi[(cb ^ 1) * L + tid] = q < a.lanes ? a.im.base(q) : 0;
+      lbo[(cb ^ 1) * L + tid] = q < a.lanes ? a.om.base(q) : 0;
+    }
+    __syncthreads();
+    if (nxt < ntiles) tile_issue(a, bufs[cb ^ 1], lbi + (cb ^ 1) * L, nxt * L, L, n, lm);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    const long long q = tile * L + l;
+    const bool valid = q < a.lanes;
+    const long long ob = lbo[cb * L + l];
+    C* cur = bufs[cb];
+    const SView<C> inv_lin = lm ? SView<C>{cur, 1, L, 0} : SView<C>{cur, n, 1, 0};
+    const SView<C> cv{cur, ld, 1, 1};
+    const int nst = a.sl.nst;
+    if (nst == 0) {
+      if (t == 0 && valid) {
+        const C v = inv_lin.at(l, 0);
+        if (a.out_op == OUT_RE) static_cast<T*>(a.out)[ob] = v.x * a.scale;
+        else static_cast<C*>(a.out)[ob] = cscale(v, a.scale);
+      }
+    }
+    for (int s = 0; s < nst; ++s) {
+      const StageDesc sd = a.sl.st[s];
+      const bool last = s == nst - 1;
+      const SView<C> src = s == 0 ? inv_lin : ((s & 1) ? wv : cv);
+      const SView<C> dst = (s & 1) ? cv : wv;
+      const C* twi = a.tw + sd.twoff;
+#define AFC_TS(R) tstage<R, INV, T>(a, src, dst, last, ob, valid, l, n, sd.Ns, twi, t, P)
+      switch (sd.R) {
+        case 2: AFC_TS(2); break;
+        case 3: AFC_TS(3); break;
+        case 4: AFC_TS(4); break;
+        case 5: AFC_TS(5); break;
+        case 7: AFC_TS(7); break;
+        case 8: AFC_TS(8); break;
+        case 11: AFC_TS(11); break;
+        case 13: AFC_TS(13); break;
+        case 16: AFC_TS(16); break;
+        default: break;
+      }
+#undef AFC_TS
+      if (!last) __syncthreads();
+    }
+    tile = nxt;
+    if (tile >= ntiles) break;
+  }
+  cp_async_wait0();
 }
 
 // ──────────────────────── convolution kernel (Rader / Bluestein) ────────────────────────
@@ -430,6 +601,38 @@ cudaError_t launch_lanes(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t s
   if (d.lanes <= 0) return cudaSuccess;
   if (dbl) return inv ? launch_lanes_t<double, true>(d, st) : launch_lanes_t<double, false>(d, st);
   return inv ? launch_lanes_t<float, true>(d, st) : launch_lanes_t<float, false>(d, st);
+}
+
+static int g_sm_count = 0;
+
+template <class T, bool INV> static cudaError_t launch_tile_t(const LaunchDesc& d, cudaStream_t st) {
+  auto k = tile_kernel<T, INV>;
+  const size_t smem = tile_smem_bytes(d, sizeof(typename CT<T>::type));
+  cudaError_t e = prep_smem(k, smem);
+  if (e != cudaSuccess) return e;
+  if (g_sm_count == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sm_count <= 0) g_sm_count = 148;
+  }
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, d.L * d.P, smem);
+  if (per_sm < 1) per_sm = 1;
+  const long long ntiles = (d.lanes + d.L - 1) / d.L;
+  long long grid = (long long)g_sm_count * per_sm;
+  if (grid > ntiles) grid = ntiles;
+  KArgs<T> ka = to_kargs<T>(d);
+  ka.lane_minor = d.lane_minor;
+  k<<<(unsigned)grid, d.L * d.P, smem, st>>>(ka);
+  count_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tile(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st) {
+  if (d.lanes <= 0) return cudaSuccess;
+  if (dbl) return inv ? launch_tile_t<double, true>(d, st) : launch_tile_t<double, false>(d, st);
+  return inv ? launch_tile_t<float, true>(d, st) : launch_tile_t<float, false>(d, st);
 }
 
 template <class T> static cudaError_t launch_conv_t(const LaunchDesc& d, cudaStream_t st) {

@@ -208,6 +208,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--shape", default=None, help="override the 3D shape, e.g. 128,256,256 (profiling cases)")
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--quick", action="store_true", help="headline only: no other shapes, e2e or CPU legs")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -215,16 +218,21 @@ def main():
     import torch
     import apollofft_b200 as afc
 
+    global SHAPE
+    if args.shape:
+        SHAPE = tuple(int(v) for v in args.shape.split(","))
+    prec = args.precision
+    cdt = torch.complex128 if prec == "f64" else torch.complex64
     world, rank, local = dist_init()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     hbm_peak, peak_kind = load_peaks()
 
     g = torch.Generator(device=dev).manual_seed(2 + rank)
-    x = torch.randn(SHAPE, dtype=torch.complex128, device=dev, generator=g)
+    x = torch.randn(SHAPE, dtype=cdt, device=dev, generator=g)
     x0 = x.clone()
     y = torch.empty_like(x)
-    plan = afc.CudaPlan(list(SHAPE), precision="f64", device=local)
+    plan = afc.CudaPlan(list(SHAPE), precision=prec, device=local)
     launches_per_transform = len(SHAPE)
 
     barrier(world)
@@ -253,7 +261,7 @@ def main():
 
     flops_step = 2 * flops_per_transform(SHAPE)
     value = world * flops_step / t_step_max / 1e9
-    vol_bytes = bytes_per_transform(SHAPE, "f64")  # read + write of the volume
+    vol_bytes = bytes_per_transform(SHAPE, prec)  # read + write of the volume
     launches_per_step = 2 * launches_per_transform
     t_launch = t_step / launches_per_step
     achieved = vol_bytes / t_launch / 1e9
@@ -270,7 +278,7 @@ def main():
     # other shapes / dtypes of the configuration
     also = []
     del y
-    for shp, prec in ALSO:
+    for shp, prec in ([] if args.quick else ALSO):
         dt = torch.complex128 if prec == "f64" else torch.complex64
         xa = torch.randn(shp, dtype=dt, device=dev, generator=g)
         ya = torch.empty_like(xa)
@@ -289,8 +297,9 @@ def main():
         del xa, ya, pa
         torch.cuda.empty_cache()
 
+    prec = args.precision
     # end to end through the host-pointer C-ABI call, pinned buffers
-    hx = torch.randn(SHAPE, dtype=torch.complex128, generator=torch.Generator().manual_seed(2)).pin_memory()
+    hx = torch.randn(SHAPE, dtype=cdt, generator=torch.Generator().manual_seed(2)).pin_memory()
     hy = torch.empty_like(hx).pin_memory()
     hz = torch.empty_like(hx).pin_memory()
     xn, yn, zn = hx.numpy(), hy.numpy(), hz.numpy()
@@ -299,20 +308,20 @@ def main():
     for _ in range(2):
         afc._lib.check(L.afc_execute_host(plan._h, xn.ctypes.data, yn.ctypes.data, 0))
         afc._lib.check(L.afc_execute_host(plan._h, yn.ctypes.data, zn.ctypes.data, 1))
-    e2e_steps = max(3, args.steps // 4)
+    e2e_steps = 0 if args.quick else max(3, args.steps // 4)
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         afc._lib.check(L.afc_execute_host(plan._h, xn.ctypes.data, yn.ctypes.data, 0))
         afc._lib.check(L.afc_execute_host(plan._h, yn.ctypes.data, zn.ctypes.data, 1))
-    t_e2e = (time.perf_counter() - t0) / e2e_steps
+    t_e2e = (time.perf_counter() - t0) / max(e2e_steps, 1)
     t_e2e = max_over_ranks(t_e2e, world, dev)
     e2e_val = world * flops_step / t_e2e / 1e9
 
     # CPU baseline (rank 0, N = 1 only) and the error against the f64 oracle
     cpu = None
     err_oracle = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and not args.quick and prec == "f64":
         from oracle import oracle as O
         gcpu, dt, xin, yref = cpu_transform_gflops(SHAPE, 1, want_output=True)
         cpu = {"value": round(gcpu, 3), "unit": "GFLOP/s", "cores": O.max_threads(), "kind": "port",
@@ -325,9 +334,11 @@ def main():
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t_step_max * 1e3, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1) re/im)",
-            "config": {"workload": "3D C2C 256x256x256 complex128 forward+inverse (1/N)", "shape": list(SHAPE),
-                       "precision": "f64 high_accuracy", "parallelism": f"replicas x{world}",
+            "scaling": "weak", "vs_baseline": None, "dtype": prec, "data": "synthetic (seeded N(0,1) re/im)",
+            "config": {"workload": f"3D C2C {'x'.join(map(str, SHAPE))} {'complex128' if prec == 'f64' else 'complex64'}"
+                                   " forward+inverse (1/N)", "shape": list(SHAPE),
+                       "precision": "f64 high_accuracy" if prec == "f64" else "f32 low_precision",
+                       "parallelism": f"replicas x{world}",
                        "l2": "inputs (268 MB) larger than L2; no flush"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                          "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
@@ -337,8 +348,10 @@ def main():
             "error_vs_oracle_rel_l2": err_oracle,
             "roundtrip_rel_l2": roundtrip_err,
             "cpu_baseline": cpu,
-            "e2e": {"value": round(e2e_val, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": int(2 * 16 * np.prod(SHAPE)),
-                    "d2h_bytes_per_step": int(2 * 16 * np.prod(SHAPE))},
+            "e2e": None if args.quick else {
+                "value": round(e2e_val, 3), "unit": "GFLOP/s",
+                "h2d_bytes_per_step": int(2 * (16 if prec == "f64" else 8) * np.prod(SHAPE)),
+                "d2h_bytes_per_step": int(2 * (16 if prec == "f64" else 8) * np.prod(SHAPE))},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "also": also,

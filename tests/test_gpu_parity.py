@@ -40,13 +40,20 @@ def test_c2c_1d_vs_oracle(afc, oracle, cuda, n, prec):
     rng = np.random.default_rng(n)
     batch = 3 if n < 100000 else 1
     x = cplx(rng, (batch, n))
+    exact = np.fft.fft(x, axis=-1)
     if oracle.dispatch_strategy(n) == "untransformed":
-        ref = np.fft.fft(x, axis=-1)  # the reference leaves p^k (p > 23) untransformed
+        ref = exact  # the reference leaves p^k (p > 23) untransformed
     else:
         ref = oracle.fft1d(x)
     dt = np.complex128 if prec == "f64" else np.complex64
     y = run(afc, x.astype(dt), [n], prec, batch=batch).reshape(batch, n)
-    assert rel_l2(y, ref) < TOL[prec], (n, rel_l2(y, ref))
+    # The reference's f64 four-step builds its twiddles by recurrence; beyond
+    # n ~ 2^17 its own error against the exact DFT exceeds 1e-12 (4e-12 at
+    # 2^18).  The GPU tables are direct FP64 sincospi, so the bar is held
+    # against the exact DFT and the oracle is matched to within its own error.
+    oracle_err = rel_l2(ref, exact)
+    assert rel_l2(y, exact) < TOL[prec], (n, rel_l2(y, exact))
+    assert rel_l2(y, ref) < max(TOL[prec], 1.5 * oracle_err), (n, rel_l2(y, ref), oracle_err)
     yi = run(afc, ref.astype(dt), [n], prec, inverse=True, batch=batch).reshape(batch, n)
     assert rel_l2(yi, x) < TOL[prec]
 
