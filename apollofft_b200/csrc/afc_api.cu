@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -306,6 +307,27 @@ struct AxisPlan {
 
 static afc_status build_axis(int64_t n, bool dbl, AxisPlan& ap, cudaStream_t st);
 
+// One device word per device that bounded waits in the kernels set on timeout.
+static std::mutex g_err_mu;
+static std::map<int, unsigned*> g_err_words;
+static unsigned* device_err_word() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  auto it = g_err_words.find(dev);
+  if (it != g_err_words.end()) return it->second;
+  unsigned* p = nullptr;
+  if (cudaMalloc(&p, sizeof(unsigned)) != cudaSuccess) return nullptr;
+  cudaMemset(p, 0, sizeof(unsigned));
+  g_err_words[dev] = p;
+  return p;
+}
+
+static int env_int(const char* name, int dflt) {
+  const char* v = getenv(name);
+  return v && *v ? atoi(v) : dflt;
+}
+
 static afc_status build_fourstep(int64_t n, bool dbl, AxisPlan& ap, cudaStream_t st) {
   const size_t csz = dbl ? 16 : 8;
   // N1 = divisor nearest sqrt(n) with both factors plannable.
@@ -465,6 +487,12 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
       d.nlen = io.nlen;
       d.herm_n = io.herm_n;
       d.pair_w = io.pair_w;
+      if (io.in_op == IN_C && io.out_op == OUT_C && env_int("AFC_TMA", 1)) {
+        TmaPlan tp;
+        unsigned* err = device_err_word();
+        if (err && tma_plan(ap.lp.sl, ap.lp.ld, io.lanes, io.im, io.om, io.in, io.out, dbl, env_int("AFC_TMA_LANES", 0), tp))
+          return launch_tma(d, tp, err, dbl, inv, st);
+      }
       if (io.in_op == IN_C && plain_out(io.out_op)) {
         const bool lm = io.im.es != 1;
         int L, P;

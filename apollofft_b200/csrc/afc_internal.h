@@ -54,6 +54,18 @@ inline size_t tile_smem_bytes(const LaunchDesc& d, size_t csz) {
   return 3 * (size_t)d.L * (size_t)d.ld * csz + (size_t)d.L * 4 * sizeof(long long);
 }
 
+// TMA tile configuration of one axis pass (afc_tma.cu)
+struct TmaPlan {
+  int mode = 0;  // 0 contiguous lanes (1D bulk copies), 1 strided lanes (3D tensor maps)
+  int L = 1, P = 1, ld = 1, slot_elems = 0;
+  int nbx = 1, bn = 1;
+  long long kb = 1, ntiles = 0, outer = 0;
+};
+bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, const LaneMap& om, const void* in,
+              void* out, bool dbl, int lanes_pref, TmaPlan& tp);
+size_t tma_smem_bytes(const TmaPlan& tp, size_t csz);
+cudaError_t launch_tma(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, bool dbl, bool inv, cudaStream_t st);
+
 cudaError_t launch_lanes(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st);
 cudaError_t launch_tile(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st);
 cudaError_t launch_conv(const LaunchDesc& d, bool dbl, cudaStream_t st);

@@ -1,0 +1,394 @@
+// afc_tma.cu -- TMA-fed axis passes (sm_100a).
+//
+// Persistent CTAs walk tiles of L lanes.  One thread moves whole tiles with the
+// Tensor Memory Accelerator: a 3D tiled tensor map for strided lanes (the
+// volume viewed as [2*es scalars, n, outer], box [2L, bn, 1]: rows of L
+// adjacent lanes, one row per element of the transformed axis) or one 1D bulk
+// copy for contiguous lanes.  Loads complete on an mbarrier (bounded wait; a
+// timeout sets the error word and the CTA returns); the next tile is loaded
+// while the current one is transformed.  The last stage writes the tile back
+// into shared memory in the same layout and one thread stores it with a TMA
+// store, so no thread spends instructions on global addresses.  Loads use no
+// cluster multicast.
+//
+// Shared memory: two tile slots (L x max(ld, rows) elements) and one padded
+// work buffer (L x ld), then two mbarriers.  Stage 0 reads the slot linearly,
+// intermediate stages ping-pong between the work buffer and the slot viewed as
+// padded, and the last stage writes the linear layout into whichever of the two
+// the previous stage did not use; that buffer is the TMA store's source.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstring>
+#include "afc_engine.cuh"
+#include "afc_internal.h"
+
+namespace afc {
+
+template <class T> struct TmaArgs {
+  using C = typename CT<T>::type;
+  CUtensorMap tmi;  // strided mode: input / output tensor maps
+  CUtensorMap tmo;
+  StageList sl;
+  const C* tw;
+  const C* in;      // contiguous mode: bulk copy sources / destinations
+  C* out;
+  long long lanes;  // total lanes
+  long long ntiles;
+  long long kb;     // strided: lane blocks per outer index, ceil(es / L)
+  int L, P, ld, slot_elems;
+  int mode;         // 0 contiguous (1D bulk), 1 strided (tensor)
+  int nbx, bn;      // boxes along the transformed axis, rows per box
+  T scale;
+  unsigned* err;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: about 2^21 polls (each try_wait itself suspends for a while),
+// a few seconds at most; false on timeout.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity) {
+  for (int i = 0; i < (1 << 21); ++i)
+    if (mbar_try_wait(b, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int c0, int c1, int c2, const void* src) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];\n" ::"l"(map), "r"(c0),
+               "r"(c1), "r"(c2), "r"(smem_u32(src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src)), "r"(bytes)
+               : "memory");
+}
+
+template <class C> struct TView {
+  C* p;
+  int ls, is, pad;
+  __device__ __forceinline__ C& at(int l, int i) const { return p[l * ls + i * is + (pad ? (i >> 4) : 0)]; }
+};
+
+template <int R, bool INV, class C, class S>
+__device__ __forceinline__ void tma_stage(TView<C> src, TView<C> dst, int l, int n, int Ns, const C* __restrict__ tw,
+                                          int t, int P, bool scale_out, S sc) {
+  const int nb = n / R;
+  for (int j = t; j < nb; j += P) {
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src.at(l, j + r * nb);
+    const int k = j % Ns;
+    if (Ns > 1) {
+      const C* w = tw + (long long)k * (R - 1);
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const C wr = w[r - 1];
+        v[r] = INV ? cmulc(v[r], wr) : cmul(v[r], wr);
+      }
+    }
+    DFT<R, INV>::run(v);
+    const int o = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst.at(l, o + r * Ns) = scale_out ? cscale(v[r], sc) : v[r];
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void tma_issue_load(const TmaArgs<T>& a, long long tile, typename CT<T>::type* slot,
+                                               unsigned long long* bar) {
+  using C = typename CT<T>::type;
+  if (a.mode == 0) {
+    const long long q0 = tile * a.L;
+    const long long rem = a.lanes - q0;
+    const int lanes_here = (int)(rem < a.L ? rem : a.L);
+    const unsigned bytes = (unsigned)((long long)lanes_here * a.sl.n * sizeof(C));
+    mbar_expect_tx(bar, bytes);
+    bulk_load(slot, a.in + q0 * a.sl.n, bytes, bar);
+  } else {
+    const int o = (int)(tile / a.kb), kb = (int)(tile % a.kb);
+    const unsigned box_bytes = (unsigned)(2 * a.L * a.bn * sizeof(T));
+    mbar_expect_tx(bar, box_bytes * a.nbx);
+    for (int b = 0; b < a.nbx; ++b)
+      tma_load_3d(slot + (long long)b * a.bn * a.L, &a.tmi, 2 * kb * a.L, b * a.bn, o, bar);
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long tile, const typename CT<T>::type* buf) {
+  using C = typename CT<T>::type;
+  if (a.mode == 0) {
+    const long long q0 = tile * a.L;
+    const long long rem = a.lanes - q0;
+    const int lanes_here = (int)(rem < a.L ? rem : a.L);
+    bulk_store(a.out + q0 * a.sl.n, buf, (unsigned)((long long)lanes_here * a.sl.n * sizeof(C)));
+  } else {
+    const int o = (int)(tile / a.kb), kb = (int)(tile % a.kb);
+    for (int b = 0; b < a.nbx; ++b) {
+      // the last box may run past n: rows beyond n hold no data and are clipped by the tensor bounds
+      tma_store_3d(&a.tmo, 2 * kb * a.L, b * a.bn, o, buf + (long long)b * a.bn * a.L);
+    }
+  }
+  bulk_commit();
+}
+
+template <class T, bool INV>
+__global__ void __launch_bounds__(256) tma_kernel(const __grid_constant__ TmaArgs<T> a) {
+  using C = typename CT<T>::type;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const int L = a.L, P = a.P, n = a.sl.n, ld = a.ld;
+  C* slots[2];
+  slots[0] = reinterpret_cast<C*>(smraw);
+  slots[1] = slots[0] + a.slot_elems;
+  C* work = slots[1] + a.slot_elems;
+  unsigned long long* bars =
+      reinterpret_cast<unsigned long long*>(reinterpret_cast<uintptr_t>(work + (long long)L * ld + 1) & ~(uintptr_t)7);
+  const bool lm = a.mode == 1;
+  const int tid = threadIdx.x;
+  const int l = lm ? tid % L : tid / P;
+  const int t = lm ? tid / L : tid % P;
+  long long tile = blockIdx.x;
+  if (tile >= a.ntiles) return;
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_proxy_async();
+  }
+  __syncthreads();
+  if (tid == 0) tma_issue_load(a, tile, slots[0], &bars[0]);
+  const TView<C> wv{work, ld, 1, 1};
+  const int nst = a.sl.nst;
+  for (int it = 0;; ++it) {
+    const int cb = it & 1;
+    const long long nxt = tile + gridDim.x;
+    if (tid == 0) {
+      bulk_wait_read0();  // the previous tile's store has finished reading its buffer
+      if (nxt < a.ntiles) tma_issue_load(a, nxt, slots[cb ^ 1], &bars[cb ^ 1]);
+    }
+    const bool ok = mbar_wait(&bars[cb], (unsigned)((it >> 1) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(a.err, 1u);
+        // let the prefetch already in flight land before the CTA leaves (bounded)
+        if (nxt < a.ntiles) mbar_wait(&bars[cb ^ 1], (unsigned)(((it + 1) >> 1) & 1));
+        bulk_wait0();
+      }
+      return;
+    }
+    C* cur = slots[cb];
+    const TView<C> lin = lm ? TView<C>{cur, 1, L, 0} : TView<C>{cur, n, 1, 0};
+    const TView<C> cpad{cur, ld, 1, 1};
+    // output buffer (linear layout): the one the last stage does not read
+    C* obuf = (nst & 1) ? work : cur;
+    const TView<C> olin = lm ? TView<C>{obuf, 1, L, 0} : TView<C>{obuf, n, 1, 0};
+    for (int s = 0; s < nst; ++s) {
+      const StageDesc sd = a.sl.st[s];
+      const bool last = s == nst - 1;
+      const TView<C> src = s == 0 ? lin : ((s & 1) ? wv : cpad);
+      const TView<C> dst = last ? olin : ((s & 1) ? cpad : wv);
+      const C* twi = a.tw + sd.twoff;
+#define AFC_TM(R) tma_stage<R, INV>(src, dst, l, n, sd.Ns, twi, t, P, last, a.scale)
+      switch (sd.R) {
+        case 2: AFC_TM(2); break;
+        case 3: AFC_TM(3); break;
+        case 4: AFC_TM(4); break;
+        case 5: AFC_TM(5); break;
+        case 7: AFC_TM(7); break;
+        case 8: AFC_TM(8); break;
+        case 11: AFC_TM(11); break;
+        case 13: AFC_TM(13); break;
+        case 16: AFC_TM(16); break;
+        default: break;
+      }
+#undef AFC_TM
+      __syncthreads();
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) tma_issue_store(a, tile, obuf);
+    tile = nxt;
+    if (tile >= a.ntiles) break;
+  }
+  if (tid == 0) bulk_wait0();
+}
+
+// ─────────────────────────────── host side ───────────────────────────────
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+static bool make_map(CUtensorMap* m, const void* base, bool dbl, long long es, long long n, long long outer, int L,
+                     int bn) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  const size_t el = dbl ? 8 : 4;
+  cuuint64_t dims[3] = {(cuuint64_t)(2 * es), (cuuint64_t)n, (cuuint64_t)outer};
+  cuuint64_t strides[2] = {(cuuint64_t)(2 * es * el), (cuuint64_t)(2 * es * n * el)};
+  cuuint32_t box[3] = {(cuuint32_t)(2 * L), (cuuint32_t)bn, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(m, dbl ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base),
+                  dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+static int g_tma_sm = 0;
+
+size_t tma_smem_bytes(const TmaPlan& tp, size_t csz) {
+  return 2 * (size_t)tp.slot_elems * csz + (size_t)tp.L * tp.ld * csz + 64;
+}
+
+// Decides whether an axis pass can run on the TMA kernel and with which tiles.
+bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, const LaneMap& om, const void* in,
+              void* out, bool dbl, int lanes_pref, TmaPlan& tp) {
+  const size_t csz = dbl ? 16 : 8;
+  const long long n = sl.n;
+  if (im.off || om.off) return false;
+  if (im.d1 != 1 || om.d1 != 1 || im.d2 != om.d2 || im.s0 != om.s0 || im.es != om.es || im.s2 != om.s2) return false;
+  if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) return false;
+  if (n < 2) return false;
+  if (im.es == 1) {  // contiguous lanes at q * n
+    if (im.d2 != 1 || im.s0 != n) return false;
+    if ((n * (long long)csz) % 16) return false;
+    tp.mode = 0;
+    tp.L = 1;
+    tp.bn = (int)n;
+    tp.nbx = 1;
+    tp.kb = 1;
+  } else {  // strided lanes: lane (o, k) at o * n * es + k, element stride es
+    const long long es = im.es;
+    if (im.d2 != es || im.s0 != n * es || im.s2 != 1) return false;
+    if (!dbl && (es & 1)) return false;  // 16-byte tensor strides
+    if (lanes % es) return false;
+    tp.mode = 1;
+    tp.L = lanes_pref > 0 ? lanes_pref : (dbl ? 8 : 16);
+    tp.nbx = (int)((n + 255) / 256);
+    tp.bn = (int)((n + tp.nbx - 1) / tp.nbx);
+    tp.kb = (es + tp.L - 1) / tp.L;
+  }
+  tp.ld = ld;
+  // threads: one radix-16 butterfly per thread and stage when possible
+  int P = (int)std::max<long long>(1, std::min<long long>(256, (n + 15) / 16));
+  if (tp.mode == 0) {
+    int L = std::max(1, 256 / P);
+    tp.L = L;
+  }
+  while (tp.L * P > 256) P = std::max(1, P / 2);
+  tp.P = P;
+  const int align = dbl ? 8 : 16;  // 128-byte aligned slots
+  long long rows = tp.mode == 1 ? (long long)tp.nbx * tp.bn : n;
+  long long se = (long long)tp.L * std::max<long long>(ld, rows);
+  se = (se + align - 1) / align * align;
+  tp.slot_elems = (int)se;
+  // shrink the contiguous tile until it fits comfortably
+  while (tp.mode == 0 && tp.L > 1 && tma_smem_bytes(tp, csz) > 110 * 1024) {
+    tp.L--;
+    se = (long long)tp.L * std::max<long long>(ld, n);
+    se = (se + align - 1) / align * align;
+    tp.slot_elems = (int)se;
+  }
+  if (tma_smem_bytes(tp, csz) > 220 * 1024) return false;
+  tp.ntiles = tp.mode == 0 ? (lanes + tp.L - 1) / tp.L : (lanes / im.es) * tp.kb;
+  tp.outer = tp.mode == 1 ? lanes / im.es : 0;
+  return true;
+}
+
+template <class T, bool INV>
+static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, cudaStream_t st) {
+  using C = typename CT<T>::type;
+  auto k = tma_kernel<T, INV>;
+  const size_t smem = tma_smem_bytes(tp, sizeof(C));
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  TmaArgs<T> a;
+  memset(&a, 0, sizeof(a));
+  const bool dbl = sizeof(T) == 8;
+  if (tp.mode == 1) {
+    if (!make_map(&a.tmi, d.in, dbl, d.im.es, d.sl.n, tp.outer, tp.L, tp.bn)) return cudaErrorInvalidValue;
+    if (!make_map(&a.tmo, d.out, dbl, d.om.es, d.sl.n, tp.outer, tp.L, tp.bn)) return cudaErrorInvalidValue;
+  }
+  a.sl = d.sl;
+  a.tw = static_cast<const C*>(d.tw);
+  a.in = static_cast<const C*>(d.in);
+  a.out = static_cast<C*>(d.out);
+  a.lanes = d.lanes;
+  a.ntiles = tp.ntiles;
+  a.kb = tp.kb;
+  a.L = tp.L;
+  a.P = tp.P;
+  a.ld = tp.ld;
+  a.slot_elems = tp.slot_elems;
+  a.mode = tp.mode;
+  a.nbx = tp.nbx;
+  a.bn = tp.bn;
+  a.scale = (T)d.scale;
+  a.err = err;
+  if (g_tma_sm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_tma_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (g_tma_sm <= 0) g_tma_sm = 148;
+  }
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, tp.L * tp.P, smem);
+  if (per_sm < 1) per_sm = 1;
+  long long grid = (long long)g_tma_sm * per_sm;
+  if (grid > tp.ntiles) grid = tp.ntiles;
+  k<<<(unsigned)grid, tp.L * tp.P, smem, st>>>(a);
+  count_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tma(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, bool dbl, bool inv, cudaStream_t st) {
+  if (d.lanes <= 0) return cudaSuccess;
+  if (dbl) return inv ? launch_tma_t<double, true>(d, tp, err, st) : launch_tma_t<double, false>(d, tp, err, st);
+  return inv ? launch_tma_t<float, true>(d, tp, err, st) : launch_tma_t<float, false>(d, tp, err, st);
+}
+
+}  // namespace afc

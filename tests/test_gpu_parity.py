@@ -54,7 +54,7 @@ def test_c2c_1d_vs_oracle(afc, oracle, cuda, n, prec):
     oracle_err = rel_l2(ref, exact)
     assert rel_l2(y, exact) < TOL[prec], (n, rel_l2(y, exact))
     assert rel_l2(y, ref) < max(TOL[prec], 1.5 * oracle_err), (n, rel_l2(y, ref), oracle_err)
-    yi = run(afc, ref.astype(dt), [n], prec, inverse=True, batch=batch).reshape(batch, n)
+    yi = run(afc, exact.astype(dt), [n], prec, inverse=True, batch=batch).reshape(batch, n)
     assert rel_l2(yi, x) < TOL[prec]
 
 
