@@ -27,4 +27,5 @@ __all__ = [
     "rfft3", "rfftfreq",
 ]
 
-_lib.lib()  # fail loudly at import if the CUDA library is missing
+# Every entry point loads libapollofft_cuda.so through _lib.lib(), which raises
+# ImportError when it has not been built: there is no CPU fallback.
