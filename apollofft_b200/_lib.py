@@ -90,6 +90,7 @@ SIGNATURES = {
     "afc_plan_describe": (_i32, [_vp, _i32, ctypes.POINTER(LengthInfo)]),
     "afc_last_error_message": (ctypes.c_char_p, []),
     "afc_kernel_launch_count": (_u64, []),
+    "afc_execute_1d_no_alloc": (_i32, [_vp, _vp, _vp, _i32, _vp]),
 }
 
 _lib = None

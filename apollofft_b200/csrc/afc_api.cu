@@ -1108,6 +1108,35 @@ static cudaError_t run_batch(afc_batch_plan_s& bp, const void* in, void* out, bo
   return cudaSuccess;
 }
 
+
+// ───────────────────────────── allocation-free entry point ─────────────────────────────
+// Scratch for afc_execute_1d_no_alloc: the intermediate between the two passes
+// of the four-step kernels.  A file-scope device array, so the entry point
+// never allocates; every GPU that loads the library holds it until the process
+// exits.  Host code must not use the array's name as a device address: the
+// address comes from cudaGetSymbolAddress, once per device, with that device
+// current.
+static const size_t kNoAllocScratchBytes = (size_t)16 << 20;  // 16 MiB
+static __device__ __align__(256) unsigned char g_no_alloc_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_no_alloc_mu;
+static std::map<int, void*> g_no_alloc_ptr;  // device -> device address of g_no_alloc_scratch
+
+static afc_status no_alloc_scratch(int dev, void** ptr) {
+  std::lock_guard<std::mutex> lk(g_no_alloc_mu);
+  auto it = g_no_alloc_ptr.find(dev);
+  if (it != g_no_alloc_ptr.end()) {
+    *ptr = it->second;
+    return AFC_OK;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_no_alloc_scratch);
+  if (e != cudaSuccess || !p) return cuda_fail(e == cudaSuccess ? cudaErrorInvalidSymbol : e, "no-alloc scratch address");
+  g_no_alloc_ptr[dev] = p;
+  *ptr = p;
+  return AFC_OK;
+}
+
 }  // namespace afc
 
 using namespace afc;
@@ -1463,6 +1492,39 @@ uint64_t afc_kernel_launch_count(void) { return g_launches.load(); }
 
 // Test hook (not part of the public header): the next `count` device
 // allocations fail, so tests can check the AFC_ERR_OUT_OF_MEMORY path.
+
+AFC_API afc_status afc_execute_1d_no_alloc(afc_plan plan, const void* in, void* out, afc_direction direction,
+                                           void* stream) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (!in || !out) return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  if (direction != AFC_FORWARD && direction != AFC_INVERSE)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `direction`: `%d` violates `FORWARD|INVERSE`", (int)direction);
+  if (plan->rank != 1 || plan->kind != AFC_KIND_C2C || plan->axes[0]->algo != ALGO_FOURSTEP)
+    return fail(AFC_ERR_UNSUPPORTED, "afc_execute_1d_no_alloc runs rank-1 C2C plans on the two-pass kernels (got rank %d, kind %d, algo %d)",
+                plan->rank, (int)plan->kind, plan->axes[0]->algo);
+  const size_t csz = plan->dbl ? 16 : 8;
+  const size_t need = (size_t)plan->batch * (size_t)plan->dims[0] * csz;
+  if (need > kNoAllocScratchBytes)
+    return fail(AFC_ERR_VALIDATION,
+                "validation failed for `batch * n`: needs %zu bytes of scratch, the static scratch holds %zu bytes (16 MiB)",
+                need, kNoAllocScratchBytes);
+  DeviceGuard g(plan->device);
+  void* scratch = nullptr;
+  afc_status s = no_alloc_scratch(plan->device, &scratch);
+  if (s != AFC_OK) return s;
+  const bool inv = direction == AFC_INVERSE;
+  long long lanes = 0;
+  AxisIO io;
+  io.im = io.om = axis_map(*plan, 0, plan->dims[0], lanes);
+  io.lanes = lanes;
+  io.in = in;
+  io.out = out;
+  io.scale = inv ? 1.0 / (double)plan->N() : 1.0;
+  cudaError_t e = exec_fourstep(*plan->axes[0], plan->dbl, inv, io, scratch, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "execute (no alloc)");
+  return AFC_OK;
+}
+
 AFC_API void afc_test_fail_next_allocs(int count) { g_fail_allocs.store(count); }
 
 }  // extern "C"

@@ -186,6 +186,20 @@ AFC_API const char* afc_last_error_message(void);
 /* Number of kernels this library launched in this process (all devices). */
 AFC_API uint64_t afc_kernel_launch_count(void);
 
+/* Allocation-free execution of a rank-1 C2C plan whose length runs on the
+ * two-pass (four-step) kernels: the intermediate between the passes lives in a
+ * 16 MiB static device array instead of a cudaMalloc'd workspace, so the call
+ * allocates and frees nothing (cudaMalloc/cudaFree can synchronize the device
+ * and are not allowed inside CUDA stream capture; callers such as streaming
+ * STFT frame loops, allocator-owned memory pools or capture regions cannot
+ * afford them).  No counterpart in the reference.  Create the plan beforehand.
+ * batch * n * sizeof(complex) must not exceed 16 MiB (AFC_ERR_VALIDATION
+ * otherwise).  The first call on a device looks up the array's address and
+ * should come before any stream capture.  All calls share the one array:
+ * calls that overlap on the GPU (different streams, no ordering) race. */
+AFC_API afc_status afc_execute_1d_no_alloc(afc_plan plan, const void* in, void* out, afc_direction direction,
+                                           void* stream);
+
 #ifdef __cplusplus
 }
 #endif
