@@ -251,11 +251,15 @@ static int choose_threads(int64_t n, const std::vector<int>& rad) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(512, p));
 }
 
+// Shared-memory budget of one single-CTA lane; batch plans lower it so that
+// every tile of their persistent kernel fits two CTAs per SM.
+static thread_local size_t tl_smem_cap = kSmemMax;
+
 // A single-CTA plan needs two shared buffers of ld elements for one lane.
 static bool plannable(int64_t n, size_t csz, std::vector<int>* rad_out = nullptr) {
   std::vector<int> rad;
   if (!gpu_radices(n, rad)) return false;
-  if (2 * (size_t)ld_for(n) * csz + 64 > kSmemMax) return false;
+  if (2 * (size_t)ld_for(n) * csz + 64 > tl_smem_cap) return false;
   if (rad_out) *rad_out = rad;
   return true;
 }
@@ -298,6 +302,7 @@ struct AxisPlan {
   int* gather = nullptr;
   int* scatter = nullptr;
   std::unique_ptr<AxisPlan> sub;     // four-step plan of length M (large Bluestein)
+  int tuned_P = 0, tuned_L = 0;      // autotuned tile shape (batch plans)
   ~AxisPlan() {
     void* ptrs[] = {lp.tw, lp1.tw, lp2.tw, tw_hi, tw_lo, chirp, spec_f, spec_i, gather, scatter};
     for (void* p : ptrs)
@@ -415,6 +420,59 @@ static void fill_common(LaunchDesc& d, const LenPlan& lp) {
 
 static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisIO& io, void* ws, cudaStream_t st);
 
+
+// Launch recorder: while a batch plan is being built, the planning code below
+// records its launches (descriptor + kind + direction) instead of issuing
+// them; pointers passed in are tagged with a base selector in their top byte
+// (1 = batch input, 2 = batch output, 3 = batch workspace) and resolved by the
+// persistent kernel at run time.
+struct RecLaunch {
+  LaunchDesc d;
+  int kind;  // 0 lanes, 1 convolution
+  bool inv;
+};
+struct Recorder {
+  std::vector<RecLaunch> launches;
+  int max_threads = 128;
+};
+static thread_local Recorder* tl_rec = nullptr;
+
+static const uint64_t kTagShift = 56;
+static void* tag_ptr(int sel, uint64_t off) { return reinterpret_cast<void*>(((uint64_t)sel << kTagShift) | off); }
+static void untag(const void*& p, int& sel) {
+  const uint64_t v = reinterpret_cast<uint64_t>(p);
+  sel = (int)(v >> kTagShift);
+  p = reinterpret_cast<const void*>(v & (((uint64_t)1 << kTagShift) - 1));
+}
+
+static void record(LaunchDesc d, int kind, bool inv) {
+  const void* in = d.in;
+  const void* out = d.out;
+  untag(in, d.in_sel);
+  untag(out, d.out_sel);
+  d.in = in;
+  d.out = const_cast<void*>(out);
+  const int mt = tl_rec->max_threads;
+  while (d.L > 1 && d.L * d.P > mt) d.L = d.L > 1 ? d.L / 2 : 1;
+  if (d.L * d.P > mt) d.P = std::max(1, mt / d.L);
+  tl_rec->launches.push_back(RecLaunch{d, kind, inv});
+}
+
+static cudaError_t do_lanes(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st) {
+  if (tl_rec) {
+    record(d, 0, inv);
+    return cudaSuccess;
+  }
+  return launch_lanes(d, dbl, inv, st);
+}
+static cudaError_t do_conv(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st) {
+  if (tl_rec) {
+    record(d, 1, inv);
+    return cudaSuccess;
+  }
+  return launch_conv(d, dbl, st);
+}
+
 // Four-step execution of one axis: pass A (N1-point columns, twiddle) into the
 // workspace, pass B (N2-point rows) into the output with the transposed store.
 static cudaError_t exec_fourstep(const AxisPlan& ap, bool dbl, bool inv, const AxisIO& io, void* ws,
@@ -443,7 +501,7 @@ static cudaError_t exec_fourstep(const AxisPlan& ap, bool dbl, bool inv, const A
   a.stage_in = a.im.es != 1 || !plain_in(a.in_op);
   a.stage_out = true;
   a.L = choose_L(ap.lp1, a.lanes, a.stage_in, a.stage_out, csz);
-  cudaError_t e = launch_lanes(a, dbl, inv, st);
+  cudaError_t e = do_lanes(a, dbl, inv, st);
   if (e != cudaSuccess) return e;
   LaunchDesc b;
   fill_common(b, ap.lp2);
@@ -466,7 +524,7 @@ static cudaError_t exec_fourstep(const AxisPlan& ap, bool dbl, bool inv, const A
   b.stage_out = b.om.es != 1 || !plain_out(b.out_op);
   if (ap.lp2.sl.nst <= 1) b.stage_out = true;
   b.L = choose_L(ap.lp2, b.lanes, b.stage_in, b.stage_out, csz);
-  return launch_lanes(b, dbl, inv, st);
+  return do_lanes(b, dbl, inv, st);
 }
 
 static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisIO& io, void* ws, cudaStream_t st) {
@@ -487,13 +545,13 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
       d.nlen = io.nlen;
       d.herm_n = io.herm_n;
       d.pair_w = io.pair_w;
-      if (io.in_op == IN_C && io.out_op == OUT_C && env_int("AFC_TMA", 1)) {
+      if (!tl_rec && io.in_op == IN_C && io.out_op == OUT_C && env_int("AFC_TMA", 1)) {
         TmaPlan tp;
         unsigned* err = device_err_word();
         if (err && tma_plan(ap.lp.sl, ap.lp.ld, io.lanes, io.im, io.om, io.in, io.out, dbl, env_int("AFC_TMA_LANES", 0), tp))
           return launch_tma(d, tp, err, dbl, inv, st);
       }
-      if (io.in_op == IN_C && plain_out(io.out_op)) {
+      if (!tl_rec && io.in_op == IN_C && plain_out(io.out_op)) {
         const bool lm = io.im.es != 1;
         int L, P;
         if (tile_config(ap.lp, io.lanes, lm, csz, L, P)) {
@@ -506,7 +564,11 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
       d.stage_in = io.im.es != 1 || !plain_in(io.in_op);
       d.stage_out = io.om.es != 1 || !plain_out(io.out_op) || ap.lp.sl.nst <= 1;
       d.L = choose_L(ap.lp, io.lanes, d.stage_in, d.stage_out, csz);
-      return launch_lanes(d, dbl, inv, st);
+      if (tl_rec && ap.tuned_P > 0) {
+        d.P = ap.tuned_P;
+        d.L = std::max(1, std::min(d.L, ap.tuned_L));
+      }
+      return do_lanes(d, dbl, inv, st);
     }
     case ALGO_FOURSTEP:
       return exec_fourstep(ap, dbl, inv, io, ws, st);
@@ -539,7 +601,7 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
         d.gather = ap.gather;
         d.scatter = ap.scatter;
         d.L = choose_L(ap.lp, io.lanes, true, true, csz, 2 * csz, 2);
-        return launch_conv(d, dbl, st);
+        return do_conv(d, dbl, inv, st);
       }
       // Bluestein with a four-step convolution: 4 passes over two workspaces.
       const AxisPlan& mp = *ap.sub;
@@ -569,7 +631,7 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
       a.stage_in = true;
       a.stage_out = true;
       a.L = choose_L(mp.lp1, a.lanes, a.stage_in, a.stage_out, csz);
-      cudaError_t e = launch_lanes(a, dbl, false, st);
+      cudaError_t e = do_lanes(a, dbl, false, st);
       if (e != cudaSuccess) return e;
       LaunchDesc b;
       fill_common(b, mp.lp2);
@@ -585,7 +647,7 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
       b.col_mod = N1;
       b.stage_out = true;
       b.L = choose_L(mp.lp2, b.lanes, b.stage_in, b.stage_out, csz);
-      e = launch_lanes(b, dbl, false, st);
+      e = do_lanes(b, dbl, false, st);
       if (e != cudaSuccess) return e;
       LaunchDesc c = a;
       c.tw_conj = 1;
@@ -595,7 +657,7 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
       c.out = w1;
       c.stage_in = true;
       c.L = choose_L(mp.lp1, c.lanes, c.stage_in, c.stage_out, csz);
-      e = launch_lanes(c, dbl, true, st);
+      e = do_lanes(c, dbl, true, st);
       if (e != cudaSuccess) return e;
       LaunchDesc f;
       fill_common(f, mp.lp2);
@@ -615,7 +677,7 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
       f.chirp_conj = inv ? 1 : 0;
       f.stage_out = true;
       f.L = choose_L(mp.lp2, f.lanes, f.stage_in, f.stage_out, csz);
-      return launch_lanes(f, dbl, true, st);
+      return do_lanes(f, dbl, true, st);
     }
     default:
       return cudaSuccess;
@@ -1060,7 +1122,17 @@ struct afc_batch_plan_s {
   size_t ws_bytes = 0;
   void* ws = nullptr;
   std::mutex mu;
-  // CUDA graph of the per-length launches, keyed by (in, out, direction)
+  // persistent phases, per direction
+  struct Phase {
+    void* descs = nullptr;          // device KArgs records
+    afc::BatchItem* items = nullptr;  // device tile list
+    int nitems = 0;
+    size_t smem = 0;
+    int grid = 0;
+  };
+  std::vector<Phase> phases[2];
+  int* counters = nullptr;  // one per phase and direction
+  // CUDA graph of the persistent phases, keyed by (in, out, direction)
   cudaGraphExec_t gexec = nullptr;
   const void* g_in = nullptr;
   void* g_out = nullptr;
@@ -1068,14 +1140,19 @@ struct afc_batch_plan_s {
   ~afc_batch_plan_s() {
     if (gexec) cudaGraphExecDestroy(gexec);
     if (ws) cudaFree(ws);
+    for (auto& v : phases)
+      for (auto& ph : v) {
+        if (ph.descs) cudaFree(ph.descs);
+        if (ph.items) cudaFree(ph.items);
+      }
+    if (counters) cudaFree(counters);
   }
 };
 
 namespace afc {
 
+// Plain per-length launches (mode 1): the same kernels the single plans use.
 static cudaError_t run_batch(afc_batch_plan_s& bp, const void* in, void* out, bool inv, cudaStream_t st) {
-  const size_t csz = bp.dbl ? 16 : 8;
-  (void)csz;
   for (auto& g : bp.groups) {
     AxisIO io;
     io.in = in;
@@ -1099,7 +1176,7 @@ static cudaError_t run_batch(afc_batch_plan_s& bp, const void* in, void* out, bo
       d.out = out;
       d.stage_in = d.stage_out = true;
       d.L = (int)std::min<long long>(256, std::max(1LL, io.lanes));
-      e = launch_lanes(d, bp.dbl, inv, st);
+      e = do_lanes(d, bp.dbl, inv, st);
     } else {
       e = exec_axis(*g->ap, bp.dbl, inv, io, bp.ws, st);
     }
@@ -1108,6 +1185,178 @@ static cudaError_t run_batch(afc_batch_plan_s& bp, const void* in, void* out, bo
   return cudaSuccess;
 }
 
+// Persistent phases (mode 0): one batch_kernel launch per phase.
+static cudaError_t run_batch_persistent(afc_batch_plan_s& bp, const void* in, void* out, bool inv, cudaStream_t st) {
+  auto& ph = bp.phases[inv ? 1 : 0];
+  const size_t np = ph.size();
+  int* ctr = bp.counters + (inv ? 8 : 0);
+  cudaError_t e = cudaMemsetAsync(ctr, 0, np * sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  for (size_t k = 0; k < np; ++k) {
+    e = launch_batch(ph[k].descs, ph[k].items, ph[k].nitems, ctr + k, ph[k].smem, ph[k].grid, in, out, bp.ws, bp.dbl,
+                     inv, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// Autotuner: for each distinct smem-resident length, time the lanes kernel on a
+// scratch buffer for a few threads-per-lane / lanes-per-tile shapes (tiles run
+// on the 128-thread persistent kernel) and keep the fastest.  Results are
+// cached per (length, precision) for the process.
+static std::mutex g_tune_mu;
+static std::map<std::pair<int64_t, int>, std::pair<int, int>> g_tune;
+
+static void tune_group(BatchGroup& g, bool dbl, void* scratch, cudaStream_t st) {
+  AxisPlan& ap = *g.ap;
+  if (ap.algo != ALGO_SMEM) return;
+  const auto key = std::make_pair(g.n, dbl ? 1 : 0);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      ap.tuned_P = it->second.first;
+      ap.tuned_L = it->second.second;
+      return;
+    }
+  }
+  const size_t csz = dbl ? 16 : 8;
+  int rmax = 2;
+  for (int s2 = 0; s2 < ap.lp.sl.nst; ++s2) rmax = std::max(rmax, ap.lp.sl.st[s2].R);
+  std::vector<int> cands;
+  for (int div : {1, 2, 4, 8}) {
+    int P = (int)std::min<int64_t>(128, std::max<int64_t>(1, (g.n + (int64_t)rmax * div - 1) / ((int64_t)rmax * div)));
+    if (std::find(cands.begin(), cands.end(), P) == cands.end()) cands.push_back(P);
+  }
+  const long long lanes = std::max(1LL, std::min<long long>(g.lanes * 4, 64));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int bestP = cands[0], bestL = 1;
+  for (int P : cands) {
+    LaunchDesc d;
+    d.sl = ap.lp.sl;
+    d.tw = ap.lp.tw;
+    d.ld = ap.lp.ld;
+    d.P = P;
+    d.lanes = lanes;
+    d.im = LaneMap{1, 1, g.n, 0, 0, 1, nullptr};
+    d.om = d.im;
+    d.in = scratch;
+    d.out = scratch;
+    const size_t per_lane = 2 * (size_t)d.ld * csz + 3 * sizeof(long long);
+    int L = std::max(1, 128 / P);
+    while (L > 1 && (size_t)L * per_lane > 100 * 1024) --L;
+    d.L = L;
+    d.stage_out = ap.lp.sl.nst <= 1;
+    if (launch_lanes(d, dbl, false, st) != cudaSuccess) continue;
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < 3; ++r) launch_lanes(d, dbl, false, st);
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) continue;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    // cost per lane on the persistent kernel: a tile of L lanes occupies one CTA
+    const float per = ms / (float)lanes;
+    if (per < best) {
+      best = per;
+      bestP = P;
+      bestL = L;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ap.tuned_P = bestP;
+  ap.tuned_L = bestL;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = std::make_pair(bestP, bestL);
+}
+
+// Records every group's launches for one direction and turns them into the
+// phase lists of the persistent kernel (launch k of a group runs in phase k).
+static afc_status build_phases(afc_batch_plan_s& bp, bool inv, cudaStream_t st) {
+  const size_t ksz = kargs_size(bp.dbl);
+  const size_t csz = bp.dbl ? 16 : 8;
+  struct PhaseAcc {
+    std::vector<unsigned char> descs;
+    std::vector<BatchItem> items;
+    std::vector<double> cost;
+    size_t smem = 0;
+  };
+  std::vector<PhaseAcc> acc;
+  for (auto& g : bp.groups) {
+    Recorder rec;
+    tl_rec = &rec;
+    AxisIO io;
+    io.in = tag_ptr(1, 0);
+    io.out = tag_ptr(2, 0);
+    io.lanes = g->lanes;
+    io.im = LaneMap{1, 1, 0, 0, 1, 1, g->d_off};
+    io.om = io.im;
+    io.scale = inv ? 1.0 / (double)g->n : 1.0;
+    cudaError_t e = cudaSuccess;
+    if (g->ap->algo == ALGO_NOOP) {
+      LaunchDesc d;
+      d.sl.n = 1;
+      d.sl.nst = 0;
+      d.P = 1;
+      d.ld = 3;
+      d.lanes = io.lanes;
+      d.im = io.im;
+      d.om = io.om;
+      d.in = io.in;
+      d.out = io.out;
+      d.stage_in = d.stage_out = true;
+      d.L = (int)std::min<long long>(64, std::max(1LL, io.lanes));
+      e = do_lanes(d, bp.dbl, inv, st);
+    } else {
+      e = exec_axis(*g->ap, bp.dbl, inv, io, tag_ptr(3, 0), st);
+    }
+    tl_rec = nullptr;
+    if (e != cudaSuccess) return cuda_fail(e, "batch record");
+    for (size_t k = 0; k < rec.launches.size(); ++k) {
+      if (acc.size() <= k) acc.resize(k + 1);
+      PhaseAcc& pa = acc[k];
+      const RecLaunch& rl = rec.launches[k];
+      const int di = (int)(pa.descs.size() / ksz);
+      pa.descs.resize(pa.descs.size() + ksz);
+      kargs_pack(rl.d, bp.dbl, pa.descs.data() + (size_t)di * ksz);
+      const size_t sm = rl.kind == 0 ? lanes_smem_bytes(rl.d, csz) : conv_smem_bytes(rl.d, csz);
+      pa.smem = std::max(pa.smem, sm);
+      const long long tiles = (rl.d.lanes + rl.d.L - 1) / rl.d.L;
+      const double c = (double)rl.d.sl.n * std::max(1, rl.d.sl.nst) * (rl.kind ? 2.0 : 1.0) * rl.d.L;
+      for (long long t = 0; t < tiles; ++t) {
+        pa.items.push_back(BatchItem{di, rl.kind, t * rl.d.L});
+        pa.cost.push_back(c);
+      }
+    }
+  }
+  if (acc.size() > 8) return fail(AFC_ERR_UNSUPPORTED, "batch plan needs %zu phases (max 8)", acc.size());
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, bp.device);
+  auto& out = bp.phases[inv ? 1 : 0];
+  for (auto& pa : acc) {
+    // longest tiles first, so the atomic tile counter balances the tail
+    std::vector<size_t> ord(pa.items.size());
+    for (size_t i = 0; i < ord.size(); ++i) ord[i] = i;
+    std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return pa.cost[a] > pa.cost[b]; });
+    std::vector<BatchItem> items(ord.size());
+    for (size_t i = 0; i < ord.size(); ++i) items[i] = pa.items[ord[i]];
+    afc_batch_plan_s::Phase ph;
+    ph.nitems = (int)items.size();
+    ph.smem = (pa.smem + 15) / 16 * 16;
+    AFC_CUDA(dev_alloc(&ph.descs, pa.descs.size()), "batch descriptors");
+    AFC_CUDA(dev_alloc((void**)&ph.items, items.size() * sizeof(BatchItem)), "batch items");
+    AFC_CUDA(cudaMemcpyAsync(ph.descs, pa.descs.data(), pa.descs.size(), cudaMemcpyHostToDevice, st), "batch descriptors");
+    AFC_CUDA(cudaMemcpyAsync(ph.items, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, st),
+             "batch items");
+    const int per = batch_blocks_per_sm(ph.smem, bp.dbl, inv);
+    ph.grid = (int)std::min<long long>((long long)sms * per, std::max(1, ph.nitems));
+    out.push_back(ph);
+  }
+  return AFC_OK;
+}
 
 // ───────────────────────────── allocation-free entry point ─────────────────────────────
 // Scratch for afc_execute_1d_no_alloc: the intermediate between the two passes
@@ -1411,6 +1660,9 @@ afc_status afc_batch_plan_create(afc_batch_plan* out, const int64_t* lengths, in
   AFC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
   const size_t csz = bp->dbl ? 16 : 8;
   afc_status s = AFC_OK;
+  // single-CTA lengths of a batch keep two persistent CTAs per SM
+  tl_smem_cap = 100 * 1024;
+  int64_t max_smem_len = 1;
   for (auto& kv : by_len) {
     std::unique_ptr<BatchGroup> grp(new BatchGroup());
     grp->n = kv.first;
@@ -1418,6 +1670,7 @@ afc_status afc_batch_plan_create(afc_batch_plan* out, const int64_t* lengths, in
     grp->ap.reset(new AxisPlan());
     s = build_axis(kv.first, bp->dbl, *grp->ap, st);
     if (s != AFC_OK) break;
+    if (grp->ap->algo == ALGO_SMEM) max_smem_len = std::max<int64_t>(max_smem_len, kv.first * (int64_t)grp->lanes);
     cudaError_t e = dev_alloc((void**)&grp->d_off, kv.second.size() * sizeof(long long));
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(grp->d_off, kv.second.data(), kv.second.size() * sizeof(long long), cudaMemcpyHostToDevice, st);
@@ -1425,11 +1678,36 @@ afc_status afc_batch_plan_create(afc_batch_plan* out, const int64_t* lengths, in
     bp->ws_bytes = std::max(bp->ws_bytes, axis_ws_bytes(*grp->ap, grp->lanes, csz));
     bp->groups.push_back(std::move(grp));
   }
+  tl_smem_cap = kSmemMax;
+  if (s == AFC_OK) {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) s = cuda_fail(e, "batch plan build");
+  }
+  // autotune the smem-resident lengths on a scratch buffer
+  if (s == AFC_OK && env_int("AFC_AUTOTUNE", 1)) {
+    void* scratch = nullptr;
+    const size_t sb = (size_t)std::max<int64_t>(max_smem_len, 1) * 4 * csz + (size_t)1 << 20;
+    if (dev_alloc(&scratch, sb) == cudaSuccess) {
+      cudaMemsetAsync(scratch, 0, sb, st);
+      for (auto& grp : bp->groups) tune_group(*grp, bp->dbl, scratch, st);
+      cudaStreamSynchronize(st);
+      cudaFree(scratch);
+    }
+  }
+  if (s == AFC_OK && bp->ws_bytes) {
+    cudaError_t e = dev_alloc(&bp->ws, bp->ws_bytes);
+    if (e != cudaSuccess) s = cuda_fail(e, "batch workspace");
+  }
+  if (s == AFC_OK) {
+    cudaError_t e = dev_alloc((void**)&bp->counters, 16 * sizeof(int));
+    if (e != cudaSuccess) s = cuda_fail(e, "batch counters");
+  }
+  if (s == AFC_OK) s = build_phases(*bp, false, st);
+  if (s == AFC_OK) s = build_phases(*bp, true, st);
   cudaError_t e = cudaStreamSynchronize(st);
   cudaStreamDestroy(st);
   if (s != AFC_OK) return s;
   if (e != cudaSuccess) return cuda_fail(e, "batch plan build");
-  if (bp->ws_bytes) AFC_CUDA(dev_alloc(&bp->ws, bp->ws_bytes), "batch workspace");
   *out = bp.release();
   return AFC_OK;
 }
@@ -1462,7 +1740,12 @@ afc_status afc_batch_execute(afc_batch_plan plan, const void* in, void* out, afc
     if (e != cudaSuccess) return cuda_fail(e, "batch execute");
     return AFC_OK;
   }
-  // mode 0: the whole batch as one CUDA graph, captured once per (in, out, direction)
+  if (mode == 2) {  // persistent phases without the graph
+    cudaError_t e = run_batch_persistent(*plan, in, out, inv, st);
+    if (e != cudaSuccess) return cuda_fail(e, "batch execute");
+    return AFC_OK;
+  }
+  // mode 0: the persistent phases as one CUDA graph, captured once per (in, out, direction)
   if (!plan->gexec || plan->g_in != in || plan->g_out != out || plan->g_dir != (int)direction) {
     if (plan->gexec) { cudaGraphExecDestroy(plan->gexec); plan->gexec = nullptr; }
     cudaStream_t cs;
@@ -1470,7 +1753,7 @@ afc_status afc_batch_execute(afc_batch_plan plan, const void* in, void* out, afc
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      cudaError_t e2 = run_batch(*plan, in, out, inv, cs);
+      cudaError_t e2 = run_batch_persistent(*plan, in, out, inv, cs);
       e = cudaStreamEndCapture(cs, &graph);
       if (e2 != cudaSuccess) e = e2;
     }

@@ -37,6 +37,15 @@ struct LaunchDesc {
   const int* gather = nullptr;
   const int* scatter = nullptr;
   int lane_minor = 0;
+  int in_sel = 0, out_sel = 0;  // batch descriptors: pointer = base[sel] + offset
+};
+
+// A tile of the persistent batch kernel: descriptor index, kind (0 lanes tile,
+// 1 convolution tile) and first lane.
+struct BatchItem {
+  int desc;
+  int kind;
+  long long q0;
 };
 
 // dynamic shared memory of lanes_kernel: L lanes x buffers x ld + 3 L lane descriptors
@@ -67,6 +76,11 @@ size_t tma_smem_bytes(const TmaPlan& tp, size_t csz);
 cudaError_t launch_tma(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, bool dbl, bool inv, cudaStream_t st);
 
 cudaError_t launch_lanes(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st);
+size_t kargs_size(bool dbl);
+void kargs_pack(const LaunchDesc& d, bool dbl, void* dst);
+cudaError_t launch_batch(const void* descs, const BatchItem* items, int nitems, int* counter, size_t smem, int grid,
+                         const void* in, void* out, void* ws, bool dbl, bool inv, cudaStream_t st);
+int batch_blocks_per_sm(size_t smem, bool dbl, bool inv);
 cudaError_t launch_tile(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st);
 cudaError_t launch_conv(const LaunchDesc& d, bool dbl, cudaStream_t st);
 

@@ -50,6 +50,7 @@ template <class T> struct KArgs {
   const int* gather;       // Rader: gather[q] = g^q mod p
   const int* scatter;      // Rader: scatter[q] = g^{-q} mod p
   int lane_minor;          // tile kernel: consecutive threads take consecutive lanes
+  int in_sel, out_sel;     // batch descriptors: 0 absolute pointer, else base[sel] + offset
 };
 
 template <class T>
@@ -178,17 +179,19 @@ template <class T> __device__ __forceinline__ long long col_of(const KArgs<T>& a
 // ─────────────────────────────── lanes kernel ───────────────────────────────
 // Shared memory: L lanes x nbuf buffers x ld elements, then 3L lane descriptors.
 
+// One tile of L lanes starting at lane q0.  Threads beyond L x P idle through
+// the barriers (the persistent batch kernel runs tiles of different shapes).
 template <class T, bool INV>
-__global__ void __launch_bounds__(512) lanes_kernel(const __grid_constant__ KArgs<T> a) {
+__device__ __forceinline__ void lanes_tile(const KArgs<T>& a, long long q0, unsigned char* smraw) {
   using C = typename CT<T>::type;
-  extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   const int P = a.P, L = a.L, n = a.sl.n, ld = a.ld;
   const int nbuf = engine_buffers(a.sl.nst, a.stage_in, a.stage_out);
   long long* lb = reinterpret_cast<long long*>(sm + (long long)L * nbuf * ld);  // in base, out base, col
   const int tid = threadIdx.x;
-  const int l = tid / P, t = tid - l * P;
-  const long long q0 = (long long)blockIdx.x * L;
+  const bool active = tid < L * P;
+  const int l = active ? tid / P : 0;
+  const int t = active ? tid - l * P : (1 << 30);  // idle threads own no butterfly
   const int lanes_here = (int)((a.lanes - q0) < L ? (a.lanes - q0) : L);
   if (tid < L) {
     const long long qq = q0 + tid;
@@ -208,7 +211,7 @@ __global__ void __launch_bounds__(512) lanes_kernel(const __grid_constant__ KArg
     }
     __syncthreads();
   }
-  const Ctx<T> cx{a, lb[l], lb[L + l], l < lanes_here};
+  const Ctx<T> cx{a, lb[l], lb[L + l], active && l < lanes_here};
   C* res = run_stages<INV>(cx, a.sl, a.tw, t, P, b0, b1, a.stage_in != 0, a.stage_out != 0);
   if (a.stage_out) {
     // every lane ends in the same buffer slot: offset of res within its lane block
@@ -220,6 +223,12 @@ __global__ void __launch_bounds__(512) lanes_kernel(const __grid_constant__ KArg
       gstore(a, lb[L + l2], lb[2 * L + l2], i, sm[(long long)l2 * nbuf * ld + off + spad(i)], z);
     }
   }
+}
+
+template <class T, bool INV>
+__global__ void __launch_bounds__(512) lanes_kernel(const __grid_constant__ KArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  lanes_tile<T, INV>(a, (long long)blockIdx.x * a.L, smraw);
 }
 
 
@@ -399,14 +408,14 @@ __global__ void __launch_bounds__(256) tile_kernel(const __grid_constant__ KArgs
 // carries 1/M), inverse FFT, staged scatter (+ x0, DC) / chirp postmultiply.
 
 template <class T>
-__global__ void __launch_bounds__(512) conv_kernel(const __grid_constant__ KArgs<T> a) {
+__device__ __forceinline__ void conv_tile(const KArgs<T>& a, long long q0, unsigned char* smraw) {
   using C = typename CT<T>::type;
-  extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   const int P = a.P, L = a.L, M = a.sl.n, ld = a.ld;
   const int tid = threadIdx.x;
-  const int l = tid / P, t = tid - l * P;
-  const long long q0 = (long long)blockIdx.x * L;
+  const bool active = tid < L * P;
+  const int l = active ? tid / P : 0;
+  const int t = active ? tid - l * P : (1 << 30);  // idle threads own no butterfly
   const bool rader = a.in_op == IN_GATHER || a.in_op == IN_GATHER_R;
   C* extra = sm + (long long)L * 2 * ld;                         // [2L]: x0, DC per lane
   long long* lb = reinterpret_cast<long long*>(extra + 2 * L);   // [2L]: in base, out base
@@ -451,6 +460,50 @@ __global__ void __launch_bounds__(512) conv_kernel(const __grid_constant__ KArgs
     const C dc = cscale(cadd(extra[2 * tid], extra[2 * tid + 1]), a.scale);
     if (a.out_op == OUT_SCATTER) static_cast<C*>(a.out)[lb[L + tid]] = dc;
     else static_cast<T*>(a.out)[lb[L + tid]] = dc.x;
+  }
+  __syncthreads();
+}
+
+template <class T>
+__global__ void __launch_bounds__(512) conv_kernel(const __grid_constant__ KArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  conv_tile<T>(a, (long long)blockIdx.x * a.L, smraw);
+}
+
+// ───────────────────────── persistent batch kernel ─────────────────────────
+// One launch runs a whole phase of an uneven batch: a list of tiles, each a
+// lanes tile or a convolution tile of some transform length, described by a
+// KArgs record in global memory.  CTAs fetch tiles from an atomic counter
+// (longest tiles first), copy the record into shared memory, resolve its
+// buffer selectors against this launch's bases and run the tile.
+
+template <class T, bool INV>
+__global__ void __launch_bounds__(128) batch_kernel(const KArgs<T>* __restrict__ descs, const BatchItem* __restrict__ items,
+                                                   int nitems, int* counter, const void* in_base, void* out_base,
+                                                   void* ws_base) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ __align__(16) KArgs<T> ka;
+  __shared__ int cur;
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) cur = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = cur;
+    if (it >= nitems) break;
+    const BatchItem bi = items[it];
+    const int* src = reinterpret_cast<const int*>(descs + bi.desc);
+    int* dst = reinterpret_cast<int*>(&ka);
+    for (int w = tid; w < (int)(sizeof(KArgs<T>) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    if (tid == 0) {
+      char* bases[4] = {nullptr, (char*)in_base, (char*)out_base, (char*)ws_base};
+      if (ka.in_sel) ka.in = bases[ka.in_sel] + (size_t)ka.in;
+      if (ka.out_sel) ka.out = bases[ka.out_sel] + (size_t)ka.out;
+    }
+    __syncthreads();
+    if (bi.kind == 0) lanes_tile<T, INV>(ka, bi.q0, smraw);
+    else conv_tile<T>(ka, bi.q0, smraw);
+    __syncthreads();
   }
 }
 
@@ -578,6 +631,9 @@ template <class T> static KArgs<T> to_kargs(const LaunchDesc& d) {
   a.chirp_conj = d.chirp_conj;
   a.gather = d.gather;
   a.scatter = d.scatter;
+  a.lane_minor = d.lane_minor;
+  a.in_sel = d.in_sel;
+  a.out_sel = d.out_sel;
   return a;
 }
 
@@ -649,6 +705,51 @@ template <class T> static cudaError_t launch_conv_t(const LaunchDesc& d, cudaStr
 cudaError_t launch_conv(const LaunchDesc& d, bool dbl, cudaStream_t st) {
   if (d.lanes <= 0) return cudaSuccess;
   return dbl ? launch_conv_t<double>(d, st) : launch_conv_t<float>(d, st);
+}
+
+size_t kargs_size(bool dbl) { return dbl ? sizeof(KArgs<double>) : sizeof(KArgs<float>); }
+
+void kargs_pack(const LaunchDesc& d, bool dbl, void* dst) {
+  if (dbl) {
+    KArgs<double> a = to_kargs<double>(d);
+    memcpy(dst, &a, sizeof(a));
+  } else {
+    KArgs<float> a = to_kargs<float>(d);
+    memcpy(dst, &a, sizeof(a));
+  }
+}
+
+template <class T, bool INV>
+static cudaError_t launch_batch_t(const void* descs, const BatchItem* items, int nitems, int* counter, size_t smem,
+                                  int grid, const void* in, void* out, void* ws, cudaStream_t st) {
+  auto k = batch_kernel<T, INV>;
+  cudaError_t e = prep_smem(k, smem);
+  if (e != cudaSuccess) return e;
+  k<<<grid, 128, smem, st>>>(static_cast<const KArgs<T>*>(descs), items, nitems, counter, in, out, ws);
+  count_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch(const void* descs, const BatchItem* items, int nitems, int* counter, size_t smem, int grid,
+                         const void* in, void* out, void* ws, bool dbl, bool inv, cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  if (dbl)
+    return inv ? launch_batch_t<double, true>(descs, items, nitems, counter, smem, grid, in, out, ws, st)
+               : launch_batch_t<double, false>(descs, items, nitems, counter, smem, grid, in, out, ws, st);
+  return inv ? launch_batch_t<float, true>(descs, items, nitems, counter, smem, grid, in, out, ws, st)
+             : launch_batch_t<float, false>(descs, items, nitems, counter, smem, grid, in, out, ws, st);
+}
+
+int batch_blocks_per_sm(size_t smem, bool dbl, bool inv) {
+  int per = 1;
+  if (dbl) {
+    if (inv) { prep_smem(batch_kernel<double, true>, smem); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<double, true>, 128, smem); }
+    else { prep_smem(batch_kernel<double, false>, smem); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<double, false>, 128, smem); }
+  } else {
+    if (inv) { prep_smem(batch_kernel<float, true>, smem); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<float, true>, 128, smem); }
+    else { prep_smem(batch_kernel<float, false>, smem); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<float, false>, 128, smem); }
+  }
+  return per < 1 ? 1 : per;
 }
 
 static unsigned table_grid(long long n) {

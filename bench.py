@@ -211,9 +211,13 @@ def main():
     ap.add_argument("--shape", default=None, help="override the 3D shape, e.g. 128,256,256 (profiling cases)")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
     ap.add_argument("--quick", action="store_true", help="headline only: no other shapes, e2e or CPU legs")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="c2 (default) is the headline; c1/c3/c4/c5 print their own lines")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "c2":
+        return run_secondary(args)
 
     import torch
     import apollofft_b200 as afc
@@ -361,6 +365,130 @@ def main():
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+    return 0
+
+
+def _events_time(fn, steps, warmup, torch):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        fn()
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / steps
+
+
+def run_secondary(args):
+    """Lines for the other configurations (not the headline)."""
+    import torch
+    import apollofft_b200 as afc
+    from apollofft_b200 import workloads as W
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    hbm_peak, peak_kind = load_peaks()
+    line = {"workload": args.workload, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "peak_gbs": hbm_peak}
+    if args.workload == "c1":
+        x = torch.from_numpy(W.c1_input()).to(dev)
+        y = torch.empty_like(x)
+        p = afc.CudaPlan([4096], precision="f64", batch=64)
+        t = _events_time(lambda: (p.execute(x, out=y), p.execute(y, out=x, inverse=True)), args.steps, args.warmup, torch)
+        fl = 2 * 64 * 5 * 4096 * 12
+        line.update({"metric": "GFLOP/s", "value": round(fl / t / 1e9, 2), "us_per_step": round(t * 1e6, 2),
+                     "config": "1D C2C f64 N=4096 x64 fwd+inv",
+                     "hbm_frac": round(2 * 2 * 64 * 4096 * 16 / t / 1e9 / hbm_peak, 4)})
+        from oracle import oracle as O
+        xin = W.c1_input()
+        t0 = time.perf_counter()
+        reps = 20
+        for _ in range(reps):
+            yy = O.fft1d(xin)
+            O.fft1d(yy, inverse=True)
+        tc = (time.perf_counter() - t0) / reps
+        line["cpu_baseline"] = {"value": round(fl / tc / 1e9, 2), "unit": "GFLOP/s", "cores": O.max_threads(),
+                                "kind": "port", "sample": f"{reps} x (64 x 4096 fwd+inv)"}
+        line["error_vs_oracle_rel_l2"] = float(np.linalg.norm(p.execute(torch.from_numpy(xin).to(dev)).cpu().numpy()
+                                                              - yy) / np.linalg.norm(yy))
+    elif args.workload == "c3":
+        lens = W.c3_lengths()
+        xv = W.c3_values(lens)
+        x = torch.from_numpy(xv).to(dev)
+        t0 = time.perf_counter()
+        bp = afc.BatchPlan(lens, precision="f32")
+        plan_s = time.perf_counter() - t0
+        y = torch.empty_like(x)
+        fl = float(np.sum(5.0 * lens * np.log2(lens)))
+        by = float(np.sum(2.0 * lens * 8))
+        res = {}
+        for mode, name in ((0, "persistent_graph"), (2, "persistent_nograph"), (1, "per_size_launches")):
+            t = _events_time(lambda: bp.execute(x, out=y, mode=mode), args.steps, args.warmup, torch)
+            res[name] = {"us": round(t * 1e6, 1), "gflops": round(fl / t / 1e9, 1),
+                         "hbm_frac": round(by / t / 1e9 / hbm_peak, 4)}
+        line.update({"metric": "GFLOP/s", "value": res["persistent_graph"]["gflops"], "modes": res,
+                     "config": "4096 uneven 1D complex64 lengths log-uniform [64, 65536], thirds pow2/7-smooth/prime",
+                     "distinct_lengths": int(len(np.unique(lens))), "points": int(lens.sum()),
+                     "plan_seconds": round(plan_s, 2)})
+        yy = bp.execute(x, mode=0).cpu().numpy()
+        offs = np.concatenate([[0], np.cumsum(lens)[:-1]])
+        errs = [np.linalg.norm(yy[o:o + n] - np.fft.fft(xv[o:o + n].astype(np.complex128)))
+                / np.linalg.norm(np.fft.fft(xv[o:o + n].astype(np.complex128))) for o, n in zip(offs[::64], lens[::64])]
+        line["max_rel_l2_sampled_lanes_vs_f64"] = float(max(errs))
+        from oracle import oracle as O
+        sample = slice(0, len(lens), 16)
+        sl = lens[sample]
+        so = np.concatenate([[0], np.cumsum(sl)[:-1]])
+        sx = np.concatenate([xv[o:o + n] for o, n in zip(offs[sample], sl)])
+        t0 = time.perf_counter()
+        O.fft_uneven(sx, so, sl)
+        tc = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(float(np.sum(5.0 * sl * np.log2(sl))) / tc / 1e9, 3), "unit": "GFLOP/s",
+                                "cores": O.max_threads(), "kind": "port",
+                                "sample": f"every 16th lane ({len(sl)} lanes), oracle per-length dispatch f32"}
+    elif args.workload == "c4":
+        xs, k = W.c4_rows()
+        x = torch.from_numpy(xs).to(dev)
+        y = torch.empty_like(x)
+        p32 = afc.CudaPlan([4096], precision="f32", batch=16384)
+        t = _events_time(lambda: p32.execute(x, out=y), args.steps, args.warmup, torch)
+        fl = 16384 * 5 * 4096 * 12
+        ref = afc.CudaPlan([4096], precision="f64", batch=16384).execute(x.to(torch.complex128))
+        y = p32.execute(x).to(torch.complex128)
+        num = torch.linalg.vector_norm(y - ref, dim=-1)
+        den = torch.linalg.vector_norm(ref, dim=-1)
+        rel = (num / den).cpu().numpy()
+        line.update({"metric": "GFLOP/s", "value": round(fl / t / 1e9, 1), "us": round(t * 1e6, 1),
+                     "config": "16384 x 4096 complex64 forward, FP32 SIMT Stockham",
+                     "hbm_frac": round(2 * 16384 * 4096 * 8 / t / 1e9 / hbm_peak, 4),
+                     "rel_l2_vs_f64_per_row": {"max": float(rel.max()), "median": float(np.median(rel))},
+                     "max_abs_vs_f64": float(torch.max(torch.abs(y - ref)).item())})
+    elif args.workload == "c5":
+        from apollofft_b200 import autograd as AG
+        g = torch.Generator(device=dev).manual_seed(5)
+        img = torch.randn(8, 2048, 2048, dtype=torch.float32, device=dev, generator=g)
+        w = torch.from_numpy(W.radial_weight(2048)).to(dev).to(torch.float32)
+
+        def fwd():
+            with torch.no_grad():
+                return torch.sum(torch.abs(w * AG.rfft2(img)) ** 2)
+
+        xg = img.clone().requires_grad_(True)
+
+        def fwdbwd():
+            xg.grad = None
+            loss = torch.sum(torch.abs(w * AG.rfft2(xg)) ** 2)
+            loss.backward()
+
+        tf = _events_time(fwd, args.steps, args.warmup, torch)
+        tb = _events_time(fwdbwd, args.steps, args.warmup, torch)
+        N = 2048 * 2048
+        fl = 8 * 2.5 * N * math.log2(N)
+        line.update({"metric": "ms", "forward_ms": round(tf * 1e3, 3), "forward_backward_ms": round(tb * 1e3, 3),
+                     "ratio": round(tb / tf, 3), "forward_gflops_r2c_convention": round(fl / tf / 1e9, 1),
+                     "config": "8 x 2048^2 f32 real, full-spectrum R2C (reference contract), loss sum |w X|^2"})
+    print(json.dumps(line), flush=True)
     return 0
 
 
