@@ -1106,6 +1106,7 @@ struct BatchGroup {
   long long lanes = 0;
   std::unique_ptr<AxisPlan> ap;
   long long* d_off = nullptr;  // device lane offsets (packed layout)
+  size_t ws_off = 0;           // this group's workspace region (groups of a phase run concurrently)
   ~BatchGroup() {
     if (d_off) cudaFree(d_off);
   }
@@ -1178,7 +1179,7 @@ static cudaError_t run_batch(afc_batch_plan_s& bp, const void* in, void* out, bo
       d.L = (int)std::min<long long>(256, std::max(1LL, io.lanes));
       e = do_lanes(d, bp.dbl, inv, st);
     } else {
-      e = exec_axis(*g->ap, bp.dbl, inv, io, bp.ws, st);
+      e = exec_axis(*g->ap, bp.dbl, inv, io, static_cast<char*>(bp.ws) + g->ws_off, st);
     }
     if (e != cudaSuccess) return e;
   }
@@ -1311,7 +1312,7 @@ static afc_status build_phases(afc_batch_plan_s& bp, bool inv, cudaStream_t st) 
       d.L = (int)std::min<long long>(64, std::max(1LL, io.lanes));
       e = do_lanes(d, bp.dbl, inv, st);
     } else {
-      e = exec_axis(*g->ap, bp.dbl, inv, io, tag_ptr(3, 0), st);
+      e = exec_axis(*g->ap, bp.dbl, inv, io, tag_ptr(3, g->ws_off), st);
     }
     tl_rec = nullptr;
     if (e != cudaSuccess) return cuda_fail(e, "batch record");
@@ -1675,7 +1676,8 @@ afc_status afc_batch_plan_create(afc_batch_plan* out, const int64_t* lengths, in
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(grp->d_off, kv.second.data(), kv.second.size() * sizeof(long long), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) { s = cuda_fail(e, "batch offsets"); break; }
-    bp->ws_bytes = std::max(bp->ws_bytes, axis_ws_bytes(*grp->ap, grp->lanes, csz));
+    grp->ws_off = bp->ws_bytes;
+    bp->ws_bytes += (axis_ws_bytes(*grp->ap, grp->lanes, csz) + 255) / 256 * 256;
     bp->groups.push_back(std::move(grp));
   }
   tl_smem_cap = kSmemMax;

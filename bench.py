@@ -11,7 +11,7 @@ value        : whole-job GFLOP/s, 5 N log2 N per transform, two transforms per s
                data already in HBM, CUDA events on the launching stream.
 e2e          : the same metric through afc_execute_host (the reference-facing slice
                API) from pinned host buffers, copies inside the timed region.
-roofline     : the dominant kernel (lanes_kernel, every launch of the step): bytes a
+roofline     : the dominant kernel (tma_kernel, every launch of the step): bytes a
                launch moves algorithmically (read + write of the volume it
                transforms) / its average duration, against MEASURED_PEAKS.json.
 cpu_baseline : the oracle's restatement of the reference CPU plan (FftPlan3D<f64>),
@@ -272,10 +272,10 @@ def main():
     transform_frac = (2 * vol_bytes / t_step / 1e9) / hbm_peak
 
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "lanes_kernel_traffic.json")
+    tf = os.path.join(ROOT, "profiles", "tma_kernel_traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get("bytes_per_launch_256cube_f64")
+            traffic = json.load(open(tf)).get("bytes_per_launch_256cube_f64") if SHAPE == (256, 256, 256) else None
         except (ValueError, OSError):
             traffic = None
 
@@ -346,7 +346,7 @@ def main():
                        "l2": "inputs (268 MB) larger than L2; no flush"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                          "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
-                         "kernel": "lanes_kernel<double> (all launches of the step)",
+                         "kernel": "tma_kernel<double> (all launches of the step)",
                          "peak_source": peak_kind},
             "transform_hbm_frac": round(transform_frac, 4),
             "error_vs_oracle_rel_l2": err_oracle,
