@@ -111,6 +111,10 @@ def lib():
             fn.argtypes = args
         L.afc_test_fail_next_allocs.restype = None
         L.afc_test_fail_next_allocs.argtypes = [ctypes.c_int]
+        L.afc_test_tc_tile.restype = ctypes.c_int
+        L.afc_test_tc_tile.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.afc_test_take_device_error.restype = ctypes.c_int
+        L.afc_test_take_device_error.argtypes = []
         _lib = L
     return _lib
 

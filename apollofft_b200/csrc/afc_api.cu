@@ -814,6 +814,7 @@ struct afc_plan_s {
   int64_t batch = 1;
   int device = 0;
   bool dbl = true;
+  int tc = 0;  // 1 BF16 split, 2 FP16 split tensor-core stages
   std::unique_ptr<afc::AxisPlan> axes[3];
   std::atomic<int> refs{1};
   bool cached = false;
@@ -1033,8 +1034,17 @@ static afc_status create_plan(afc_plan* out, int rank, const int64_t* dims, afc_
       return fail(AFC_ERR_VALIDATION, "validation failed for `%s`: `%lld` violates `must be > 0`", names[rank - 1][a],
                   (long long)dims[a]);
   if (batch < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `batch`: `%lld` violates `must be > 0`", (long long)batch);
-  if (prec != AFC_PREC_F32 && prec != AFC_PREC_F64)
-    return fail(AFC_ERR_UNSUPPORTED, "precision %d needs the tensor-core plan (afc_tc_* entry points)", (int)prec);
+  if (prec != AFC_PREC_F32 && prec != AFC_PREC_F64 && prec != AFC_PREC_TC_BF16_SPLIT && prec != AFC_PREC_TC_FP16_SPLIT)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `precision`: `%d` violates `F32|F64|TC_BF16_SPLIT|TC_FP16_SPLIT`", (int)prec);
+  const bool tcp = prec == AFC_PREC_TC_BF16_SPLIT || prec == AFC_PREC_TC_FP16_SPLIT;
+  if (tcp) {
+    const int64_t n = dims[0];
+    bool pow16 = rank == 1 && kind == AFC_KIND_C2C && n >= 16 && (n & (n - 1)) == 0 && (__builtin_ctzll(n) % 4 == 0);
+    if (!pow16 || n > 4096)
+      return fail(AFC_ERR_UNSUPPORTED,
+                  "tensor-core plans are rank-1 C2C with n = 16^s <= 4096 (radix-16 stages only); got rank %d, n %lld",
+                  rank, (long long)n);
+  }
   if (kind != AFC_KIND_C2C && kind != AFC_KIND_R2C_FULL && kind != AFC_KIND_R2C_HALF)
     return fail(AFC_ERR_VALIDATION, "validation failed for `kind`: `%d` violates `C2C|R2C_FULL|R2C_HALF`", (int)kind);
   int ndev = 0;
@@ -1051,6 +1061,7 @@ static afc_status create_plan(afc_plan* out, int rank, const int64_t* dims, afc_
   p->batch = batch;
   p->device = device;
   p->dbl = prec == AFC_PREC_F64;
+  p->tc = prec == AFC_PREC_TC_BF16_SPLIT ? 1 : (prec == AFC_PREC_TC_FP16_SPLIT ? 2 : 0);
   cudaStream_t st;
   AFC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
   afc_status s = AFC_OK;
@@ -1084,6 +1095,22 @@ static afc_status execute(afc_plan p, const void* in, void* out, afc_direction d
   const double sc = use_scale ? scale : (inv ? 1.0 / (double)p->N() : 1.0);
   DeviceGuard g(p->device);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (p->tc) {
+    const AxisPlan& ap = *p->axes[0];
+    TcLaunch d;
+    d.in = in;
+    d.out = out;
+    d.tw = ap.lp.tw;
+    d.sl = ap.lp.sl;
+    d.lanes = p->batch;
+    d.scale = sc;
+    d.inverse = inv ? 1 : 0;
+    d.err = device_err_word();
+    if (!d.err) return fail(AFC_ERR_OUT_OF_MEMORY, "error word allocation failed");
+    cudaError_t e = launch_tc_fft(d, p->tc == 2, st);
+    if (e != cudaSuccess) return cuda_fail(e, "execute (tensor cores)");
+    return AFC_OK;
+  }
   if (own_ws) {
     std::lock_guard<std::mutex> lk(p->ws_mu);
     if (p->ws_bytes && !p->ws) AFC_CUDA(dev_alloc(&p->ws, p->ws_bytes), "workspace");
@@ -1807,6 +1834,47 @@ AFC_API afc_status afc_execute_1d_no_alloc(afc_plan plan, const void* in, void* 
   io.scale = inv ? 1.0 / (double)plan->N() : 1.0;
   cudaError_t e = exec_fourstep(*plan->axes[0], plan->dbl, inv, io, scratch, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "execute (no alloc)");
+  return AFC_OK;
+}
+
+// Test hook (not part of the public header): one tensor-core tile
+// D = A * B^T (A 128 x 32, B 32 x 32, f32 host arrays split into hi/lo BF16 or
+// FP16 halves), used to check the operand descriptors.  Returns AFC_ERR_TIMEOUT
+// if the MMA completion barrier timed out.
+AFC_API afc_status afc_test_tc_tile(const float* hA, const float* hB, float* hD, int fp16) {
+  float *dA = nullptr, *dB = nullptr, *dD = nullptr;
+  unsigned* err = nullptr;
+  AFC_CUDA(cudaMalloc(&dA, 128 * 32 * 4), "alloc");
+  AFC_CUDA(cudaMalloc(&dB, 32 * 32 * 4), "alloc");
+  AFC_CUDA(cudaMalloc(&dD, 128 * 32 * 4), "alloc");
+  AFC_CUDA(cudaMalloc(&err, 4), "alloc");
+  cudaMemcpy(dA, hA, 128 * 32 * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(dB, hB, 32 * 32 * 4, cudaMemcpyHostToDevice);
+  cudaMemset(err, 0, 4);
+  cudaError_t e = launch_tc_selftest(dA, dB, dD, err, fp16 != 0, 0);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  unsigned he = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(hD, dD, 128 * 32 * 4, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(&he, err, 4, cudaMemcpyDeviceToHost);
+  cudaFree(dA);
+  cudaFree(dB);
+  cudaFree(dD);
+  cudaFree(err);
+  if (e != cudaSuccess) return cuda_fail(e, "tc tile");
+  if (he) return fail(AFC_ERR_TIMEOUT, "tensor-core completion barrier timed out");
+  return AFC_OK;
+}
+
+// Reads and clears the device error word bounded waits set on timeout (after
+// synchronizing the device): AFC_ERR_TIMEOUT if any kernel gave up waiting.
+AFC_API afc_status afc_test_take_device_error(void) {
+  unsigned* w = device_err_word();
+  if (!w) return fail(AFC_ERR_OUT_OF_MEMORY, "error word");
+  unsigned h = 0;
+  AFC_CUDA(cudaDeviceSynchronize(), "synchronize");
+  AFC_CUDA(cudaMemcpy(&h, w, 4, cudaMemcpyDeviceToHost), "read error word");
+  cudaMemset(w, 0, 4);
+  if (h) return fail(AFC_ERR_TIMEOUT, "a kernel's bounded wait timed out");
   return AFC_OK;
 }
 

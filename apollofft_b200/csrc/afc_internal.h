@@ -75,6 +75,21 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
 size_t tma_smem_bytes(const TmaPlan& tp, size_t csz);
 cudaError_t launch_tma(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, bool dbl, bool inv, cudaStream_t st);
 
+// tensor-core radix-16 FFT (afc_tc.cu)
+struct TcLaunch {
+  const void* in = nullptr;
+  void* out = nullptr;
+  const void* tw = nullptr;
+  StageList sl{};
+  long long lanes = 0;
+  double scale = 1.0;
+  int inverse = 0;
+  unsigned* err = nullptr;
+};
+cudaError_t launch_tc_fft(const TcLaunch& d, bool fp16, cudaStream_t st);
+cudaError_t launch_tc_selftest(const float* A, const float* B, float* D, unsigned* err, bool fp16, cudaStream_t st);
+size_t tc_fft_smem(int n);
+
 cudaError_t launch_lanes(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st);
 size_t kargs_size(bool dbl);
 void kargs_pack(const LaunchDesc& d, bool dbl, void* dst);

@@ -1,0 +1,390 @@
+// afc_tc.cu -- split-precision tensor-core radix-16 stages (tcgen05, sm_100a).
+//
+// A radix-16 Stockham stage applied to 128 butterflies is one small matrix
+// product: D[b][o] = sum_i X[b][i] F[o][i], with X the 128 x 32 real block of
+// twiddled inputs (row b = butterfly b: 16 real parts then 16 imaginary parts)
+// and F the 32 x 32 real form of the 16-point DFT matrix (rows: 16 real then 16
+// imaginary outputs).  X and F are split into hi + lo halves of BF16 or FP16
+// (v = hi + lo, lo = v - hi rounded again) and the four products
+// Xh Fh + Xh Fl + Xl Fh + Xl Fl accumulate in FP32 in tensor memory: one
+// tcgen05.mma (M = 128, N = 32, K = 16) per half-K step, issued by one thread;
+// the accumulator row of butterfly b lives in TMEM lane b, so after
+// tcgen05.ld each thread holds its butterfly's 16 outputs.  FP16 blocks are
+// scaled per butterfly by a power of two so high-dynamic-range rows stay in
+// range (the scale is undone exactly after the product).
+//
+// Operands sit in shared memory in the canonical K-major, no-swizzle layout:
+// 8-row x 16-byte core matrices, LBO = 128 B between the two K halves of a
+// 16-wide K step, SBO = 512 B between 8-row groups (K = 32 per row group).
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cstdint>
+#include <cstring>
+#include "afc_engine.cuh"
+#include "afc_internal.h"
+
+namespace afc {
+
+__device__ __forceinline__ unsigned tc_smem(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t umma_desc(const void* p) {
+  const uint64_t addr = (uint64_t)(tc_smem(p) >> 4) & 0x3FFF;
+  const uint64_t lbo = (128 >> 4) & 0x3FFF;
+  const uint64_t sbo = (512 >> 4) & 0x3FFF;
+  return addr | (lbo << 16) | (sbo << 32) | ((uint64_t)1 << 46);  // version 1, base 0, SWIZZLE_NONE
+}
+
+// kind::f16 instruction descriptor: D f32, A/B bf16 (fmt 1) or f16 (fmt 0), both K-major, M = 128, N = 32.
+__host__ __device__ constexpr uint32_t umma_idesc(uint32_t fmt) {
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit(unsigned long long* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(tc_smem(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+__device__ __forceinline__ void tc_mbar_init(unsigned long long* b) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(tc_smem(b)) : "memory");
+}
+__device__ __forceinline__ bool tc_mbar_wait(unsigned long long* b, unsigned parity) {
+  for (int i = 0; i < (1 << 21); ++i) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(tc_smem(b)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+// TMEM: 32 columns per CTA, allocated by warp 0.
+__device__ __forceinline__ void tmem_alloc32(unsigned* dst_smem) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;\n" ::"r"(tc_smem(dst_smem))
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc32(unsigned taddr) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;\n" ::"r"(taddr) : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(unsigned taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Byte offset of element (row, k) in a K-major no-swizzle tile with K = 32 (16-bit elements).
+__device__ __forceinline__ int kmaj_off(int row, int k) {
+  return (row >> 3) * 512 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
+}
+
+template <bool FP16> struct Half;
+template <> struct Half<false> {
+  using H = __nv_bfloat16;
+  __device__ static H from(float v) { return __float2bfloat16_rn(v); }
+  __device__ static float to(H h) { return __bfloat162float(h); }
+};
+template <> struct Half<true> {
+  using H = __half;
+  __device__ static H from(float v) { return __float2half_rn(v); }
+  __device__ static float to(H h) { return __half2float(h); }
+};
+
+// Writes one row (32 values) as hi and lo halves into two K-major tiles.
+template <bool FP16>
+__device__ __forceinline__ void split_row(unsigned char* hi, unsigned char* lo, int row, const float* v) {
+  using HH = Half<FP16>;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    alignas(16) typename HH::H h8[8], l8[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const float x = v[c * 8 + e];
+      h8[e] = HH::from(x);
+      l8[e] = HH::from(x - HH::to(h8[e]));
+    }
+    *reinterpret_cast<uint4*>(hi + kmaj_off(row, c * 8)) = *reinterpret_cast<const uint4*>(h8);
+    *reinterpret_cast<uint4*>(lo + kmaj_off(row, c * 8)) = *reinterpret_cast<const uint4*>(l8);
+  }
+}
+
+// The real 32 x 32 form of the 16-point DFT (sign -1 forward, +1 inverse), hi/lo split.
+template <bool FP16>
+__device__ void build_dft16(unsigned char* Fh, unsigned char* Fl, bool inverse) {
+  for (int o = threadIdx.x; o < 32; o += blockDim.x) {
+    float row[32];
+    const int k = o & 15;
+    const bool im_out = o >= 16;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      double s, c;
+      sincospi((inverse ? 2.0 : -2.0) * (double)((k * m) & 15) / 16.0, &s, &c);
+      // out_re = sum c*re - s*im ; out_im = sum s*re + c*im   (w = c + i s)
+      row[m] = im_out ? (float)s : (float)c;
+      row[16 + m] = im_out ? (float)c : (float)-s;
+    }
+    split_row<FP16>(Fh, Fl, o, row);
+  }
+}
+
+// Self test: D = A * B^T for A (128 x 32) and B (32 x 32) f32 inputs, split like the FFT.
+template <bool FP16>
+__global__ void __launch_bounds__(128) tc_selftest_kernel(const float* A, const float* B, float* D, unsigned* err) {
+  __shared__ __align__(1024) unsigned char Ah[8192], Al[8192], Bh[2048], Bl[2048];
+  __shared__ __align__(8) unsigned long long bar;
+  __shared__ unsigned tslot;
+  const int t = threadIdx.x;
+  if (t < 32) tmem_alloc32(&tslot);
+  if (t == 0) tc_mbar_init(&bar);
+  float v[32];
+  for (int k = 0; k < 32; ++k) v[k] = A[t * 32 + k];
+  split_row<FP16>(Ah, Al, t, v);
+  if (t < 32) {
+    for (int k = 0; k < 32; ++k) v[k] = B[t * 32 + k];
+    split_row<FP16>(Bh, Bl, t, v);
+  }
+  tc_proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned taddr = tslot;
+  if (t == 0) {
+    const uint32_t id = umma_idesc(FP16 ? 0u : 1u);
+    const unsigned char* As[2] = {Ah, Al};
+    const unsigned char* Bs[2] = {Bh, Bl};
+    int first = 1;
+    for (int ai = 0; ai < 2; ++ai)
+      for (int bi = 0; bi < 2; ++bi)
+        for (int ks = 0; ks < 2; ++ks) {
+          tc_mma(taddr, umma_desc(As[ai] + ks * 256), umma_desc(Bs[bi] + ks * 256), id, first ? 0u : 1u);
+          first = 0;
+        }
+    tc_commit(&bar);
+  }
+  const bool ok = tc_mbar_wait(&bar, 0);
+  if (!ok && t == 0) atomicExch(err, 1u);
+  tc_fence_after();
+  float out[32];
+  tmem_ld32(taddr + ((unsigned)((t >> 5) * 32) << 16), out);
+  for (int c = 0; c < 32; ++c) D[t * 32 + c] = out[c];
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (t < 32) tmem_dealloc32(taddr);
+}
+
+// ───────────────────────── tensor-core FFT of 16^s points ─────────────────────────
+// One CTA (128 threads) transforms one lane at a time (persistent over lanes):
+// the lane is loaded into shared memory (f32 complex), each radix-16 stage runs
+// in groups of 128 butterflies through the tensor cores, the last stage's
+// outputs are stored to global memory (scaled for the inverse).
+
+struct TcArgs {
+  const float2* in;
+  float2* out;
+  const float2* tw;   // stage twiddles of the radix-16 plan (same layout as the SIMT plan)
+  StageList sl;
+  long long lanes;
+  float scale;
+  int inverse;
+  unsigned* err;
+};
+
+template <bool FP16>
+__global__ void __launch_bounds__(128) tc_fft_kernel(const __grid_constant__ TcArgs a) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  // layout: Ah 8K | Al 8K | Fh 2K | Fl 2K | bufA n*8 | bufB n*8
+  unsigned char* Ah = smraw;
+  unsigned char* Al = Ah + 8192;
+  unsigned char* Fh = Al + 8192;
+  unsigned char* Fl = Fh + 2048;
+  const int n = a.sl.n;
+  float2* bufA = reinterpret_cast<float2*>(Fl + 2048);
+  float2* bufB = bufA + n;
+  __shared__ __align__(8) unsigned long long bar;
+  __shared__ unsigned tslot;
+  const int t = threadIdx.x;
+  if (t < 32) tmem_alloc32(&tslot);
+  if (t == 0) tc_mbar_init(&bar);
+  build_dft16<FP16>(Fh, Fl, a.inverse != 0);
+  tc_proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned taddr = tslot;
+  const unsigned trow = taddr + ((unsigned)((t >> 5) * 32) << 16);
+  const uint32_t id = umma_idesc(FP16 ? 0u : 1u);
+  unsigned phase = 0;
+  bool failed = false;
+  const int nb = n / 16;
+  for (long long lane = blockIdx.x; lane < a.lanes && !failed; lane += gridDim.x) {
+    const float2* src = a.in + lane * n;
+    for (int i = t; i < n; i += 128) bufA[i] = src[i];
+    __syncthreads();
+    float2* cur = bufA;
+    float2* nxt = bufB;
+    for (int s = 0; s < a.sl.nst && !failed; ++s) {
+      const int Ns = a.sl.st[s].Ns;
+      const float2* tws = a.tw + a.sl.st[s].twoff;
+      const bool last = s == a.sl.nst - 1;
+      for (int g = 0; g < nb; g += 128) {
+        const int j = g + t;
+        const bool have = j < nb;
+        const int k = have ? j % Ns : 0;
+        float v[32];
+        float sc = 1.0f;
+        if (have) {
+#pragma unroll
+          for (int r = 0; r < 16; ++r) {
+            float2 x = cur[j + r * nb];
+            if (Ns > 1 && r > 0) {
+              const float2 w = tws[(long long)k * 15 + r - 1];
+              const float wy = a.inverse ? -w.y : w.y;
+              x = make_float2(x.x * w.x - x.y * wy, x.x * wy + x.y * w.x);
+            }
+            v[r] = x.x;
+            v[16 + r] = x.y;
+          }
+          if (FP16) {  // power-of-two block scale: largest magnitude near 2^11
+            float m = 0.f;
+#pragma unroll
+            for (int r = 0; r < 32; ++r) m = fmaxf(m, fabsf(v[r]));
+            int e = 0;
+            frexpf(m, &e);
+            sc = m > 0.f ? ldexpf(1.0f, 11 - e) : 1.0f;
+#pragma unroll
+            for (int r = 0; r < 32; ++r) v[r] *= sc;
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < 32; ++r) v[r] = 0.f;
+        }
+        split_row<FP16>(Ah, Al, t, v);
+        tc_proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (t == 0) {
+          const unsigned char* As[2] = {Ah, Al};
+          const unsigned char* Bs[2] = {Fh, Fl};
+          int first = 1;
+          for (int ai = 0; ai < 2; ++ai)
+            for (int bi = 0; bi < 2; ++bi)
+              for (int ks = 0; ks < 2; ++ks) {
+                tc_mma(taddr, umma_desc(As[ai] + ks * 256), umma_desc(Bs[bi] + ks * 256), id, first ? 0u : 1u);
+                first = 0;
+              }
+          tc_commit(&bar);
+        }
+        const bool ok = tc_mbar_wait(&bar, phase);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+          if (t == 0) atomicExch(a.err, 1u);
+          failed = true;
+          break;
+        }
+        tc_fence_after();
+        float o[32];
+        tmem_ld32(trow, o);
+        if (have) {
+          const float inv_sc = 1.0f / sc;
+          const int ob = (j - k) * 16 + k;
+#pragma unroll
+          for (int r = 0; r < 16; ++r) {
+            float2 y = make_float2(o[r] * inv_sc, o[16 + r] * inv_sc);
+            if (last) {
+              y.x *= a.scale;
+              y.y *= a.scale;
+              a.out[lane * n + ob + r * Ns] = y;
+            } else {
+              nxt[ob + r * Ns] = y;
+            }
+          }
+        }
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+      }
+      float2* tmp = cur;
+      cur = nxt;
+      nxt = tmp;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (t < 32) tmem_dealloc32(taddr);
+}
+
+cudaError_t launch_tc_selftest(const float* A, const float* B, float* D, unsigned* err, bool fp16, cudaStream_t st) {
+  if (fp16) tc_selftest_kernel<true><<<1, 128, 0, st>>>(A, B, D, err);
+  else tc_selftest_kernel<false><<<1, 128, 0, st>>>(A, B, D, err);
+  count_launch(1);
+  return cudaGetLastError();
+}
+
+size_t tc_fft_smem(int n) { return 8192 * 2 + 2048 * 2 + 2 * (size_t)n * sizeof(float2); }
+
+cudaError_t launch_tc_fft(const TcLaunch& d, bool fp16, cudaStream_t st) {
+  TcArgs a;
+  memset(&a, 0, sizeof(a));
+  a.in = static_cast<const float2*>(d.in);
+  a.out = static_cast<float2*>(d.out);
+  a.tw = static_cast<const float2*>(d.tw);
+  a.sl = d.sl;
+  a.lanes = d.lanes;
+  a.scale = (float)d.scale;
+  a.inverse = d.inverse;
+  a.err = d.err;
+  const size_t smem = tc_fft_smem(d.sl.n);
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  cudaError_t e;
+  int per = 1;
+  if (fp16) {
+    e = cudaFuncSetAttribute(tc_fft_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tc_fft_kernel<true>, 128, smem);
+  } else {
+    e = cudaFuncSetAttribute(tc_fft_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tc_fft_kernel<false>, 128, smem);
+  }
+  if (per < 1) per = 1;
+  // every resident CTA holds 32 TMEM columns; 512 columns per SM
+  if (per > 16) per = 16;
+  long long grid = (long long)sms * per;
+  if (grid > d.lanes) grid = d.lanes;
+  if (fp16) tc_fft_kernel<true><<<(unsigned)grid, 128, smem, st>>>(a);
+  else tc_fft_kernel<false><<<(unsigned)grid, 128, smem, st>>>(a);
+  count_launch(1);
+  return cudaGetLastError();
+}
+
+}  // namespace afc

@@ -14,7 +14,7 @@ import numpy as np
 
 from . import _lib as L
 
-_PREC = {"f32": L.PREC_F32, "f64": L.PREC_F64}
+_PREC = {"f32": L.PREC_F32, "f64": L.PREC_F64, "tc_bf16": L.PREC_TC_BF16, "tc_fp16": L.PREC_TC_FP16}
 _KIND = {"c2c": L.KIND_C2C, "r2c_full": L.KIND_R2C_FULL, "r2c_half": L.KIND_R2C_HALF}
 
 
@@ -25,7 +25,7 @@ class CudaPlan:
                  device: int = 0, cached: bool = True):
         dims = [int(d) for d in dims]
         if precision not in _PREC:
-            raise ValueError(f"unsupported precision `{precision}`; expected f32 or f64")
+            raise ValueError(f"unsupported precision `{precision}`; expected f32, f64, tc_bf16 or tc_fp16")
         if kind not in _KIND:
             raise ValueError(f"unsupported kind `{kind}`; expected c2c, r2c_full or r2c_half")
         self.dims = tuple(dims)
@@ -65,7 +65,7 @@ class CudaPlan:
         return np.float64 if self.precision == "f64" else np.float32
 
     def _cplx_dtype(self):
-        return np.complex128 if self.precision == "f64" else np.complex64
+        return np.complex128 if self.precision == "f64" else np.complex64  # tensor-core plans use complex64
 
     def in_dtype(self, inverse: bool):
         if self.kind == "c2c" or inverse:
