@@ -49,6 +49,8 @@ def test_validation_errors(afc):
     st, _ = _create(afc, 1, [8], batch=0)
     assert st == L.AFC_ERR_VALIDATION
     st, _ = _create(afc, 1, [8], prec=7)
+    assert st == L.AFC_ERR_VALIDATION and "precision" in L.last_error()
+    st, _ = _create(afc, 2, [16, 16], prec=L.PREC_TC_FP16)  # tensor-core plans: rank-1, n = 16^s
     assert st == L.AFC_ERR_UNSUPPORTED
     assert afc._lib.lib().afc_execute(None, None, None, 0, None) == L.AFC_ERR_VALIDATION
 
