@@ -1355,7 +1355,7 @@ static afc_status build_phases(afc_batch_plan_s& bp, bool inv, cudaStream_t st) 
       const long long tiles = (rl.d.lanes + rl.d.L - 1) / rl.d.L;
       const double c = (double)rl.d.sl.n * std::max(1, rl.d.sl.nst) * (rl.kind ? 2.0 : 1.0) * rl.d.L;
       for (long long t = 0; t < tiles; ++t) {
-        pa.items.push_back(BatchItem{di, rl.kind, t * rl.d.L});
+        pa.items.push_back(BatchItem{di, rl.kind == 1 ? 1 : (rl.inv ? 2 : 0), t * rl.d.L});
         pa.cost.push_back(c);
       }
     }

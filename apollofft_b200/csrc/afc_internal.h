@@ -40,8 +40,8 @@ struct LaunchDesc {
   int in_sel = 0, out_sel = 0;  // batch descriptors: pointer = base[sel] + offset
 };
 
-// A tile of the persistent batch kernel: descriptor index, kind (0 lanes tile,
-// 1 convolution tile) and first lane.
+// A tile of the persistent batch kernel: descriptor index, kind (0 forward lanes
+// tile, 1 convolution tile, 2 inverse lanes tile) and first lane.
 struct BatchItem {
   int desc;
   int kind;

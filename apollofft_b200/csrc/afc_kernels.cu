@@ -473,11 +473,12 @@ __global__ void __launch_bounds__(512) conv_kernel(const __grid_constant__ KArgs
 // ───────────────────────── persistent batch kernel ─────────────────────────
 // One launch runs a whole phase of an uneven batch: a list of tiles, each a
 // lanes tile or a convolution tile of some transform length, described by a
-// KArgs record in global memory.  CTAs fetch tiles from an atomic counter
+// KArgs record in global memory (kind 0 forward lanes, 2 inverse lanes, 1
+// convolution: a phase can mix directions).  CTAs fetch tiles from an atomic counter
 // (longest tiles first), copy the record into shared memory, resolve its
 // buffer selectors against this launch's bases and run the tile.
 
-template <class T, bool INV>
+template <class T>
 __global__ void __launch_bounds__(128) batch_kernel(const KArgs<T>* __restrict__ descs, const BatchItem* __restrict__ items,
                                                    int nitems, int* counter, const void* in_base, void* out_base,
                                                    void* ws_base) {
@@ -501,7 +502,8 @@ __global__ void __launch_bounds__(128) batch_kernel(const KArgs<T>* __restrict__
       if (ka.out_sel) ka.out = bases[ka.out_sel] + (size_t)ka.out;
     }
     __syncthreads();
-    if (bi.kind == 0) lanes_tile<T, INV>(ka, bi.q0, smraw);
+    if (bi.kind == 0) lanes_tile<T, false>(ka, bi.q0, smraw);
+    else if (bi.kind == 2) lanes_tile<T, true>(ka, bi.q0, smraw);
     else conv_tile<T>(ka, bi.q0, smraw);
     __syncthreads();
   }
@@ -719,10 +721,10 @@ void kargs_pack(const LaunchDesc& d, bool dbl, void* dst) {
   }
 }
 
-template <class T, bool INV>
+template <class T>
 static cudaError_t launch_batch_t(const void* descs, const BatchItem* items, int nitems, int* counter, size_t smem,
                                   int grid, const void* in, void* out, void* ws, cudaStream_t st) {
-  auto k = batch_kernel<T, INV>;
+  auto k = batch_kernel<T>;
   cudaError_t e = prep_smem(k, smem);
   if (e != cudaSuccess) return e;
   k<<<grid, 128, smem, st>>>(static_cast<const KArgs<T>*>(descs), items, nitems, counter, in, out, ws);
@@ -733,21 +735,20 @@ static cudaError_t launch_batch_t(const void* descs, const BatchItem* items, int
 cudaError_t launch_batch(const void* descs, const BatchItem* items, int nitems, int* counter, size_t smem, int grid,
                          const void* in, void* out, void* ws, bool dbl, bool inv, cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
-  if (dbl)
-    return inv ? launch_batch_t<double, true>(descs, items, nitems, counter, smem, grid, in, out, ws, st)
-               : launch_batch_t<double, false>(descs, items, nitems, counter, smem, grid, in, out, ws, st);
-  return inv ? launch_batch_t<float, true>(descs, items, nitems, counter, smem, grid, in, out, ws, st)
-             : launch_batch_t<float, false>(descs, items, nitems, counter, smem, grid, in, out, ws, st);
+  (void)inv;
+  if (dbl) return launch_batch_t<double>(descs, items, nitems, counter, smem, grid, in, out, ws, st);
+  return launch_batch_t<float>(descs, items, nitems, counter, smem, grid, in, out, ws, st);
 }
 
 int batch_blocks_per_sm(size_t smem, bool dbl, bool inv) {
+  (void)inv;
   int per = 1;
   if (dbl) {
-    if (inv) { prep_smem(batch_kernel<double, true>, smem); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<double, true>, 128, smem); }
-    else { prep_smem(batch_kernel<double, false>, smem); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<double, false>, 128, smem); }
+    prep_smem(batch_kernel<double>, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<double>, 128, smem);
   } else {
-    if (inv) { prep_smem(batch_kernel<float, true>, smem); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<float, true>, 128, smem); }
-    else { prep_smem(batch_kernel<float, false>, smem); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<float, false>, 128, smem); }
+    prep_smem(batch_kernel<float>, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<float>, 128, smem);
   }
   return per < 1 ? 1 : per;
 }

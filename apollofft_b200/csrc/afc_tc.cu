@@ -213,9 +213,14 @@ struct TcArgs {
 
 template <bool FP16>
 __global__ void __launch_bounds__(128) tc_fft_kernel(const __grid_constant__ TcArgs a) {
-  extern __shared__ __align__(1024) unsigned char smraw[];
-  // layout: Ah 8K | Al 8K | Fh 2K | Fl 2K | bufA n*8 | bufB n*8
-  unsigned char* Ah = smraw;
+  // Declared 16-byte aligned on purpose: with separately compiled device code
+  // the dynamic block starts at any 16-byte boundary after the static
+  // variables (0x410 here), whatever alignment the declaration claims, and a
+  // larger claimed alignment lets the compiler fold the padding below to zero.
+  // Operand tiles off a 1024-byte boundary read back wrong in the MMA.
+  extern __shared__ __align__(16) unsigned char smraw[];
+  // layout from the first 1024-byte boundary: Ah 8K | Al 8K | Fh 2K | Fl 2K | bufA n*8 | bufB n*8
+  unsigned char* Ah = smraw + ((1024u - (tc_smem(smraw) & 1023u)) & 1023u);
   unsigned char* Al = Ah + 8192;
   unsigned char* Fh = Al + 8192;
   unsigned char* Fl = Fh + 2048;
@@ -344,7 +349,7 @@ cudaError_t launch_tc_selftest(const float* A, const float* B, float* D, unsigne
   return cudaGetLastError();
 }
 
-size_t tc_fft_smem(int n) { return 8192 * 2 + 2048 * 2 + 2 * (size_t)n * sizeof(float2); }
+size_t tc_fft_smem(int n) { return 1024 + 8192 * 2 + 2048 * 2 + 2 * (size_t)n * sizeof(float2); }
 
 cudaError_t launch_tc_fft(const TcLaunch& d, bool fp16, cudaStream_t st) {
   TcArgs a;
