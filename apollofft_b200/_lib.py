@@ -115,6 +115,8 @@ def lib():
         L.afc_test_tc_tile.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.afc_test_take_device_error.restype = ctypes.c_int
         L.afc_test_take_device_error.argtypes = []
+        L.afc_test_bounded_wait.restype = ctypes.c_int
+        L.afc_test_bounded_wait.argtypes = [ctypes.c_int]
         _lib = L
     return _lib
 

@@ -1878,6 +1878,20 @@ AFC_API afc_status afc_test_take_device_error(void) {
   return AFC_OK;
 }
 
+// Runs one bounded wait that nothing completes (a barrier with no arrival), so
+// the timeout path can be tested without a fault: the wait gives up after
+// `polls` polls, the kernel returns, and the result is read back through the
+// error word like any kernel timeout (AFC_ERR_TIMEOUT).
+AFC_API afc_status afc_test_bounded_wait(int polls) {
+  if (polls < 1 || polls > (1 << 21))
+    return fail(AFC_ERR_VALIDATION, "validation failed for `polls`: `%d` violates `1..2^21`", polls);
+  unsigned* w = device_err_word();
+  if (!w) return fail(AFC_ERR_OUT_OF_MEMORY, "error word");
+  cudaError_t e = launch_wait_probe(w, polls, 0);
+  if (e != cudaSuccess) return cuda_fail(e, "wait probe");
+  return afc_test_take_device_error();
+}
+
 AFC_API void afc_test_fail_next_allocs(int count) { g_fail_allocs.store(count); }
 
 }  // extern "C"

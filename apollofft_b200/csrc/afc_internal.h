@@ -87,6 +87,7 @@ struct TcLaunch {
   unsigned* err = nullptr;
 };
 cudaError_t launch_tc_fft(const TcLaunch& d, bool fp16, cudaStream_t st);
+cudaError_t launch_wait_probe(unsigned* err, int polls, cudaStream_t st);
 cudaError_t launch_tc_selftest(const float* A, const float* B, float* D, unsigned* err, bool fp16, cudaStream_t st);
 size_t tc_fft_smem(int n);
 

@@ -61,10 +61,22 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned pa
 }
 // Bounded wait: about 2^21 polls (each try_wait itself suspends for a while),
 // a few seconds at most; false on timeout.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity) {
-  for (int i = 0; i < (1 << 21); ++i)
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity, int limit = 1 << 21) {
+  for (int i = 0; i < limit; ++i)
     if (mbar_try_wait(b, parity)) return true;
   return false;
+}
+
+// Exercises the timeout path of the bounded wait: one thread waits on a
+// barrier that nothing arrives on, gives up after `polls` polls and records the
+// timeout in the error word, exactly as the transform kernels do.
+__global__ void wait_probe_kernel(unsigned* err, int polls) {
+  __shared__ __align__(8) unsigned long long bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    if (!mbar_wait(&bar, 0, polls)) atomicExch(err, 1u);
+  }
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
@@ -389,6 +401,12 @@ cudaError_t launch_tma(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, bo
   if (d.lanes <= 0) return cudaSuccess;
   if (dbl) return inv ? launch_tma_t<double, true>(d, tp, err, st) : launch_tma_t<double, false>(d, tp, err, st);
   return inv ? launch_tma_t<float, true>(d, tp, err, st) : launch_tma_t<float, false>(d, tp, err, st);
+}
+
+cudaError_t launch_wait_probe(unsigned* err, int polls, cudaStream_t st) {
+  wait_probe_kernel<<<1, 32, 0, st>>>(err, polls);
+  count_launch(1);
+  return cudaGetLastError();
 }
 
 }  // namespace afc
