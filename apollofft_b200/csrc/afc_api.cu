@@ -433,7 +433,7 @@ struct RecLaunch {
 };
 struct Recorder {
   std::vector<RecLaunch> launches;
-  int max_threads = 128;
+  int max_threads = kBatchThreads;
 };
 static thread_local Recorder* tl_rec = nullptr;
 
@@ -1230,7 +1230,7 @@ static cudaError_t run_batch_persistent(afc_batch_plan_s& bp, const void* in, vo
 
 // Autotuner: for each distinct smem-resident length, time the lanes kernel on a
 // scratch buffer for a few threads-per-lane / lanes-per-tile shapes (tiles run
-// on the 128-thread persistent kernel) and keep the fastest.  Results are
+// on the persistent kernel's kBatchThreads-thread CTAs) and keep the fastest.  Results are
 // cached per (length, precision) for the process.
 static std::mutex g_tune_mu;
 static std::map<std::pair<int64_t, int>, std::pair<int, int>> g_tune;
@@ -1253,7 +1253,8 @@ static void tune_group(BatchGroup& g, bool dbl, void* scratch, cudaStream_t st) 
   for (int s2 = 0; s2 < ap.lp.sl.nst; ++s2) rmax = std::max(rmax, ap.lp.sl.st[s2].R);
   std::vector<int> cands;
   for (int div : {1, 2, 4, 8}) {
-    int P = (int)std::min<int64_t>(128, std::max<int64_t>(1, (g.n + (int64_t)rmax * div - 1) / ((int64_t)rmax * div)));
+    int P = (int)std::min<int64_t>(kBatchThreads,
+                                   std::max<int64_t>(1, (g.n + (int64_t)rmax * div - 1) / ((int64_t)rmax * div)));
     if (std::find(cands.begin(), cands.end(), P) == cands.end()) cands.push_back(P);
   }
   const long long lanes = std::max(1LL, std::min<long long>(g.lanes * 4, 64));
@@ -1274,7 +1275,7 @@ static void tune_group(BatchGroup& g, bool dbl, void* scratch, cudaStream_t st) 
     d.in = scratch;
     d.out = scratch;
     const size_t per_lane = 2 * (size_t)d.ld * csz + 3 * sizeof(long long);
-    int L = std::max(1, 128 / P);
+    int L = std::max(1, kBatchThreads / P);
     while (L > 1 && (size_t)L * per_lane > 100 * 1024) --L;
     d.L = L;
     d.stage_out = ap.lp.sl.nst <= 1;

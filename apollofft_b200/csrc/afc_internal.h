@@ -94,6 +94,8 @@ size_t tc_fft_smem(int n);
 cudaError_t launch_lanes(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st);
 size_t kargs_size(bool dbl);
 void kargs_pack(const LaunchDesc& d, bool dbl, void* dst);
+// Threads of a persistent batch CTA (a tile uses at most this many).
+constexpr int kBatchThreads = 256;
 cudaError_t launch_batch(const void* descs, const BatchItem* items, int nitems, int* counter, size_t smem, int grid,
                          const void* in, void* out, void* ws, bool dbl, bool inv, cudaStream_t st);
 int batch_blocks_per_sm(size_t smem, bool dbl, bool inv);

@@ -479,7 +479,7 @@ __global__ void __launch_bounds__(512) conv_kernel(const __grid_constant__ KArgs
 // buffer selectors against this launch's bases and run the tile.
 
 template <class T>
-__global__ void __launch_bounds__(128) batch_kernel(const KArgs<T>* __restrict__ descs, const BatchItem* __restrict__ items,
+__global__ void __launch_bounds__(kBatchThreads, 2) batch_kernel(const KArgs<T>* __restrict__ descs, const BatchItem* __restrict__ items,
                                                    int nitems, int* counter, const void* in_base, void* out_base,
                                                    void* ws_base) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -727,7 +727,7 @@ static cudaError_t launch_batch_t(const void* descs, const BatchItem* items, int
   auto k = batch_kernel<T>;
   cudaError_t e = prep_smem(k, smem);
   if (e != cudaSuccess) return e;
-  k<<<grid, 128, smem, st>>>(static_cast<const KArgs<T>*>(descs), items, nitems, counter, in, out, ws);
+  k<<<grid, kBatchThreads, smem, st>>>(static_cast<const KArgs<T>*>(descs), items, nitems, counter, in, out, ws);
   count_launch(1);
   return cudaGetLastError();
 }
@@ -745,10 +745,10 @@ int batch_blocks_per_sm(size_t smem, bool dbl, bool inv) {
   int per = 1;
   if (dbl) {
     prep_smem(batch_kernel<double>, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<double>, 128, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<double>, kBatchThreads, smem);
   } else {
     prep_smem(batch_kernel<float>, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<float>, 128, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<float>, kBatchThreads, smem);
   }
   return per < 1 ? 1 : per;
 }

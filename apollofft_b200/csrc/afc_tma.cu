@@ -175,8 +175,11 @@ __device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long t
   bulk_commit();
 }
 
-template <class T, bool INV>
-__global__ void __launch_bounds__(256) tma_kernel(const __grid_constant__ TmaArgs<T> a) {
+// P2: every stage has a power-of-two radix (2, 4, 8, 16).  That variant carries
+// no odd-radix butterflies, needs fewer registers and is built for two
+// resident CTAs per SM (at most 128 registers a thread).
+template <class T, bool INV, bool P2>
+__global__ void __launch_bounds__(256, (P2 && sizeof(T) == 4) ? 2 : 1) tma_kernel(const __grid_constant__ TmaArgs<T> a) {
   using C = typename CT<T>::type;
   extern __shared__ __align__(128) unsigned char smraw[];
   const int L = a.L, P = a.P, n = a.sl.n, ld = a.ld;
@@ -231,17 +234,27 @@ __global__ void __launch_bounds__(256) tma_kernel(const __grid_constant__ TmaArg
       const TView<C> dst = last ? olin : ((s & 1) ? cpad : wv);
       const C* twi = a.tw + sd.twoff;
 #define AFC_TM(R) tma_stage<R, INV>(src, dst, l, n, sd.Ns, twi, t, P, last, a.scale)
-      switch (sd.R) {
-        case 2: AFC_TM(2); break;
-        case 3: AFC_TM(3); break;
-        case 4: AFC_TM(4); break;
-        case 5: AFC_TM(5); break;
-        case 7: AFC_TM(7); break;
-        case 8: AFC_TM(8); break;
-        case 11: AFC_TM(11); break;
-        case 13: AFC_TM(13); break;
-        case 16: AFC_TM(16); break;
-        default: break;
+      if constexpr (P2) {
+        switch (sd.R) {
+          case 2: AFC_TM(2); break;
+          case 4: AFC_TM(4); break;
+          case 8: AFC_TM(8); break;
+          case 16: AFC_TM(16); break;
+          default: break;
+        }
+      } else {
+        switch (sd.R) {
+          case 2: AFC_TM(2); break;
+          case 3: AFC_TM(3); break;
+          case 4: AFC_TM(4); break;
+          case 5: AFC_TM(5); break;
+          case 7: AFC_TM(7); break;
+          case 8: AFC_TM(8); break;
+          case 11: AFC_TM(11); break;
+          case 13: AFC_TM(13); break;
+          case 16: AFC_TM(16); break;
+          default: break;
+        }
       }
 #undef AFC_TM
       __syncthreads();
@@ -354,7 +367,12 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
 template <class T, bool INV>
 static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, cudaStream_t st) {
   using C = typename CT<T>::type;
-  auto k = tma_kernel<T, INV>;
+  bool p2 = true;
+  for (int i = 0; i < d.sl.nst; ++i) {
+    const int R = d.sl.st[i].R;
+    p2 = p2 && (R == 2 || R == 4 || R == 8 || R == 16);
+  }
+  auto k = p2 ? tma_kernel<T, INV, true> : tma_kernel<T, INV, false>;
   const size_t smem = tma_smem_bytes(tp, sizeof(C));
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

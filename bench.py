@@ -275,7 +275,8 @@ def main():
     tf = os.path.join(ROOT, "profiles", "tma_kernel_traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get("bytes_per_launch_256cube_f64") if SHAPE == (256, 256, 256) else None
+            traffic = (json.load(open(tf)).get("bytes_per_launch_256cube_f64")
+                       if SHAPE == (256, 256, 256) and prec == "f64" else None)
         except (ValueError, OSError):
             traffic = None
 
@@ -346,7 +347,7 @@ def main():
                        "l2": "inputs (268 MB) larger than L2; no flush"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                          "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
-                         "kernel": "tma_kernel<double> (all launches of the step)",
+                         "kernel": f"tma_kernel<{'double' if prec == 'f64' else 'float'}> (all launches of the step)",
                          "peak_source": peak_kind},
             "transform_hbm_frac": round(transform_frac, 4),
             "error_vs_oracle_rel_l2": err_oracle,
