@@ -33,7 +33,7 @@ constexpr int kMaxStages = 24;
 struct StageDesc {
   int R;
   int Ns;
-  int twoff;  // offset (in complex elements) of this stage's twiddles
+  int twoff;  // offset (in complex elements) of this stage's twiddles, stored r-major: [(r-1) Ns + k]
 };
 
 struct StageList {
@@ -89,10 +89,9 @@ __device__ __forceinline__ void stage(const Ctx& cx, const C* __restrict__ src, 
     for (int r = 0; r < R; ++r) v[r] = src ? src[spad(j + r * nb)] : cx.gload(j + r * nb);
     const int k = j % Ns;
     if (Ns > 1) {
-      const C* w = tw + (long long)k * (R - 1);
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        const C wr = w[r - 1];
+        const C wr = tw[(long long)(r - 1) * Ns + k];
         v[r] = INV ? cmulc(v[r], wr) : cmul(v[r], wr);
       }
     }

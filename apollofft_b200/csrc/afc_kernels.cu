@@ -275,10 +275,9 @@ __device__ __forceinline__ void tstage(const KArgs<T>& a, SView<typename CT<T>::
     for (int r = 0; r < R; ++r) v[r] = src.at(l, j + r * nb);
     const int k = j % Ns;
     if (Ns > 1) {
-      const C* w = tw + (long long)k * (R - 1);
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        const C wr = w[r - 1];
+        const C wr = tw[(long long)(r - 1) * Ns + k];
         v[r] = INV ? cmulc(v[r], wr) : cmul(v[r], wr);
       }
     }
@@ -511,7 +510,8 @@ __global__ void __launch_bounds__(kBatchThreads, 2) batch_kernel(const KArgs<T>*
 
 // ────────────────────────────── table kernels ──────────────────────────────
 
-// Stage twiddles: tw[off + k(R-1) + r-1] = exp(-2 pi i (r k mod NsR) / (NsR)).
+// Stage twiddles: tw[off + (r-1) Ns + k] = exp(-2 pi i (r k mod NsR) / (NsR)), r-major so
+// that the butterflies of consecutive threads (consecutive k) read consecutive entries.
 template <class T>
 __global__ void gen_stage_twiddles(typename CT<T>::type* tw, StageList sl) {
   using C = typename CT<T>::type;
@@ -521,7 +521,7 @@ __global__ void gen_stage_twiddles(typename CT<T>::type* tw, StageList sl) {
     const long long cnt = (long long)Ns * (R - 1);
     const long long Lr = (long long)Ns * R;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < cnt; e += (long long)gridDim.x * blockDim.x) {
-      const long long k = e / (R - 1), r = e % (R - 1) + 1;
+      const long long r = e / Ns + 1, k = e % Ns;
       const long long m = (r * k) % Lr;
       double sn, cs;
       sincospi(-2.0 * (double)m / (double)Lr, &sn, &cs);

@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(128) tc_fft_kernel(const __grid_constant__ TcA
           for (int r = 0; r < 16; ++r) {
             float2 x = cur[j + r * nb];
             if (Ns > 1 && r > 0) {
-              const float2 w = tws[(long long)k * 15 + r - 1];
+              const float2 w = tws[(long long)(r - 1) * Ns + k];
               const float wy = a.inverse ? -w.y : w.y;
               x = make_float2(x.x * w.x - x.y * wy, x.x * wy + x.y * w.x);
             }

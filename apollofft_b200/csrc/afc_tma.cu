@@ -123,10 +123,9 @@ __device__ __forceinline__ void tma_stage(TView<C> src, TView<C> dst, int l, int
     for (int r = 0; r < R; ++r) v[r] = src.at(l, j + r * nb);
     const int k = j % Ns;
     if (Ns > 1) {
-      const C* w = tw + (long long)k * (R - 1);
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        const C wr = w[r - 1];
+        const C wr = tw[(long long)(r - 1) * Ns + k];
         v[r] = INV ? cmulc(v[r], wr) : cmul(v[r], wr);
       }
     }
