@@ -69,6 +69,12 @@ struct TmaPlan {
   int L = 1, P = 1, ld = 1, slot_elems = 0;
   int nbx = 1, bn = 1;
   long long kb = 1, ntiles = 0, outer = 0;
+  // every stage has at most P butterflies per lane: stages run in place in the
+  // tile's slot (registers hold the butterfly across a barrier), no work buffer
+  bool inplace = false;
+  // kernel build: 0 any radix (256 threads), 1 radix 2/4/8/16 (256 threads),
+  // 2 radix 2/4/8/16 complex128 at <= 128 threads, three CTAs per SM
+  int variant = 0;
 };
 bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, const LaneMap& om, const void* in,
               void* out, bool dbl, int lanes_pref, TmaPlan& tp);

@@ -18,6 +18,7 @@
 // the previous stage did not use; that buffer is the TMA store's source.
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <cstdlib>
 #include <cstring>
 #include "afc_engine.cuh"
 #include "afc_internal.h"
@@ -37,6 +38,7 @@ template <class T> struct TmaArgs {
   long long kb;     // strided: lane blocks per outer index, ceil(es / L)
   int L, P, ld, slot_elems;
   int mode;         // 0 contiguous (1D bulk), 1 strided (tensor)
+  int inplace;      // stages run in place in the slot (no work buffer)
   int nbx, bn;      // boxes along the transformed axis, rows per box
   T scale;
   unsigned* err;
@@ -136,6 +138,39 @@ __device__ __forceinline__ void tma_stage(TView<C> src, TView<C> dst, int l, int
   }
 }
 
+// One stage in place: every thread owns at most one butterfly of its lane
+// (n / R <= P).  All reads of the stage finish before the barrier, all writes
+// come after it, so source and destination may share the slot.  Every thread
+// of the CTA reaches the barrier.
+template <int R, bool INV, class C, class S>
+__device__ __forceinline__ void tma_stage_inplace(TView<C> src, TView<C> dst, int l, int n, int Ns,
+                                                  const C* __restrict__ tw, int t, bool scale_out, S sc) {
+  const int nb = n / R;
+  const int j = t;
+  const bool have = j < nb;
+  C v[R];
+  int k = 0;
+  if (have) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src.at(l, j + r * nb);
+  }
+  __syncthreads();
+  if (have) {
+    k = j % Ns;
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const C wr = tw[(long long)(r - 1) * Ns + k];
+        v[r] = INV ? cmulc(v[r], wr) : cmul(v[r], wr);
+      }
+    }
+    DFT<R, INV>::run(v);
+    const int o = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst.at(l, o + r * Ns) = scale_out ? cscale(v[r], sc) : v[r];
+  }
+}
+
 template <class T>
 __device__ __forceinline__ void tma_issue_load(const TmaArgs<T>& a, long long tile, typename CT<T>::type* slot,
                                                unsigned long long* bar) {
@@ -174,20 +209,25 @@ __device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long t
   bulk_commit();
 }
 
-// P2: every stage has a power-of-two radix (2, 4, 8, 16).  That variant carries
-// no odd-radix butterflies, needs fewer registers and is built for two
-// resident CTAs per SM (at most 128 registers a thread).
-template <class T, bool INV, bool P2>
-__global__ void __launch_bounds__(256, (P2 && sizeof(T) == 4) ? 2 : 1) tma_kernel(const __grid_constant__ TmaArgs<T> a) {
+// V (variant): 0 any radix, 256 threads; 1 every stage radix 2/4/8/16 (no
+// odd-radix butterflies, fewer registers; complex64 built for two CTAs per
+// SM); 2 the same for complex128 tiles of at most 128 threads, built for three
+// CTAs per SM (at most 168 registers).
+// IP: stages run in place (TmaPlan::inplace); variant 2 is always in place.
+template <class T, bool INV, int V, bool IP>
+__global__ void __launch_bounds__(V == 2 ? 128 : 256, V == 2 ? 3 : ((V == 1 && sizeof(T) == 4) ? 2 : 1))
+    tma_kernel(const __grid_constant__ TmaArgs<T> a) {
+  constexpr bool P2 = V != 0;
   using C = typename CT<T>::type;
   extern __shared__ __align__(128) unsigned char smraw[];
   const int L = a.L, P = a.P, n = a.sl.n, ld = a.ld;
   C* slots[2];
   slots[0] = reinterpret_cast<C*>(smraw);
   slots[1] = slots[0] + a.slot_elems;
-  C* work = slots[1] + a.slot_elems;
+  C* work = IP ? nullptr : slots[1] + a.slot_elems;
+  C* end = IP ? slots[1] + a.slot_elems : work + (long long)L * ld;
   unsigned long long* bars =
-      reinterpret_cast<unsigned long long*>(reinterpret_cast<uintptr_t>(work + (long long)L * ld + 1) & ~(uintptr_t)7);
+      reinterpret_cast<unsigned long long*>(reinterpret_cast<uintptr_t>(end + 1) & ~(uintptr_t)7);
   const bool lm = a.mode == 1;
   const int tid = threadIdx.x;
   const int l = lm ? tid % L : tid / P;
@@ -224,9 +264,41 @@ __global__ void __launch_bounds__(256, (P2 && sizeof(T) == 4) ? 2 : 1) tma_kerne
     const TView<C> lin = lm ? TView<C>{cur, 1, L, 0} : TView<C>{cur, n, 1, 0};
     const TView<C> cpad{cur, ld, 1, 1};
     // output buffer (linear layout): the one the last stage does not read
-    C* obuf = (nst & 1) ? work : cur;
+    C* obuf = (IP || !(nst & 1)) ? cur : work;
     const TView<C> olin = lm ? TView<C>{obuf, 1, L, 0} : TView<C>{obuf, n, 1, 0};
-    for (int s = 0; s < nst; ++s) {
+    for (int s = 0; IP && s < nst; ++s) {
+      const StageDesc sd = a.sl.st[s];
+      const bool last = s == nst - 1;
+      const TView<C> src = s == 0 ? lin : cpad;
+      const TView<C> dst = last ? olin : cpad;
+      const C* twi = a.tw + sd.twoff;
+#define AFC_TI(R) tma_stage_inplace<R, INV>(src, dst, l, n, sd.Ns, twi, t, last, a.scale)
+      if constexpr (P2) {
+        switch (sd.R) {
+          case 2: AFC_TI(2); break;
+          case 4: AFC_TI(4); break;
+          case 8: AFC_TI(8); break;
+          case 16: AFC_TI(16); break;
+          default: break;
+        }
+      } else {
+        switch (sd.R) {
+          case 2: AFC_TI(2); break;
+          case 3: AFC_TI(3); break;
+          case 4: AFC_TI(4); break;
+          case 5: AFC_TI(5); break;
+          case 7: AFC_TI(7); break;
+          case 8: AFC_TI(8); break;
+          case 11: AFC_TI(11); break;
+          case 13: AFC_TI(13); break;
+          case 16: AFC_TI(16); break;
+          default: break;
+        }
+      }
+#undef AFC_TI
+      __syncthreads();
+    }
+    for (int s = 0; !IP && s < nst; ++s) {
       const StageDesc sd = a.sl.st[s];
       const bool last = s == nst - 1;
       const TView<C> src = s == 0 ? lin : ((s & 1) ? wv : cpad);
@@ -305,7 +377,7 @@ static bool make_map(CUtensorMap* m, const void* base, bool dbl, long long es, l
 static int g_tma_sm = 0;
 
 size_t tma_smem_bytes(const TmaPlan& tp, size_t csz) {
-  return 2 * (size_t)tp.slot_elems * csz + (size_t)tp.L * tp.ld * csz + 64;
+  return 2 * (size_t)tp.slot_elems * csz + (tp.inplace ? 0 : (size_t)tp.L * tp.ld * csz) + 64;
 }
 
 // Decides whether an axis pass can run on the TMA kernel and with which tiles.
@@ -339,12 +411,31 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
   tp.ld = ld;
   // threads: one radix-16 butterfly per thread and stage when possible
   int P = (int)std::max<long long>(1, std::min<long long>(256, (n + 15) / 16));
+  bool p2 = true;
+  for (int i = 0; i < sl.nst; ++i) {
+    const int R = sl.st[i].R;
+    p2 = p2 && (R == 2 || R == 4 || R == 8 || R == 16);
+  }
+  // complex128 power-of-two tiles of <= 128 threads whose stages run in place
+  // (one butterfly per thread) use the three-CTA build
+  bool ip128 = P <= 128;
+  for (int i = 0; i < sl.nst; ++i) ip128 = ip128 && n / sl.st[i].R <= P;
+  static const int v2_on = [] {
+    const char* e = getenv("AFC_TMA_V2");
+    return e && *e ? atoi(e) : 1;
+  }();
+  const int tmax = (v2_on && dbl && p2 && ip128) ? 128 : 256;
   if (tp.mode == 0) {
-    int L = std::max(1, 256 / P);
+    int L = std::max(1, tmax / P);
     tp.L = L;
   }
-  while (tp.L * P > 256) P = std::max(1, P / 2);
+  while (tp.L * P > tmax) P = std::max(1, P / 2);
   tp.P = P;
+  tp.variant = !p2 ? 0 : (tmax == 128 ? 2 : 1);
+  // in place only for power-of-two plans: odd-radix butterflies held across
+  // the barrier cost spills
+  tp.inplace = p2;
+  for (int i = 0; i < sl.nst; ++i) tp.inplace = tp.inplace && n / sl.st[i].R <= P;
   const int align = dbl ? 8 : 16;  // 128-byte aligned slots
   long long rows = tp.mode == 1 ? (long long)tp.nbx * tp.bn : n;
   long long se = (long long)tp.L * std::max<long long>(ld, rows);
@@ -366,12 +457,9 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
 template <class T, bool INV>
 static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, cudaStream_t st) {
   using C = typename CT<T>::type;
-  bool p2 = true;
-  for (int i = 0; i < d.sl.nst; ++i) {
-    const int R = d.sl.st[i].R;
-    p2 = p2 && (R == 2 || R == 4 || R == 8 || R == 16);
-  }
-  auto k = p2 ? tma_kernel<T, INV, true> : tma_kernel<T, INV, false>;
+  auto k = tp.variant == 2  ? tma_kernel<T, INV, 2, true>
+           : tp.variant == 1 ? (tp.inplace ? tma_kernel<T, INV, 1, true> : tma_kernel<T, INV, 1, false>)
+                             : tma_kernel<T, INV, 0, false>;
   const size_t smem = tma_smem_bytes(tp, sizeof(C));
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -394,6 +482,7 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
   a.ld = tp.ld;
   a.slot_elems = tp.slot_elems;
   a.mode = tp.mode;
+  a.inplace = tp.inplace ? 1 : 0;
   a.nbx = tp.nbx;
   a.bn = tp.bn;
   a.scale = (T)d.scale;
