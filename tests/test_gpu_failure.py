@@ -34,3 +34,31 @@ def test_bounded_wait_rejects_bad_limits(afc, cuda):
     L = afc._lib.lib()
     assert L.afc_test_bounded_wait(0) == AFC_ERR_VALIDATION
     assert L.afc_test_bounded_wait(1 << 22) == AFC_ERR_VALIDATION
+
+
+AFC_ERR_OUT_OF_MEMORY = 6
+
+
+@pytest.mark.parametrize("dims", [[4096], [97], [20011], [64, 48, 40]])
+def test_allocation_failure_reports_out_of_memory(afc, cuda, dims):
+    """A failed device allocation during plan build (twiddles, Rader/Bluestein
+    tables, workspaces) comes back as AFC_ERR_OUT_OF_MEMORY, and the next plan
+    builds and runs normally."""
+    L = afc._lib.lib()
+    for k in (1, 2, 3):
+        L.afc_test_fail_next_allocs(k)
+        try:
+            afc.CudaPlan(dims, precision="f64", cached=False)
+            built = True
+        except afc.AfcError as e:
+            built = False
+            assert e.status == AFC_ERR_OUT_OF_MEMORY, (e.status, str(e))
+        finally:
+            L.afc_test_fail_next_allocs(0)
+        if built:
+            break  # the plan needs fewer than k allocations: nothing left to fail
+    rng = np.random.default_rng(3)
+    x = (rng.standard_normal(dims) + 1j * rng.standard_normal(dims)).astype(np.complex128)
+    p = afc.CudaPlan(dims, precision="f64", cached=False)
+    y = p.execute(torch.from_numpy(x).cuda()).cpu().numpy()
+    assert rel_l2(y, np.fft.fftn(x)) < 1e-12
