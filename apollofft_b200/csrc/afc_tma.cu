@@ -214,10 +214,13 @@ __device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long t
 // SM); 2 the same for complex128 tiles of at most 128 threads, built for three
 // CTAs per SM (at most 168 registers).
 // IP: stages run in place (TmaPlan::inplace); variant 2 is always in place.
+// Variant 3: 7-smooth plans (radix 2/3/4/5/7/8/16, no 11 or 13), built for two
+// CTAs of up to 256 threads per SM (at most 128 registers).
 template <class T, bool INV, int V, bool IP>
-__global__ void __launch_bounds__(V == 2 ? 128 : 256, V == 2 ? 3 : ((V == 1 && sizeof(T) == 4) ? 2 : 1))
+__global__ void __launch_bounds__(V == 2 ? 128 : 256, V == 2 ? 3 : (V == 3 || (V == 1 && sizeof(T) == 4)) ? 2 : 1)
     tma_kernel(const __grid_constant__ TmaArgs<T> a) {
-  constexpr bool P2 = V != 0;
+  constexpr bool P2 = V == 1 || V == 2;
+  constexpr bool S7 = V == 3;
   using C = typename CT<T>::type;
   extern __shared__ __align__(128) unsigned char smraw[];
   const int L = a.L, P = a.P, n = a.sl.n, ld = a.ld;
@@ -309,6 +312,17 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256, V == 2 ? 3 : ((V == 1 && s
         switch (sd.R) {
           case 2: AFC_TM(2); break;
           case 4: AFC_TM(4); break;
+          case 8: AFC_TM(8); break;
+          case 16: AFC_TM(16); break;
+          default: break;
+        }
+      } else if constexpr (S7) {
+        switch (sd.R) {
+          case 2: AFC_TM(2); break;
+          case 3: AFC_TM(3); break;
+          case 4: AFC_TM(4); break;
+          case 5: AFC_TM(5); break;
+          case 7: AFC_TM(7); break;
           case 8: AFC_TM(8); break;
           case 16: AFC_TM(16); break;
           default: break;
@@ -431,7 +445,13 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
   }
   while (tp.L * P > tmax) P = std::max(1, P / 2);
   tp.P = P;
-  tp.variant = !p2 ? 0 : (tmax == 128 ? 2 : 1);
+  bool s7 = true;
+  for (int i = 0; i < sl.nst; ++i) s7 = s7 && sl.st[i].R != 11 && sl.st[i].R != 13;
+  static const int v3_on = [] {
+    const char* e = getenv("AFC_TMA_V3");
+    return e && *e ? atoi(e) : 1;
+  }();
+  tp.variant = p2 ? (tmax == 128 ? 2 : 1) : ((s7 && v3_on) ? 3 : 0);
   // in place only for power-of-two plans: odd-radix butterflies held across
   // the barrier cost spills
   tp.inplace = p2;
@@ -459,6 +479,7 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
   using C = typename CT<T>::type;
   auto k = tp.variant == 2  ? tma_kernel<T, INV, 2, true>
            : tp.variant == 1 ? (tp.inplace ? tma_kernel<T, INV, 1, true> : tma_kernel<T, INV, 1, false>)
+           : tp.variant == 3 ? tma_kernel<T, INV, 3, false>
                              : tma_kernel<T, INV, 0, false>;
   const size_t smem = tma_smem_bytes(tp, sizeof(C));
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
