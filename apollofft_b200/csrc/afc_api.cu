@@ -545,10 +545,12 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
       d.nlen = io.nlen;
       d.herm_n = io.herm_n;
       d.pair_w = io.pair_w;
-      if (!tl_rec && io.in_op == IN_C && io.out_op == OUT_C && env_int("AFC_TMA", 1)) {
+      const bool rin = io.in_op == IN_R && io.out_op == OUT_C, rout = io.in_op == IN_C && io.out_op == OUT_RE;
+      if (!tl_rec && ((io.in_op == IN_C && io.out_op == OUT_C) || rin || rout) && env_int("AFC_TMA", 1)) {
         TmaPlan tp;
         unsigned* err = device_err_word();
-        if (err && tma_plan(ap.lp.sl, ap.lp.ld, io.lanes, io.im, io.om, io.in, io.out, dbl, env_int("AFC_TMA_LANES", 0), tp))
+        if (err && tma_plan(ap.lp.sl, ap.lp.ld, io.lanes, io.im, io.om, io.in, io.out, dbl, env_int("AFC_TMA_LANES", 0), tp,
+                            rin, rout))
           return launch_tma(d, tp, err, dbl, inv, st);
       }
       if (!tl_rec && io.in_op == IN_C && plain_out(io.out_op)) {

@@ -75,9 +75,12 @@ struct TmaPlan {
   // kernel build: 0 any radix (256 threads), 1 radix 2/4/8/16 (256 threads),
   // 2 radix 2/4/8/16 complex128 at <= 128 threads, three CTAs per SM
   int variant = 0;
+  // contiguous in-place tiles only: real input lanes (widened in the first
+  // stage) / real output lanes (real parts stored by the last stage)
+  bool real_in = false, real_out = false;
 };
 bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, const LaneMap& om, const void* in,
-              void* out, bool dbl, int lanes_pref, TmaPlan& tp);
+              void* out, bool dbl, int lanes_pref, TmaPlan& tp, bool real_in = false, bool real_out = false);
 size_t tma_smem_bytes(const TmaPlan& tp, size_t csz);
 cudaError_t launch_tma(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, bool dbl, bool inv, cudaStream_t st);
 

@@ -39,6 +39,8 @@ template <class T> struct TmaArgs {
   int L, P, ld, slot_elems;
   int mode;         // 0 contiguous (1D bulk), 1 strided (tensor)
   int inplace;      // stages run in place in the slot (no work buffer)
+  int real_in;      // contiguous in-place mode: input lanes are real (widened to complex in stage 0)
+  int real_out;     // contiguous in-place mode: output lanes are the real parts
   int nbx, bn;      // boxes along the transformed axis, rows per box
   T scale;
   unsigned* err;
@@ -142,17 +144,26 @@ __device__ __forceinline__ void tma_stage(TView<C> src, TView<C> dst, int l, int
 // (n / R <= P).  All reads of the stage finish before the barrier, all writes
 // come after it, so source and destination may share the slot.  Every thread
 // of the CTA reaches the barrier.
+// rsrc / rdst (contiguous lanes only): when set, the stage reads real input
+// lanes (widened to complex) from rsrc, or writes the real parts of its output
+// to rdst, both with lane stride n.
 template <int R, bool INV, class C, class S>
 __device__ __forceinline__ void tma_stage_inplace(TView<C> src, TView<C> dst, int l, int n, int Ns,
-                                                  const C* __restrict__ tw, int t, bool scale_out, S sc) {
+                                                  const C* __restrict__ tw, int t, bool scale_out, S sc,
+                                                  const S* rsrc = nullptr, S* rdst = nullptr) {
   const int nb = n / R;
   const int j = t;
   const bool have = j < nb;
   C v[R];
   int k = 0;
   if (have) {
+    if (rsrc) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = src.at(l, j + r * nb);
+      for (int r = 0; r < R; ++r) v[r] = C{rsrc[(long long)l * n + j + r * nb], (S)0};
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = src.at(l, j + r * nb);
+    }
   }
   __syncthreads();
   if (have) {
@@ -166,8 +177,13 @@ __device__ __forceinline__ void tma_stage_inplace(TView<C> src, TView<C> dst, in
     }
     DFT<R, INV>::run(v);
     const int o = (j - k) * R + k;
+    if (rdst) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) dst.at(l, o + r * Ns) = scale_out ? cscale(v[r], sc) : v[r];
+      for (int r = 0; r < R; ++r) rdst[(long long)l * n + o + r * Ns] = scale_out ? v[r].x * sc : v[r].x;
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) dst.at(l, o + r * Ns) = scale_out ? cscale(v[r], sc) : v[r];
+    }
   }
 }
 
@@ -179,9 +195,10 @@ __device__ __forceinline__ void tma_issue_load(const TmaArgs<T>& a, long long ti
     const long long q0 = tile * a.L;
     const long long rem = a.lanes - q0;
     const int lanes_here = (int)(rem < a.L ? rem : a.L);
-    const unsigned bytes = (unsigned)((long long)lanes_here * a.sl.n * sizeof(C));
+    const size_t es = a.real_in ? sizeof(T) : sizeof(C);
+    const unsigned bytes = (unsigned)((long long)lanes_here * a.sl.n * es);
     mbar_expect_tx(bar, bytes);
-    bulk_load(slot, a.in + q0 * a.sl.n, bytes, bar);
+    bulk_load(slot, reinterpret_cast<const char*>(a.in) + q0 * a.sl.n * es, bytes, bar);
   } else {
     const int o = (int)(tile / a.kb), kb = (int)(tile % a.kb);
     const unsigned box_bytes = (unsigned)(2 * a.L * a.bn * sizeof(T));
@@ -198,7 +215,8 @@ __device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long t
     const long long q0 = tile * a.L;
     const long long rem = a.lanes - q0;
     const int lanes_here = (int)(rem < a.L ? rem : a.L);
-    bulk_store(a.out + q0 * a.sl.n, buf, (unsigned)((long long)lanes_here * a.sl.n * sizeof(C)));
+    const size_t es = a.real_out ? sizeof(T) : sizeof(C);
+    bulk_store(reinterpret_cast<char*>(a.out) + q0 * a.sl.n * es, buf, (unsigned)((long long)lanes_here * a.sl.n * es));
   } else {
     const int o = (int)(tile / a.kb), kb = (int)(tile % a.kb);
     for (int b = 0; b < a.nbx; ++b) {
@@ -275,7 +293,9 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256, V == 2 ? 3 : (V == 3 || (V
       const TView<C> src = s == 0 ? lin : cpad;
       const TView<C> dst = last ? olin : cpad;
       const C* twi = a.tw + sd.twoff;
-#define AFC_TI(R) tma_stage_inplace<R, INV>(src, dst, l, n, sd.Ns, twi, t, last, a.scale)
+      const T* rsrc = (s == 0 && a.real_in) ? reinterpret_cast<const T*>(cur) : nullptr;
+      T* rdst = (last && a.real_out) ? reinterpret_cast<T*>(cur) : nullptr;
+#define AFC_TI(R) tma_stage_inplace<R, INV>(src, dst, l, n, sd.Ns, twi, t, last, a.scale, rsrc, rdst)
       if constexpr (P2) {
         switch (sd.R) {
           case 2: AFC_TI(2); break;
@@ -396,9 +416,11 @@ size_t tma_smem_bytes(const TmaPlan& tp, size_t csz) {
 
 // Decides whether an axis pass can run on the TMA kernel and with which tiles.
 bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, const LaneMap& om, const void* in,
-              void* out, bool dbl, int lanes_pref, TmaPlan& tp) {
+              void* out, bool dbl, int lanes_pref, TmaPlan& tp, bool real_in, bool real_out) {
   const size_t csz = dbl ? 16 : 8;
   const long long n = sl.n;
+  const bool real = real_in || real_out;
+  if (real && (im.es != 1 || (n * (long long)(csz / 2)) % 16)) return false;
   if (im.off || om.off) return false;
   if (im.d1 != 1 || om.d1 != 1 || im.d2 != om.d2 || im.s0 != om.s0 || im.es != om.es || im.s2 != om.s2) return false;
   if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) return false;
@@ -420,15 +442,28 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
     tp.L = lanes_pref > 0 ? lanes_pref : (dbl ? 8 : 16);
     tp.nbx = (int)((n + 255) / 256);
     tp.bn = (int)((n + tp.nbx - 1) / tp.nbx);
+    // long axes: narrower tiles (down to 32-byte rows) until two slots and a
+    // work buffer fit in shared memory
+    const long long rows = (long long)tp.nbx * tp.bn;
+    const int Lmin = dbl ? 2 : 4;
+    while (lanes_pref <= 0 && tp.L > Lmin &&
+           3 * (size_t)tp.L * (size_t)std::max<long long>(ld, rows) * csz + 64 > 220 * 1024)
+      tp.L /= 2;
     tp.kb = (es + tp.L - 1) / tp.L;
   }
   tp.ld = ld;
   // threads: one radix-16 butterfly per thread and stage when possible
   int P = (int)std::max<long long>(1, std::min<long long>(256, (n + 15) / 16));
   bool p2 = true;
+  long long nbmax = 1;
   for (int i = 0; i < sl.nst; ++i) {
     const int R = sl.st[i].R;
     p2 = p2 && (R == 2 || R == 4 || R == 8 || R == 16);
+    nbmax = std::max<long long>(nbmax, n / R);
+  }
+  if (real) {  // real lanes need in-place stages: one thread per butterfly of the widest stage
+    if (!p2 || nbmax > 256) return false;
+    P = (int)nbmax;
   }
   // complex128 power-of-two tiles of <= 128 threads whose stages run in place
   // (one butterfly per thread) use the three-CTA build
@@ -456,6 +491,9 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
   // the barrier cost spills
   tp.inplace = p2;
   for (int i = 0; i < sl.nst; ++i) tp.inplace = tp.inplace && n / sl.st[i].R <= P;
+  if (real && !tp.inplace) return false;
+  tp.real_in = real_in;
+  tp.real_out = real_out;
   const int align = dbl ? 8 : 16;  // 128-byte aligned slots
   long long rows = tp.mode == 1 ? (long long)tp.nbx * tp.bn : n;
   long long se = (long long)tp.L * std::max<long long>(ld, rows);
@@ -504,6 +542,8 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
   a.slot_elems = tp.slot_elems;
   a.mode = tp.mode;
   a.inplace = tp.inplace ? 1 : 0;
+  a.real_in = tp.real_in ? 1 : 0;
+  a.real_out = tp.real_out ? 1 : 0;
   a.nbx = tp.nbx;
   a.bn = tp.bn;
   a.scale = (T)d.scale;
