@@ -73,7 +73,8 @@ struct TmaPlan {
   // tile's slot (registers hold the butterfly across a barrier), no work buffer
   bool inplace = false;
   // kernel build: 0 any radix (256 threads), 1 radix 2/4/8/16 (256 threads),
-  // 2 radix 2/4/8/16 complex128 at <= 128 threads, three CTAs per SM
+  // 2 radix 2/4/8/16 complex128 at <= 128 threads, three CTAs per SM,
+  // 3 7-smooth, 4 complex64 in place with two butterflies of a radix <= 8 stage
   int variant = 0;
   // contiguous in-place tiles only: real input lanes (widened in the first
   // stage) / real output lanes (real parts stored by the last stage)

@@ -144,45 +144,55 @@ __device__ __forceinline__ void tma_stage(TView<C> src, TView<C> dst, int l, int
 // (n / R <= P).  All reads of the stage finish before the barrier, all writes
 // come after it, so source and destination may share the slot.  Every thread
 // of the CTA reaches the barrier.
-// rsrc / rdst (contiguous lanes only): when set, the stage reads real input
-// lanes (widened to complex) from rsrc, or writes the real parts of its output
-// to rdst, both with lane stride n.
-template <int R, bool INV, class C, class S>
+// One stage in place: a thread holds one butterfly of its lane, or with NB2 up
+// to two of a radix <= 8 stage (the plan guarantees the count).  All
+// reads of the stage finish before the barrier, all writes come after it, so
+// source and destination may share the slot.  Every thread of the CTA reaches
+// the barrier.  rsrc / rdst (contiguous lanes only): when set, the stage reads
+// real input lanes (widened to complex) from rsrc, or writes the real parts of
+// its output to rdst, both with lane stride n.
+template <int R, bool INV, int NB2, class C, class S>
 __device__ __forceinline__ void tma_stage_inplace(TView<C> src, TView<C> dst, int l, int n, int Ns,
-                                                  const C* __restrict__ tw, int t, bool scale_out, S sc,
+                                                  const C* __restrict__ tw, int t, int P, bool scale_out, S sc,
                                                   const S* rsrc = nullptr, S* rdst = nullptr) {
+  constexpr int NB = (R <= 8 && NB2) ? 2 : 1;
   const int nb = n / R;
-  const int j = t;
-  const bool have = j < nb;
-  C v[R];
-  int k = 0;
-  if (have) {
-    if (rsrc) {
+  C v[NB][R];
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[r] = C{rsrc[(long long)l * n + j + r * nb], (S)0};
-    } else {
+  for (int b = 0; b < NB; ++b) {
+    const int j = t + b * P;
+    if (j < nb) {
+      if (rsrc) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[r] = src.at(l, j + r * nb);
+        for (int r = 0; r < R; ++r) v[b][r] = C{rsrc[(long long)l * n + j + r * nb], (S)0};
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[b][r] = src.at(l, j + r * nb);
+      }
     }
   }
   __syncthreads();
-  if (have) {
-    k = j % Ns;
-    if (Ns > 1) {
 #pragma unroll
-      for (int r = 1; r < R; ++r) {
-        const C wr = tw[(long long)(r - 1) * Ns + k];
-        v[r] = INV ? cmulc(v[r], wr) : cmul(v[r], wr);
+  for (int b = 0; b < NB; ++b) {
+    const int j = t + b * P;
+    if (j < nb) {
+      const int k = j % Ns;
+      if (Ns > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          const C wr = tw[(long long)(r - 1) * Ns + k];
+          v[b][r] = INV ? cmulc(v[b][r], wr) : cmul(v[b][r], wr);
+        }
       }
-    }
-    DFT<R, INV>::run(v);
-    const int o = (j - k) * R + k;
-    if (rdst) {
+      DFT<R, INV>::run(v[b]);
+      const int o = (j - k) * R + k;
+      if (rdst) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) rdst[(long long)l * n + o + r * Ns] = scale_out ? v[r].x * sc : v[r].x;
-    } else {
+        for (int r = 0; r < R; ++r) rdst[(long long)l * n + o + r * Ns] = scale_out ? v[b][r].x * sc : v[b][r].x;
+      } else {
 #pragma unroll
-      for (int r = 0; r < R; ++r) dst.at(l, o + r * Ns) = scale_out ? cscale(v[r], sc) : v[r];
+        for (int r = 0; r < R; ++r) dst.at(l, o + r * Ns) = scale_out ? cscale(v[b][r], sc) : v[b][r];
+      }
     }
   }
 }
@@ -233,11 +243,14 @@ __device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long t
 // CTAs per SM (at most 168 registers).
 // IP: stages run in place (TmaPlan::inplace); variant 2 is always in place.
 // Variant 3: 7-smooth plans (radix 2/3/4/5/7/8/16, no 11 or 13), built for two
-// CTAs of up to 256 threads per SM (at most 128 registers).
+// CTAs of up to 256 threads per SM (at most 128 registers).  Variant 4:
+// complex64 power-of-two in place with two butterflies per thread in the
+// radix <= 8 stages (the 256-thread build of variant 1 otherwise).
 template <class T, bool INV, int V, bool IP>
-__global__ void __launch_bounds__(V == 2 ? 128 : 256, V == 2 ? 3 : (V == 3 || (V == 1 && sizeof(T) == 4)) ? 2 : 1)
+__global__ void __launch_bounds__(V == 2 ? 128 : 256,
+                                  V == 2 ? 3 : (V == 3 || ((V == 1 || V == 4) && sizeof(T) == 4)) ? 2 : 1)
     tma_kernel(const __grid_constant__ TmaArgs<T> a) {
-  constexpr bool P2 = V == 1 || V == 2;
+  constexpr bool P2 = V == 1 || V == 2 || V == 4;
   constexpr bool S7 = V == 3;
   using C = typename CT<T>::type;
   extern __shared__ __align__(128) unsigned char smraw[];
@@ -295,7 +308,7 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256, V == 2 ? 3 : (V == 3 || (V
       const C* twi = a.tw + sd.twoff;
       const T* rsrc = (s == 0 && a.real_in) ? reinterpret_cast<const T*>(cur) : nullptr;
       T* rdst = (last && a.real_out) ? reinterpret_cast<T*>(cur) : nullptr;
-#define AFC_TI(R) tma_stage_inplace<R, INV>(src, dst, l, n, sd.Ns, twi, t, last, a.scale, rsrc, rdst)
+#define AFC_TI(R) tma_stage_inplace<R, INV, (V == 4 ? 1 : 0)>(src, dst, l, n, sd.Ns, twi, t, P, last, a.scale, rsrc, rdst)
       if constexpr (P2) {
         switch (sd.R) {
           case 2: AFC_TI(2); break;
@@ -442,12 +455,12 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
     tp.L = lanes_pref > 0 ? lanes_pref : (dbl ? 8 : 16);
     tp.nbx = (int)((n + 255) / 256);
     tp.bn = (int)((n + tp.nbx - 1) / tp.nbx);
-    // long axes: narrower tiles (down to 32-byte rows) until two slots and a
-    // work buffer fit in shared memory
+    // long axes: narrower tiles (down to 16-byte rows) until two slots and a
+    // work buffer fit twice per SM
     const long long rows = (long long)tp.nbx * tp.bn;
-    const int Lmin = dbl ? 2 : 4;
+    const int Lmin = dbl ? 1 : 2;
     while (lanes_pref <= 0 && tp.L > Lmin &&
-           3 * (size_t)tp.L * (size_t)std::max<long long>(ld, rows) * csz + 64 > 220 * 1024)
+           3 * (size_t)tp.L * (size_t)std::max<long long>(ld, rows) * csz + 64 > 110 * 1024)
       tp.L /= 2;
     tp.kb = (es + tp.L - 1) / tp.L;
   }
@@ -461,14 +474,20 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
     p2 = p2 && (R == 2 || R == 4 || R == 8 || R == 16);
     nbmax = std::max<long long>(nbmax, n / R);
   }
-  if (real) {  // real lanes need in-place stages: one thread per butterfly of the widest stage
-    if (!p2 || nbmax > 256) return false;
-    P = (int)nbmax;
-  }
+  (void)nbmax;
+  if (real && !p2) return false;  // real lanes need in-place stages
+  // in place: a thread holds one butterfly per stage (complex64: two of a radix <= 8 stage)
+  auto fits_inplace = [&](int Pc, bool two) {
+    if (!p2) return false;
+    for (int i = 0; i < sl.nst; ++i) {
+      const long long nb = n / sl.st[i].R;
+      if ((nb + Pc - 1) / Pc > ((two && sl.st[i].R <= 8 && !dbl) ? 2 : 1)) return false;
+    }
+    return true;
+  };
   // complex128 power-of-two tiles of <= 128 threads whose stages run in place
-  // (one butterfly per thread) use the three-CTA build
-  bool ip128 = P <= 128;
-  for (int i = 0; i < sl.nst; ++i) ip128 = ip128 && n / sl.st[i].R <= P;
+  // use the three-CTA build
+  const bool ip128 = P <= 128 && fits_inplace(P, false);
   static const int v2_on = [] {
     const char* e = getenv("AFC_TMA_V2");
     return e && *e ? atoi(e) : 1;
@@ -489,8 +508,11 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
   tp.variant = p2 ? (tmax == 128 ? 2 : 1) : ((s7 && v3_on) ? 3 : 0);
   // in place only for power-of-two plans: odd-radix butterflies held across
   // the barrier cost spills
-  tp.inplace = p2;
-  for (int i = 0; i < sl.nst; ++i) tp.inplace = tp.inplace && n / sl.st[i].R <= P;
+  tp.inplace = fits_inplace(P, false);
+  if (!tp.inplace && !dbl && fits_inplace(P, true)) {
+    tp.inplace = true;
+    tp.variant = 4;
+  }
   if (real && !tp.inplace) return false;
   tp.real_in = real_in;
   tp.real_out = real_out;
@@ -515,7 +537,8 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
 template <class T, bool INV>
 static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, cudaStream_t st) {
   using C = typename CT<T>::type;
-  auto k = tp.variant == 2  ? tma_kernel<T, INV, 2, true>
+  auto k = tp.variant == 4  ? tma_kernel<T, INV, 4, true>
+           : tp.variant == 2 ? tma_kernel<T, INV, 2, true>
            : tp.variant == 1 ? (tp.inplace ? tma_kernel<T, INV, 1, true> : tma_kernel<T, INV, 1, false>)
            : tp.variant == 3 ? tma_kernel<T, INV, 3, false>
                              : tma_kernel<T, INV, 0, false>;
