@@ -711,6 +711,49 @@ static afc_status fft_table(const AxisPlan& mp, bool dbl, void* buf, cudaStream_
   return AFC_OK;
 }
 
+// Stages of the GPU plan of length m (one CTA, or the two passes of a
+// four-step split plus a weight for its extra global-memory round trip);
+// -1 when m has no GPU plan.
+static int plan_stages(int64_t m, size_t csz) {
+  std::vector<int> rad;
+  if (!gpu_radices(m, rad)) return -1;
+  if (plannable(m, csz)) return (int)rad.size();
+  int best = -1;
+  for (int64_t d = 2; d * d <= m * 4 && d < m; ++d) {
+    if (m % d) continue;
+    std::vector<int> r1, r2;
+    if (!plannable(d, csz, &r1) || !plannable(m / d, csz, &r2)) continue;
+    const int c = (int)(r1.size() + r2.size()) + 2;
+    if (best < 0 || c < best) best = c;
+  }
+  return best;
+}
+
+// Convolution length for Rader / Bluestein: the length >= need with the least
+// work (length x stages) among the next power of two and the 7-smooth lengths
+// below it (Bluestein's convolution is exact for any length >= 2n - 1).
+static int64_t conv_length(int64_t need, size_t csz) {
+  int64_t p2 = 1;
+  while (p2 < need) p2 <<= 1;
+  int64_t best = p2;
+  const int s2 = plan_stages(p2, csz);
+  double best_cost = s2 > 0 ? (double)p2 * s2 : 1e300;
+  for (int64_t a = 1; a < p2; a *= 2)
+    for (int64_t b = a; b < p2; b *= 3)
+      for (int64_t c = b; c < p2; c *= 5)
+        for (int64_t d = c; d < p2; d *= 7) {
+          if (d < need) continue;
+          const int sd = plan_stages(d, csz);
+          if (sd <= 0) continue;
+          const double cost = (double)d * sd;
+          if (cost < 0.97 * best_cost) {
+            best_cost = cost;
+            best = d;
+          }
+        }
+  return best;
+}
+
 static afc_status build_axis(int64_t n, bool dbl, AxisPlan& ap, cudaStream_t st) {
   const size_t csz = dbl ? 16 : 8;
   ap.n = n;
@@ -725,10 +768,7 @@ static afc_status build_axis(int64_t n, bool dbl, AxisPlan& ap, cudaStream_t st)
     // convolution of length p-1, exact or zero-padded to a power of two.
     const int64_t L = n - 1;
     int64_t M = L;
-    if (!plannable(L, csz)) {
-      M = 1;
-      while (M < 2 * L - 1) M <<= 1;
-    }
+    if (!plannable(L, csz)) M = conv_length(2 * L - 1, csz);
     if (!plannable(M, csz))
       return fail(AFC_ERR_UNSUPPORTED, "no Rader plan for %lld", (long long)n);
     ap.algo = ALGO_RADER;
@@ -757,9 +797,8 @@ static afc_status build_axis(int64_t n, bool dbl, AxisPlan& ap, cudaStream_t st)
     mp.lp.tw = nullptr;  // owned by ap
     return s;
   }
-  // Bluestein chirp-z with a power-of-two convolution of length M >= 2n-1.
-  int64_t M = 1;
-  while (M < 2 * n - 1) M <<= 1;
+  // Bluestein chirp-z with a convolution of length M >= 2n-1.
+  const int64_t M = conv_length(2 * n - 1, csz);
   ap.algo = ALGO_BLUESTEIN;
   ap.M = M;
   AFC_CUDA(dev_alloc(&ap.chirp, (size_t)n * csz), "chirp");
