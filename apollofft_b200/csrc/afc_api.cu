@@ -252,8 +252,19 @@ static int choose_threads(int64_t n, const std::vector<int>& rad) {
 }
 
 // Shared-memory budget of one single-CTA lane; batch plans lower it so that
-// every tile of their persistent kernel fits two CTAs per SM.
+// every tile of their persistent kernel fits several CTAs per SM.
 static thread_local size_t tl_smem_cap = kSmemMax;
+
+// Per-CTA shared memory of persistent batch tiles: three complex64 CTAs per SM
+// (the float batch kernel is built for three), two complex128 CTAs.
+static size_t batch_smem_cap(bool dbl) {
+  static const long kb = [] {
+    const char* e = getenv("AFC_BATCH_SMEM_KB");
+    return e && *e ? atol(e) : 0L;
+  }();
+  if (kb > 0) return (size_t)kb * 1024;
+  return dbl ? 100 * 1024 : 72 * 1024;
+}
 
 // A single-CTA plan needs two shared buffers of ld elements for one lane.
 static bool plannable(int64_t n, size_t csz, std::vector<int>* rad_out = nullptr) {
@@ -385,7 +396,7 @@ static int choose_L(const LenPlan& lp, long long lanes, bool stage_in, bool stag
   const int Lmin = staged ? (csz == 16 ? 8 : 16) : 1;
   L = std::max(L, Lmin);
   while (L > 1 && ((size_t)L * lp.P > 512 || (size_t)L * per_lane > kSmemMax)) --L;
-  while (L > Lmin && (size_t)L * per_lane > 100 * 1024) --L;
+  while (L > Lmin && (size_t)L * per_lane > std::min<size_t>(100 * 1024, tl_smem_cap)) --L;
   if ((long long)L > lanes) L = (int)std::max(1LL, lanes);
   return L;
 }
@@ -711,10 +722,29 @@ static afc_status fft_table(const AxisPlan& mp, bool dbl, void* buf, cudaStream_
   return AFC_OK;
 }
 
+static int plan_stages_uncached(int64_t m, size_t csz);
+
 // Stages of the GPU plan of length m (one CTA, or the two passes of a
 // four-step split plus a weight for its extra global-memory round trip);
 // -1 when m has no GPU plan.
 static int plan_stages(int64_t m, size_t csz) {
+  // memo per (length, element size, shared-memory budget): batch plans ask
+  // for hundreds of candidate lengths per prime
+  static std::mutex mu;
+  static std::map<std::tuple<int64_t, size_t, size_t>, int> memo;
+  const auto key = std::make_tuple(m, csz, tl_smem_cap);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = memo.find(key);
+    if (it != memo.end()) return it->second;
+  }
+  const int r = plan_stages_uncached(m, csz);
+  std::lock_guard<std::mutex> lk(mu);
+  memo[key] = r;
+  return r;
+}
+
+static int plan_stages_uncached(int64_t m, size_t csz) {
   std::vector<int> rad;
   if (!gpu_radices(m, rad)) return -1;
   if (plannable(m, csz)) return (int)rad.size();
@@ -1317,7 +1347,7 @@ static void tune_group(BatchGroup& g, bool dbl, void* scratch, cudaStream_t st) 
     d.out = scratch;
     const size_t per_lane = 2 * (size_t)d.ld * csz + 3 * sizeof(long long);
     int L = std::max(1, kBatchThreads / P);
-    while (L > 1 && (size_t)L * per_lane > 100 * 1024) --L;
+    while (L > 1 && (size_t)L * per_lane > batch_smem_cap(dbl)) --L;
     d.L = L;
     d.stage_out = ap.lp.sl.nst <= 1;
     if (launch_lanes(d, dbl, false, st) != cudaSuccess) continue;
@@ -1730,8 +1760,8 @@ afc_status afc_batch_plan_create(afc_batch_plan* out, const int64_t* lengths, in
   AFC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
   const size_t csz = bp->dbl ? 16 : 8;
   afc_status s = AFC_OK;
-  // single-CTA lengths of a batch keep two persistent CTAs per SM
-  tl_smem_cap = 100 * 1024;
+  // single-CTA lengths of a batch keep several persistent CTAs per SM
+  tl_smem_cap = batch_smem_cap(bp->dbl);
   int64_t max_smem_len = 1;
   for (auto& kv : by_len) {
     std::unique_ptr<BatchGroup> grp(new BatchGroup());
@@ -1749,7 +1779,6 @@ afc_status afc_batch_plan_create(afc_batch_plan* out, const int64_t* lengths, in
     bp->ws_bytes += (axis_ws_bytes(*grp->ap, grp->lanes, csz) + 255) / 256 * 256;
     bp->groups.push_back(std::move(grp));
   }
-  tl_smem_cap = kSmemMax;
   if (s == AFC_OK) {
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) s = cuda_fail(e, "batch plan build");
@@ -1775,6 +1804,7 @@ afc_status afc_batch_plan_create(afc_batch_plan* out, const int64_t* lengths, in
   }
   if (s == AFC_OK) s = build_phases(*bp, false, st);
   if (s == AFC_OK) s = build_phases(*bp, true, st);
+  tl_smem_cap = kSmemMax;
   cudaError_t e = cudaStreamSynchronize(st);
   cudaStreamDestroy(st);
   if (s != AFC_OK) return s;

@@ -204,8 +204,26 @@ __device__ __forceinline__ void lanes_tile(const KArgs<T>& a, long long q0, unsi
   C* b1 = b0 + (nbuf > 1 ? ld : 0);
   __syncthreads();
   if (a.stage_in) {
+    // four independent loads in flight per thread before their shared stores
     const int total = lanes_here * n;
-    for (int e = tid; e < total; e += blockDim.x) {
+    const int stride = blockDim.x;
+    int e = tid;
+    for (; e + 3 * stride < total; e += 4 * stride) {
+      C v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int ee = e + u * stride;
+        const int l2 = ee % lanes_here, i = ee / lanes_here;
+        v[u] = gload(a, lb[l2], lb[2 * L + l2], i);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int ee = e + u * stride;
+        const int l2 = ee % lanes_here, i = ee / lanes_here;
+        sm[(long long)l2 * nbuf * ld + spad(i)] = v[u];
+      }
+    }
+    for (; e < total; e += stride) {
       const int l2 = e % lanes_here, i = e / lanes_here;
       sm[(long long)l2 * nbuf * ld + spad(i)] = gload(a, lb[l2], lb[2 * L + l2], i);
     }
@@ -478,7 +496,7 @@ __global__ void __launch_bounds__(512) conv_kernel(const __grid_constant__ KArgs
 // buffer selectors against this launch's bases and run the tile.
 
 template <class T>
-__global__ void __launch_bounds__(kBatchThreads, 2) batch_kernel(const KArgs<T>* __restrict__ descs, const BatchItem* __restrict__ items,
+__global__ void __launch_bounds__(kBatchThreads, sizeof(T) == 4 ? 3 : 2) batch_kernel(const KArgs<T>* __restrict__ descs, const BatchItem* __restrict__ items,
                                                    int nitems, int* counter, const void* in_base, void* out_base,
                                                    void* ws_base) {
   extern __shared__ __align__(16) unsigned char smraw[];
