@@ -115,6 +115,15 @@ template <class C> struct TView {
   C* p;
   int ls, is, pad;
   __device__ __forceinline__ C& at(int l, int i) const { return p[l * ls + i * is + (pad ? (i >> 4) : 0)]; }
+  // Elements i0 + r d (r < R) of lane l as a pointer and a fixed stride when
+  // the padding term is linear in r: no padding, d a multiple of 16, or the
+  // whole run inside one 16-element block.  False otherwise.
+  __device__ __forceinline__ bool run(int l, int i0, int d, int R, C*& q, int& s) const {
+    if (pad && (d & 15) && (i0 & 15) + (R - 1) * d >= 16) return false;
+    q = p + l * ls + i0 * is + (pad ? (i0 >> 4) : 0);
+    s = d * is + (pad ? (d >> 4) : 0);
+    return true;
+  }
 };
 
 template <int R, bool INV, class C, class S>
@@ -162,9 +171,14 @@ __device__ __forceinline__ void tma_stage_inplace(TView<C> src, TView<C> dst, in
   for (int b = 0; b < NB; ++b) {
     const int j = t + b * P;
     if (j < nb) {
+      C* q;
+      int qs;
       if (rsrc) {
 #pragma unroll
         for (int r = 0; r < R; ++r) v[b][r] = C{rsrc[(long long)l * n + j + r * nb], (S)0};
+      } else if (sizeof(S) == 4 && src.run(l, j, nb, R, q, qs)) {  // complex64 only: complex128 spills
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[b][r] = q[r * qs];
       } else {
 #pragma unroll
         for (int r = 0; r < R; ++r) v[b][r] = src.at(l, j + r * nb);
@@ -186,9 +200,14 @@ __device__ __forceinline__ void tma_stage_inplace(TView<C> src, TView<C> dst, in
       }
       DFT<R, INV>::run(v[b]);
       const int o = (j - k) * R + k;
+      C* q;
+      int qs;
       if (rdst) {
 #pragma unroll
         for (int r = 0; r < R; ++r) rdst[(long long)l * n + o + r * Ns] = scale_out ? v[b][r].x * sc : v[b][r].x;
+      } else if (sizeof(S) == 4 && dst.run(l, o, Ns, R, q, qs)) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) q[r * qs] = scale_out ? cscale(v[b][r], sc) : v[b][r];
       } else {
 #pragma unroll
         for (int r = 0; r < R; ++r) dst.at(l, o + r * Ns) = scale_out ? cscale(v[b][r], sc) : v[b][r];
