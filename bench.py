@@ -87,18 +87,53 @@ def barrier(world):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed region.
+
+    NVML is polled about every millisecond from a thread (a timed region of a
+    few milliseconds still gets samples; nvidia-smi's loop cannot go below a
+    few hundred milliseconds).  Only samples taken between `start()` and
+    `stop()` count.  Falls back to an `nvidia-smi -lms 200` loop when NVML is
+    unavailable."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.lines = []
+        self.samples = []  # (sm_mhz, reason bits)
+        self.max_mhz = None
+        self.active = False
+        self.done = False
+        self.nv = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def __enter__(self):
+        try:
+            self.nv, self.h = self._handle()
+            nv = self.nv
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+            self.get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nv = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -109,11 +144,33 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def _poll(self):
+        nv = self.nv
+        while not self.done:
+            if self.active:
+                try:
+                    self.samples.append((float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)),
+                                         int(self.get_reasons(self.h))))
+                except Exception:
+                    pass
+            time.sleep(0.001)
+
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            if self.active:
+                self.lines.append(line.strip())
+
+    def start(self):
+        self.active = True
+
+    def stop(self):
+        self.active = False
 
     def __exit__(self, *a):
+        self.done = True
+        self.active = False
+        if self.nv is not None:
+            self.t.join(timeout=2)
         if self.proc:
             self.proc.terminate()
             try:
@@ -122,7 +179,12 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
+        sm, mx, reasons = [], self.max_mhz, set()
+        for mhz, bits in self.samples:
+            sm.append(mhz)
+            for nm, b in self.REASONS.items():
+                if bits & b:
+                    reasons.add(nm)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
@@ -137,7 +199,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 def cpu_transform_gflops(shape, reps, threads=0, want_output=False):
@@ -251,12 +313,14 @@ def main():
         n1 = afc.kernel_launch_count()
         st = torch.cuda.current_stream()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clk.start()
         e0.record(st)
         for _ in range(args.steps):
             plan.execute(x, out=y)
             plan.execute(y, out=x, inverse=True)
         e1.record(st)
         torch.cuda.synchronize()
+        clk.stop()
         t_step = e0.elapsed_time(e1) / 1e3 / args.steps
         n2 = afc.kernel_launch_count()
     t_step_max = max_over_ranks(t_step, world, dev)
