@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -212,16 +213,80 @@ static const int64_t kRaderMax = 1024;  // Rader below, Bluestein above (primes)
 // Radices the engine executes for n: odd primes <= 13 (innermost, largest
 // first, as the reference orders its factors) then the power of two as 16s and
 // one 8/4/2.  False when n has another prime factor (Rader / Bluestein).
+// GPU stage radices of n.  Pure powers of two: radix 16 stages, then one of
+// 8 / 4 / 2.  Lengths with factors 3, 5, 7: the fewest stages over the radices
+// 2..16 of the register butterflies (composites 6, 9, 10, 12, 14, 15 are
+// nested butterflies), ties broken toward the cheaper butterflies; 11 and 13
+// each take a stage.  Non-power-of-two radices come first.
+static bool gpu_radices_uncached(int64_t n, std::vector<int>& rad);
 static bool gpu_radices(int64_t n, std::vector<int>& rad) {
+  // memo: plan building asks for the same lengths many times
+  static std::mutex mu;
+  static std::map<int64_t, std::pair<bool, std::vector<int>>> memo;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = memo.find(n);
+    if (it != memo.end()) {
+      rad = it->second.second;
+      return it->second.first;
+    }
+  }
+  const bool ok = gpu_radices_uncached(n, rad);
+  std::lock_guard<std::mutex> lk(mu);
+  memo[n] = std::make_pair(ok, rad);
+  return ok;
+}
+
+static bool gpu_radices_uncached(int64_t n, std::vector<int>& rad) {
   rad.clear();
   if (n <= 1) return false;
   int64_t m = n;
-  static const int odd[] = {13, 11, 7, 5, 3};
-  for (int p : odd)
-    while (m % p == 0) { rad.push_back(p); m /= p; }
-  int k = 0;
-  while (m % 2 == 0) { m /= 2; ++k; }
+  int e[6] = {0, 0, 0, 0, 0, 0};  // exponents of 2, 3, 5, 7, 11, 13
+  static const int pr[6] = {2, 3, 5, 7, 11, 13};
+  for (int i = 0; i < 6; ++i)
+    while (m % pr[i] == 0) { m /= pr[i]; ++e[i]; }
   if (m != 1) return false;
+  for (int i = 0; i < e[5]; ++i) rad.push_back(13);
+  for (int i = 0; i < e[4]; ++i) rad.push_back(11);
+  int k = e[0];
+  if (e[1] + e[2] + e[3] > 0) {
+    // radix -> exponents of (2, 3, 5, 7) and a tie-break penalty
+    struct Opt { int r, a, b, c, d, pen; };
+    static const Opt opts[] = {{16, 4, 0, 0, 0, 0}, {15, 0, 1, 1, 0, 2}, {14, 1, 0, 0, 1, 3}, {12, 2, 1, 0, 0, 2},
+                               {10, 1, 0, 1, 0, 3}, {9, 0, 2, 0, 0, 2},  {8, 3, 0, 0, 0, 1},  {7, 0, 0, 0, 1, 3},
+                               {6, 1, 1, 0, 0, 3},  {5, 0, 0, 1, 0, 3},  {4, 2, 0, 0, 0, 2},  {3, 0, 1, 0, 0, 4},
+                               {2, 1, 0, 0, 0, 3}};
+    std::map<std::tuple<int, int, int, int>, std::pair<int, int>> memo;  // state -> (cost, option)
+    std::function<int(int, int, int, int)> best = [&](int a, int b, int c, int d) -> int {
+      if (a == 0 && b == 0 && c == 0 && d == 0) return 0;
+      const auto key = std::make_tuple(a, b, c, d);
+      auto it = memo.find(key);
+      if (it != memo.end()) return it->second.first;
+      int bc = 1 << 30, bo = -1;
+      for (int o = 0; o < (int)(sizeof(opts) / sizeof(opts[0])); ++o) {
+        const Opt& q = opts[o];
+        if (q.a > a || q.b > b || q.c > c || q.d > d) continue;
+        const int sub = best(a - q.a, b - q.b, c - q.c, d - q.d);
+        if (sub >= (1 << 30)) continue;
+        const int cost = sub + 64 + q.pen;  // stages first, then the penalty
+        if (cost < bc) { bc = cost; bo = o; }
+      }
+      memo[key] = std::make_pair(bc, bo);
+      return bc;
+    };
+    best(k, e[1], e[2], e[3]);
+    std::vector<int> p2;
+    int a = k, b = e[1], c = e[2], d = e[3];
+    while (a || b || c || d) {
+      const Opt& q = opts[memo[std::make_tuple(a, b, c, d)].second];
+      if (q.b || q.c || q.d) rad.push_back(q.r);
+      else p2.push_back(q.r);
+      a -= q.a; b -= q.b; c -= q.c; d -= q.d;
+    }
+    std::sort(p2.begin(), p2.end(), std::greater<int>());
+    rad.insert(rad.end(), p2.begin(), p2.end());
+    return (int)rad.size() <= kMaxStages;
+  }
   while (k >= 4) { rad.push_back(16); k -= 4; }
   if (k == 3) rad.push_back(8);
   else if (k == 2) rad.push_back(4);
@@ -766,6 +831,8 @@ static int64_t conv_length(int64_t need, size_t csz) {
   int64_t p2 = 1;
   while (p2 < need) p2 <<= 1;
   int64_t best = p2;
+  static const int mode = env_int("AFC_CONV_LEN", 0);  // 0 cost model, 1 powers of two only
+  if (mode == 1) return p2;
   const int s2 = plan_stages(p2, csz);
   double best_cost = s2 > 0 ? (double)p2 * s2 : 1e300;
   for (int64_t a = 1; a < p2; a *= 2)

@@ -10,6 +10,7 @@
 //   y[m] = v0 + sum_k a_k cos(2pi km/R) -/+ i sum_k b_k sin(2pi km/R).
 #pragma once
 #include <cuda_runtime.h>
+#include "afc_roots.cuh"
 
 namespace afc {
 
@@ -597,5 +598,46 @@ template <int R, bool INV> struct DFT {
     v[0] = y0;
   }
 };
+
+// Composite radix R = R1 x R2 (6, 9, 10, 12, 14, 15) as nested butterflies:
+// input m = a + R1 b, output k = c + R2 d; R1 DFTs of size R2 over b, twiddle
+// W_R^{a c}, R2 DFTs of size R1 over a (the same index split as DFT<16>).
+template <int R1, int R2, bool INV> struct DFTNest {
+  template <class C> __device__ __forceinline__ static void run(C* v) {
+    using T = decltype(v[0].x);
+    constexpr int R = R1 * R2;
+    C z[R1][R2];
+#pragma unroll
+    for (int a = 0; a < R1; ++a) {
+#pragma unroll
+      for (int b = 0; b < R2; ++b) z[a][b] = v[a + R1 * b];
+      DFT<R2, INV>::run(z[a]);
+    }
+#pragma unroll
+    for (int a = 1; a < R1; ++a)
+#pragma unroll
+      for (int c = 1; c < R2; ++c) {
+        const T cs = (T)CompRoots<R>::c(a * c), sn = (T)CompRoots<R>::s(a * c);
+        const C x = z[a][c];
+        // forward multiplies by exp(-i theta) = cs - i sn, inverse by cs + i sn
+        z[a][c] = INV ? C{x.x * cs - x.y * sn, x.y * cs + x.x * sn} : C{x.x * cs + x.y * sn, x.y * cs - x.x * sn};
+      }
+#pragma unroll
+    for (int c = 0; c < R2; ++c) {
+      C col[R1];
+#pragma unroll
+      for (int a = 0; a < R1; ++a) col[a] = z[a][c];
+      DFT<R1, INV>::run(col);
+#pragma unroll
+      for (int d = 0; d < R1; ++d) v[c + R2 * d] = col[d];
+    }
+  }
+};
+template <bool INV> struct DFT<6, INV> : DFTNest<3, 2, INV> {};
+template <bool INV> struct DFT<9, INV> : DFTNest<3, 3, INV> {};
+template <bool INV> struct DFT<10, INV> : DFTNest<5, 2, INV> {};
+template <bool INV> struct DFT<12, INV> : DFTNest<4, 3, INV> {};
+template <bool INV> struct DFT<14, INV> : DFTNest<7, 2, INV> {};
+template <bool INV> struct DFT<15, INV> : DFTNest<5, 3, INV> {};
 
 }  // namespace afc

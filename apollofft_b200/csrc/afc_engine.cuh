@@ -134,8 +134,14 @@ __device__ __forceinline__ C* run_stages(const Ctx& cx, const StageList& sl, con
       case 3: AFC_ST(3); break;
       case 4: AFC_ST(4); break;
       case 5: AFC_ST(5); break;
+      case 6: AFC_ST(6); break;
       case 7: AFC_ST(7); break;
       case 8: AFC_ST(8); break;
+      case 9: AFC_ST(9); break;
+      case 10: AFC_ST(10); break;
+      case 12: AFC_ST(12); break;
+      case 14: AFC_ST(14); break;
+      case 15: AFC_ST(15); break;
       case 11: AFC_ST(11); break;
       case 13: AFC_ST(13); break;
       case 16: AFC_ST(16); break;

@@ -402,8 +402,14 @@ __global__ void __launch_bounds__(256) tile_kernel(const __grid_constant__ KArgs
         case 3: AFC_TS(3); break;
         case 4: AFC_TS(4); break;
         case 5: AFC_TS(5); break;
+        case 6: AFC_TS(6); break;
         case 7: AFC_TS(7); break;
         case 8: AFC_TS(8); break;
+        case 9: AFC_TS(9); break;
+        case 10: AFC_TS(10); break;
+        case 12: AFC_TS(12); break;
+        case 14: AFC_TS(14); break;
+        case 15: AFC_TS(15); break;
         case 11: AFC_TS(11); break;
         case 13: AFC_TS(13); break;
         case 16: AFC_TS(16); break;

@@ -374,8 +374,14 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
           case 3: AFC_TM(3); break;
           case 4: AFC_TM(4); break;
           case 5: AFC_TM(5); break;
+          case 6: AFC_TM(6); break;
           case 7: AFC_TM(7); break;
           case 8: AFC_TM(8); break;
+          case 9: AFC_TM(9); break;
+          case 10: AFC_TM(10); break;
+          case 12: AFC_TM(12); break;
+          case 14: AFC_TM(14); break;
+          case 15: AFC_TM(15); break;
           case 16: AFC_TM(16); break;
           default: break;
         }
@@ -385,8 +391,14 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
           case 3: AFC_TM(3); break;
           case 4: AFC_TM(4); break;
           case 5: AFC_TM(5); break;
+          case 6: AFC_TM(6); break;
           case 7: AFC_TM(7); break;
           case 8: AFC_TM(8); break;
+          case 9: AFC_TM(9); break;
+          case 10: AFC_TM(10); break;
+          case 12: AFC_TM(12); break;
+          case 14: AFC_TM(14); break;
+          case 15: AFC_TM(15); break;
           case 11: AFC_TM(11); break;
           case 13: AFC_TM(13); break;
           case 16: AFC_TM(16); break;
