@@ -31,7 +31,9 @@ def cplx(rng, shape, dtype=np.complex128):
 
 LENGTHS_1D = [1, 2, 3, 4, 5, 7, 8, 11, 13, 16, 17, 23, 31, 32, 45, 60, 64, 81, 97, 100, 128, 192, 243, 250, 256, 343,
               361, 512, 1000, 1009, 1024, 1031, 2048, 2053, 4096, 4099, 6561, 8192, 10007, 16384, 65536, 65521,
-              1 << 18]
+              1 << 18,
+              # composite radices 6 / 9 / 10 / 12 / 14 / 15 (nested butterflies) in every stage position
+              6, 12, 14, 15, 90, 168, 210, 225, 1960, 2430, 3375, 5040, 9261, 15120, 27000, 3 * 11 * 13 * 14]
 
 
 @pytest.mark.parametrize("n", LENGTHS_1D)

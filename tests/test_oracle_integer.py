@@ -140,3 +140,16 @@ def test_library_pfa_perm_matches_oracle(oracle, afc, n1, n2):
     oa, ob = oracle.pfa_perm(n1, n2)
     np.testing.assert_array_equal(a, oa)
     np.testing.assert_array_equal(b, ob)
+
+
+# The GPU stage factorization (this library's choice, not the reference's):
+# fewest stages over the register butterflies 2..16, composites 6, 9, 10, 12,
+# 14, 15 nested; powers of two keep radix 16 stages then one of 8 / 4 / 2.
+@pytest.mark.parametrize("n,rad", [(4096, [16, 16, 16]), (2048, [16, 16, 8]), (243, [9, 9, 3]),
+                                   (250, [10, 5, 5]), (343, [7, 7, 7]), (1000, [10, 10, 10]),
+                                   (45, [9, 5]), (12, [12]), (6, [6]), (2310, [11, 15, 14])])
+def test_gpu_stage_radices(afc, n, rad):
+    info = afc.length_info(n)
+    got = info["gpu_radices"]
+    assert sorted(got) == sorted(rad), (n, got)
+    assert int(np.prod(got)) == n
