@@ -375,12 +375,14 @@ struct AxisPlan {
   void* chirp = nullptr;
   void* spec_f = nullptr;
   void* spec_i = nullptr;
+  void* spec_rf = nullptr;           // large Bluestein: spectra in row-major [k1][k2] order
+  void* spec_ri = nullptr;
   int* gather = nullptr;
   int* scatter = nullptr;
   std::unique_ptr<AxisPlan> sub;     // four-step plan of length M (large Bluestein)
   int tuned_P = 0, tuned_L = 0;      // autotuned tile shape (batch plans)
   ~AxisPlan() {
-    void* ptrs[] = {lp.tw, lp1.tw, lp2.tw, tw_hi, tw_lo, chirp, spec_f, spec_i, gather, scatter};
+    void* ptrs[] = {lp.tw, lp1.tw, lp2.tw, tw_hi, tw_lo, chirp, spec_f, spec_i, spec_rf, spec_ri, gather, scatter};
     for (void* p : ptrs)
       if (p) cudaFree(p);
   }
@@ -681,7 +683,17 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
         d.L = choose_L(ap.lp, io.lanes, true, true, csz, 2 * csz, 2);
         return do_conv(d, dbl, inv, st);
       }
-      // Bluestein with a four-step convolution: 4 passes over two workspaces.
+      // Bluestein with a four-step convolution of length M = N1 x N2, three
+      // passes over two workspaces (input n = N2 n1 + n2, spectrum k = k1 + N1 k2):
+      //   1. columns n2: chirp premultiply, DFT_N1 over n1, twiddle W_M^{n2 k1}
+      //      -> w1[k1 N2 + n2];
+      //   2. rows k1 (one convolution tile): DFT_N2 over n2, times the
+      //      spectrum at k1 + N1 k2, inverse DFT_N2 back over n2, conjugate
+      //      twiddle W_M^{-n2 k1} -> w2[k1 N2 + n2];
+      //   3. columns n2: inverse DFT_N1 over k1, chirp postmultiply -> output
+      //      index N2 n1 + n2 (kept for indices < n).
+      // The forward DFT's output stays in the transposed order between the
+      // two row transforms, so no transpose pass is needed.
       const AxisPlan& mp = *ap.sub;
       const long long M = ap.M, N1 = mp.N1, N2 = mp.N2, d2 = io.im.d2;
       char* w1 = static_cast<char*>(ws);
@@ -715,47 +727,44 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
       fill_common(b, mp.lp2);
       b.lanes = io.lanes * N1;
       b.im = LaneMap{N1, d2, d2 * M, N2, M, 1, nullptr};
-      b.om = LaneMap{N1, d2, d2 * M, 1, M, N1, nullptr};
+      b.om = b.im;
       b.in = w1;
       b.out = w2;
-      b.out_op = OUT_MUL;
-      b.spec = inv ? ap.spec_i : ap.spec_f;
-      b.jmul = N1;
+      b.in_op = IN_C;
+      b.out_op = OUT_TW;
+      b.tw_conj = 1;
+      b.twN = M;
+      b.twB = mp.twB;
+      b.tw_hi = mp.tw_hi;
+      b.tw_lo = mp.tw_lo;
+      b.spec = inv ? ap.spec_ri : ap.spec_rf;
+      b.spec_ld = N2;
       b.col_div = d2;
       b.col_mod = N1;
-      b.stage_out = true;
-      b.L = choose_L(mp.lp2, b.lanes, b.stage_in, b.stage_out, csz);
-      e = do_lanes(b, dbl, false, st);
+      b.L = choose_L(mp.lp2, b.lanes, true, true, csz, 2 * csz + 3 * sizeof(long long), 2);
+      e = do_conv(b, dbl, false, st);
       if (e != cudaSuccess) return e;
-      LaunchDesc c = a;
-      c.tw_conj = 1;
+      LaunchDesc c;
+      fill_common(c, mp.lp1);
+      c.lanes = io.lanes * N2;
       c.im = LaneMap{N2, d2, d2 * M, 1, M, N2, nullptr};
+      c.om = io.om.off ? LaneMap{1, N2, 0, 0, io.om.es, N2 * io.om.es, io.om.off}
+                       : LaneMap{N2, io.om.d2, io.om.s0, io.om.es, io.om.s2, N2 * io.om.es, nullptr};
       c.in = w2;
+      c.out = io.out;
       c.in_op = IN_C;
-      c.out = w1;
+      c.out_op = real_out ? OUT_CHIRP_RE : OUT_CHIRP;
+      c.scale = io.scale;
+      c.jmul = N2;
+      c.col_div = d2;
+      c.col_mod = N2;
+      c.nlen = io.out_op == OUT_TRUNC ? io.nlen : ap.n;
+      c.chirp = ap.chirp;
+      c.chirp_conj = inv ? 1 : 0;
       c.stage_in = true;
+      c.stage_out = true;
       c.L = choose_L(mp.lp1, c.lanes, c.stage_in, c.stage_out, csz);
-      e = do_lanes(c, dbl, true, st);
-      if (e != cudaSuccess) return e;
-      LaunchDesc f;
-      fill_common(f, mp.lp2);
-      f.lanes = io.lanes * N1;
-      f.im = LaneMap{N1, d2, d2 * M, N2, M, 1, nullptr};
-      f.om = io.om.off ? LaneMap{1, N1, 0, 0, io.om.es, N1 * io.om.es, io.om.off}
-                       : LaneMap{N1, io.om.d2, io.om.s0, io.om.es, io.om.s2, N1 * io.om.es, nullptr};
-      f.in = w1;
-      f.out = io.out;
-      f.out_op = real_out ? OUT_CHIRP_RE : OUT_CHIRP;
-      f.scale = io.scale;
-      f.jmul = N1;
-      f.col_div = d2;
-      f.col_mod = N1;
-      f.nlen = io.out_op == OUT_TRUNC ? io.nlen : ap.n;
-      f.chirp = ap.chirp;
-      f.chirp_conj = inv ? 1 : 0;
-      f.stage_out = true;
-      f.L = choose_L(mp.lp2, f.lanes, f.stage_in, f.stage_out, csz);
-      return do_lanes(f, dbl, true, st);
+      return do_lanes(c, dbl, true, st);
     }
     default:
       return cudaSuccess;
@@ -925,7 +934,13 @@ static afc_status build_axis(int64_t n, bool dbl, AxisPlan& ap, cudaStream_t st)
   if (s != AFC_OK) return s;
   s = fft_table(*ap.sub, dbl, ap.spec_f, st);
   if (s == AFC_OK) s = fft_table(*ap.sub, dbl, ap.spec_i, st);
-  return s;
+  if (s != AFC_OK) return s;
+  // the fused middle pass reads each row k1 of the spectrum contiguously
+  AFC_CUDA(dev_alloc(&ap.spec_rf, (size_t)M * csz), "Bluestein spectrum");
+  AFC_CUDA(dev_alloc(&ap.spec_ri, (size_t)M * csz), "Bluestein spectrum");
+  AFC_CUDA(gen_row_spectrum_dev(ap.spec_rf, ap.spec_f, ap.sub->N1, ap.sub->N2, dbl, st), "Bluestein spectrum");
+  AFC_CUDA(gen_row_spectrum_dev(ap.spec_ri, ap.spec_i, ap.sub->N1, ap.sub->N2, dbl, st), "Bluestein spectrum");
+  return AFC_OK;
 }
 
 // ───────────────────────────── plans ─────────────────────────────

@@ -32,6 +32,7 @@ struct LaunchDesc {
   const void* tw_hi = nullptr;
   const void* tw_lo = nullptr;
   const void* spec = nullptr;
+  long long spec_ld = 0;  // convolution tiles: lane spectrum = spec + col * spec_ld (0: one spectrum for all lanes)
   const void* chirp = nullptr;
   int chirp_conj = 0;
   const int* gather = nullptr;
@@ -55,7 +56,7 @@ inline size_t lanes_smem_bytes(const LaunchDesc& d, size_t csz) {
 }
 // conv_kernel: L lanes x 2 buffers x ld + 2 L extra complex + 2 L lane descriptors
 inline size_t conv_smem_bytes(const LaunchDesc& d, size_t csz) {
-  return (size_t)d.L * 2 * (size_t)d.ld * csz + (size_t)d.L * 2 * csz + (size_t)d.L * 2 * sizeof(long long);
+  return (size_t)d.L * 2 * (size_t)d.ld * csz + (size_t)d.L * 2 * csz + (size_t)d.L * 3 * sizeof(long long);
 }
 
 // tile_kernel: 3 buffers of L x ld elements + 4 L lane bases
@@ -112,6 +113,7 @@ int batch_blocks_per_sm(size_t smem, bool dbl, bool inv);
 cudaError_t launch_tile(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st);
 cudaError_t launch_conv(const LaunchDesc& d, bool dbl, cudaStream_t st);
 
+cudaError_t gen_row_spectrum_dev(void* dst, const void* src, long long N1, long long N2, bool dbl, cudaStream_t st);
 cudaError_t gen_stage_twiddles_dev(void* tw, const StageList& sl, bool dbl, cudaStream_t st);
 cudaError_t gen_roots_dev(void* out, long long cnt, long long mult, long long N, bool dbl, cudaStream_t st);
 cudaError_t gen_chirp_dev(void* out, long long n, bool dbl, cudaStream_t st);

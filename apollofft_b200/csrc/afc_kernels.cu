@@ -45,6 +45,7 @@ template <class T> struct KArgs {
   const C* tw_hi;
   const C* tw_lo;
   const C* spec;           // pointwise spectrum
+  long long spec_ld;       // convolution tiles: lane spectrum = spec + col * spec_ld (0: shared)
   const C* chirp;          // Bluestein chirp (forward sign; conj if chirp_conj)
   int chirp_conj;
   const int* gather;       // Rader: gather[q] = g^q mod p
@@ -441,13 +442,14 @@ __device__ __forceinline__ void conv_tile(const KArgs<T>& a, long long q0, unsig
   const int t = active ? tid - l * P : (1 << 30);  // idle threads own no butterfly
   const bool rader = a.in_op == IN_GATHER || a.in_op == IN_GATHER_R;
   C* extra = sm + (long long)L * 2 * ld;                         // [2L]: x0, DC per lane
-  long long* lb = reinterpret_cast<long long*>(extra + 2 * L);   // [2L]: in base, out base
+  long long* lb = reinterpret_cast<long long*>(extra + 2 * L);   // [3L]: in base, out base, col
   const int lanes_here = (int)((a.lanes - q0) < L ? (a.lanes - q0) : L);
   if (tid < L) {
     const long long qq = q0 + tid;
     const bool v = tid < lanes_here;
     lb[tid] = v ? a.im.base(qq) : 0;
     lb[L + tid] = v ? a.om.base(qq) : 0;
+    lb[2 * L + tid] = v ? col_of(a, qq) : 0;
     C x0 = C{(T)0, (T)0};
     if (v && rader) x0 = a.in_op == IN_GATHER ? static_cast<const C*>(a.in)[lb[tid]] : C{static_cast<const T*>(a.in)[lb[tid]], (T)0};
     extra[2 * tid] = x0;
@@ -468,7 +470,7 @@ __device__ __forceinline__ void conv_tile(const KArgs<T>& a, long long q0, unsig
   for (int e = tid; e < lanes_here * M; e += blockDim.x) {
     const int l2 = e % lanes_here, i = e / lanes_here;
     C* p = sm + (long long)l2 * 2 * ld + off + spad(i);
-    *p = cmul(*p, a.spec[i]);
+    *p = cmul(*p, a.spec[lb[2 * L + l2] * a.spec_ld + i]);
   }
   __syncthreads();
   // the inverse FFT starts from the buffer holding the product
@@ -477,7 +479,7 @@ __device__ __forceinline__ void conv_tile(const KArgs<T>& a, long long q0, unsig
   const long long off2 = (long long)(res2 - b0);
   for (int e = tid; e < lanes_here * M; e += blockDim.x) {
     const int l2 = e % lanes_here, i = e / lanes_here;
-    gstore(a, lb[L + l2], 0, i, sm[(long long)l2 * 2 * ld + off2 + spad(i)], extra[2 * l2]);
+    gstore(a, lb[L + l2], lb[2 * L + l2], i, sm[(long long)l2 * 2 * ld + off2 + spad(i)], extra[2 * l2]);
   }
   if (rader && tid < lanes_here) {
     const C dc = cscale(cadd(extra[2 * tid], extra[2 * tid + 1]), a.scale);
@@ -620,6 +622,16 @@ __global__ void gen_rader_b(typename CT<T>::type* b, const int* scatter, long lo
   }
 }
 
+// Row-major spectrum for the fused middle pass of a large Bluestein
+// convolution: dst[k1 N2 + k2] = src[k1 + N1 k2] (natural index k = k1 + N1 k2).
+template <class T>
+__global__ void gen_row_spectrum(typename CT<T>::type* dst, const typename CT<T>::type* src, long long N1, long long N2) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < N1 * N2; e += (long long)gridDim.x * blockDim.x) {
+    const long long k1 = e / N2, k2 = e % N2;
+    dst[e] = src[k1 + N1 * k2];
+  }
+}
+
 // ─────────────────────────────── launchers ────────────────────────────────
 
 template <class T> static KArgs<T> to_kargs(const LaunchDesc& d) {
@@ -653,6 +665,7 @@ template <class T> static KArgs<T> to_kargs(const LaunchDesc& d) {
   a.tw_hi = static_cast<const C*>(d.tw_hi);
   a.tw_lo = static_cast<const C*>(d.tw_lo);
   a.spec = static_cast<const C*>(d.spec);
+  a.spec_ld = d.spec_ld;
   a.chirp = static_cast<const C*>(d.chirp);
   a.chirp_conj = d.chirp_conj;
   a.gather = d.gather;
@@ -787,6 +800,16 @@ static unsigned table_grid(long long n) {
 cudaError_t gen_stage_twiddles_dev(void* tw, const StageList& sl, bool dbl, cudaStream_t st) {
   if (dbl) gen_stage_twiddles<double><<<table_grid(sl.n), 256, 0, st>>>(static_cast<double2*>(tw), sl);
   else gen_stage_twiddles<float><<<table_grid(sl.n), 256, 0, st>>>(static_cast<float2*>(tw), sl);
+  count_launch(1);
+  return cudaGetLastError();
+}
+cudaError_t gen_row_spectrum_dev(void* dst, const void* src, long long N1, long long N2, bool dbl, cudaStream_t st) {
+  if (dbl)
+    gen_row_spectrum<double><<<table_grid(N1 * N2), 256, 0, st>>>(static_cast<double2*>(dst),
+                                                                   static_cast<const double2*>(src), N1, N2);
+  else
+    gen_row_spectrum<float><<<table_grid(N1 * N2), 256, 0, st>>>(static_cast<float2*>(dst),
+                                                                 static_cast<const float2*>(src), N1, N2);
   count_launch(1);
   return cudaGetLastError();
 }
