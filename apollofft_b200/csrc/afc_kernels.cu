@@ -455,9 +455,27 @@ __device__ __forceinline__ void conv_tile(const KArgs<T>& a, long long q0, unsig
     extra[2 * tid] = x0;
   }
   __syncthreads();
-  for (int e = tid; e < lanes_here * M; e += blockDim.x) {
-    const int l2 = e % lanes_here, i = e / lanes_here;
-    sm[(long long)l2 * 2 * ld + spad(i)] = gload(a, lb[l2], 0, i);
+  {
+    // four independent loads in flight per thread before their shared stores
+    const int total = lanes_here * M, stride = blockDim.x;
+    int e = tid;
+    for (; e + 3 * stride < total; e += 4 * stride) {
+      C v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int ee = e + u * stride;
+        v[u] = gload(a, lb[ee % lanes_here], 0, ee / lanes_here);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int ee = e + u * stride;
+        sm[(long long)(ee % lanes_here) * 2 * ld + spad(ee / lanes_here)] = v[u];
+      }
+    }
+    for (; e < total; e += stride) {
+      const int l2 = e % lanes_here, i = e / lanes_here;
+      sm[(long long)l2 * 2 * ld + spad(i)] = gload(a, lb[l2], 0, i);
+    }
   }
   __syncthreads();
   C* b0 = sm + (long long)l * 2 * ld;
@@ -467,10 +485,28 @@ __device__ __forceinline__ void conv_tile(const KArgs<T>& a, long long q0, unsig
   const long long off = (long long)(res - b0);
   if (tid < lanes_here) extra[2 * tid + 1] = sm[(long long)tid * 2 * ld + off];  // DC = sum of the gathered values
   __syncthreads();
-  for (int e = tid; e < lanes_here * M; e += blockDim.x) {
-    const int l2 = e % lanes_here, i = e / lanes_here;
-    C* p = sm + (long long)l2 * 2 * ld + off + spad(i);
-    *p = cmul(*p, a.spec[lb[2 * L + l2] * a.spec_ld + i]);
+  {
+    const int total = lanes_here * M, stride = blockDim.x;
+    int e = tid;
+    for (; e + 3 * stride < total; e += 4 * stride) {
+      C w[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int ee = e + u * stride;
+        w[u] = a.spec[lb[2 * L + ee % lanes_here] * a.spec_ld + ee / lanes_here];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int ee = e + u * stride;
+        C* p = sm + (long long)(ee % lanes_here) * 2 * ld + off + spad(ee / lanes_here);
+        *p = cmul(*p, w[u]);
+      }
+    }
+    for (; e < total; e += stride) {
+      const int l2 = e % lanes_here, i = e / lanes_here;
+      C* p = sm + (long long)l2 * 2 * ld + off + spad(i);
+      *p = cmul(*p, a.spec[lb[2 * L + l2] * a.spec_ld + i]);
+    }
   }
   __syncthreads();
   // the inverse FFT starts from the buffer holding the product
