@@ -195,151 +195,222 @@ __global__ void __launch_bounds__(128) tc_selftest_kernel(const float* A, const 
 }
 
 // ───────────────────────── tensor-core FFT of 16^s points ─────────────────────────
-// One CTA (128 threads) transforms one lane at a time (persistent over lanes):
-// the lane is loaded into shared memory (f32 complex), each radix-16 stage runs
-// in groups of 128 butterflies through the tensor cores, the last stage's
-// outputs are stored to global memory (scaled for the inverse).
+// Persistent CTAs of 256 threads over tiles of L = 4096 / n lanes, so every
+// radix-16 stage has exactly 256 butterflies = two 128-row MMA tiles, one per
+// thread.  Lanes arrive by 1D bulk copy (two slots: the next tile's copy flies
+// while this one is transformed) and leave by bulk store.  Per stage, in place
+// in the slot: each thread gathers its butterfly's 16 inputs and twiddles
+// them (FP32), splits them into hi / lo rows of its A tile, one thread issues
+// the 2 x 6 MMAs (Xh Fh, Xh Fl, Xl Fh over two K halves per tile; Xl Fl is
+// below FP32 rounding and skipped) and commits to an mbarrier, and each thread
+// reads its row of the accumulators back from TMEM (warp w: lanes 32 (w mod 4),
+// columns 32 (w / 4)) and writes its 16 outputs in Stockham order.
 
 struct TcArgs {
   const float2* in;
   float2* out;
-  const float2* tw;   // stage twiddles of the radix-16 plan (same layout as the SIMT plan)
+  const float2* tw;   // stage twiddles of the radix-16 plan (r-major, same table as the SIMT plan)
   StageList sl;
-  long long lanes;
+  long long lanes, ntiles;
+  int L, ld, slot_elems;
   float scale;
   int inverse;
   unsigned* err;
 };
 
+__device__ __forceinline__ void tcb_expect_tx(unsigned long long* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(tc_smem(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tcb_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   tc_smem(dst)),
+               "l"(src), "r"(bytes), "r"(tc_smem(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tcb_store(void* dst, const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(tc_smem(src)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void tcb_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void tcb_wait0() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc64(unsigned* dst_smem) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;\n" ::"r"(tc_smem(dst_smem))
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc64(unsigned taddr) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;\n" ::"r"(taddr) : "memory");
+}
+
+__device__ __forceinline__ void tc_issue_load(const TcArgs& a, long long tile, float2* slot, unsigned long long* bar) {
+  const long long q0 = tile * a.L;
+  const long long rem = a.lanes - q0;
+  const int here = (int)(rem < a.L ? rem : a.L);
+  const unsigned bytes = (unsigned)((long long)here * a.sl.n * sizeof(float2));
+  tcb_expect_tx(bar, bytes);
+  tcb_load(slot, a.in + q0 * a.sl.n, bytes, bar);
+}
+
 template <bool FP16>
-__global__ void __launch_bounds__(128) tc_fft_kernel(const __grid_constant__ TcArgs a) {
+__global__ void __launch_bounds__(256, 2) tc_fft_kernel(const __grid_constant__ TcArgs a) {
   // Declared 16-byte aligned on purpose: with separately compiled device code
   // the dynamic block starts at any 16-byte boundary after the static
   // variables (0x410 here), whatever alignment the declaration claims, and a
   // larger claimed alignment lets the compiler fold the padding below to zero.
   // Operand tiles off a 1024-byte boundary read back wrong in the MMA.
   extern __shared__ __align__(16) unsigned char smraw[];
-  // layout from the first 1024-byte boundary: Ah 8K | Al 8K | Fh 2K | Fl 2K | bufA n*8 | bufB n*8
-  unsigned char* Ah = smraw + ((1024u - (tc_smem(smraw) & 1023u)) & 1023u);
-  unsigned char* Al = Ah + 8192;
-  unsigned char* Fh = Al + 8192;
+  // layout from the first 1024-byte boundary:
+  // A0h 8K | A0l 8K | A1h 8K | A1l 8K | Fh 2K | Fl 2K | slot0 | slot1
+  unsigned char* A = smraw + ((1024u - (tc_smem(smraw) & 1023u)) & 1023u);
+  unsigned char* Fh = A + 4 * 8192;
   unsigned char* Fl = Fh + 2048;
-  const int n = a.sl.n;
-  float2* bufA = reinterpret_cast<float2*>(Fl + 2048);
-  float2* bufB = bufA + n;
-  __shared__ __align__(8) unsigned long long bar;
+  float2* slots[2];
+  slots[0] = reinterpret_cast<float2*>(Fl + 2048);
+  slots[1] = slots[0] + a.slot_elems;
+  __shared__ __align__(8) unsigned long long bars[3];  // two slot loads, one MMA completion
   __shared__ unsigned tslot;
   const int t = threadIdx.x;
-  if (t < 32) tmem_alloc32(&tslot);
-  if (t == 0) tc_mbar_init(&bar);
+  long long tile = blockIdx.x;
+  if (tile >= a.ntiles) return;  // uniform: before any TMEM allocation
+  const int n = a.sl.n, nb = n / 16, ld = a.ld;
+  const int l = t / nb, j = t - l * nb;  // lane in the tile, butterfly in the lane (L nb = 256)
+  const int mt = t >> 7, row = t & 127;  // MMA tile and row of this butterfly
+  unsigned char* Ah = A + mt * 16384;
+  unsigned char* Al = Ah + 8192;
+  if (t < 32) tmem_alloc64(&tslot);
+  if (t == 0) {
+    tc_mbar_init(&bars[0]);
+    tc_mbar_init(&bars[1]);
+    tc_mbar_init(&bars[2]);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
   build_dft16<FP16>(Fh, Fl, a.inverse != 0);
   tc_proxy_fence();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const unsigned taddr = tslot;
-  const unsigned trow = taddr + ((unsigned)((t >> 5) * 32) << 16);
+  const unsigned trow = taddr + ((unsigned)(((t >> 5) & 3) * 32) << 16) + (unsigned)(32 * mt);
   const uint32_t id = umma_idesc(FP16 ? 0u : 1u);
-  unsigned phase = 0;
+  if (t == 0) tc_issue_load(a, tile, slots[0], &bars[0]);
+  unsigned mphase = 0;
   bool failed = false;
-  const int nb = n / 16;
-  for (long long lane = blockIdx.x; lane < a.lanes && !failed; lane += gridDim.x) {
-    const float2* src = a.in + lane * n;
-    for (int i = t; i < n; i += 128) bufA[i] = src[i];
-    __syncthreads();
-    float2* cur = bufA;
-    float2* nxt = bufB;
-    for (int s = 0; s < a.sl.nst && !failed; ++s) {
+  for (int it = 0; !failed; ++it) {
+    const int cb = it & 1;
+    const long long nxt = tile + gridDim.x;
+    if (t == 0) {
+      tcb_wait_read0();  // the previous tile's store has finished reading its slot
+      if (nxt < a.ntiles) tc_issue_load(a, nxt, slots[cb ^ 1], &bars[cb ^ 1]);
+    }
+    const bool okl = tc_mbar_wait(&bars[cb], (unsigned)((it >> 1) & 1));
+    if (__syncthreads_or(!okl)) {
+      if (t == 0) {
+        atomicExch(a.err, 1u);
+        if (nxt < a.ntiles) tc_mbar_wait(&bars[cb ^ 1], (unsigned)(((it + 1) >> 1) & 1));
+      }
+      failed = true;
+      break;
+    }
+    float2* cur = slots[cb];
+    for (int s = 0; s < a.sl.nst; ++s) {
       const int Ns = a.sl.st[s].Ns;
       const float2* tws = a.tw + a.sl.st[s].twoff;
       const bool last = s == a.sl.nst - 1;
-      for (int g = 0; g < nb; g += 128) {
-        const int j = g + t;
-        const bool have = j < nb;
-        const int k = have ? j % Ns : 0;
-        float v[32];
-        float sc = 1.0f;
-        if (have) {
+      const int k = j % Ns;
+      float v[32];
+      float sc = 1.0f;
 #pragma unroll
-          for (int r = 0; r < 16; ++r) {
-            float2 x = cur[j + r * nb];
-            if (Ns > 1 && r > 0) {
-              const float2 w = tws[(long long)(r - 1) * Ns + k];
-              const float wy = a.inverse ? -w.y : w.y;
-              x = make_float2(x.x * w.x - x.y * wy, x.x * wy + x.y * w.x);
-            }
-            v[r] = x.x;
-            v[16 + r] = x.y;
-          }
-          if (FP16) {  // power-of-two block scale: largest magnitude near 2^11
-            float m = 0.f;
-#pragma unroll
-            for (int r = 0; r < 32; ++r) m = fmaxf(m, fabsf(v[r]));
-            int e = 0;
-            frexpf(m, &e);
-            sc = m > 0.f ? ldexpf(1.0f, 11 - e) : 1.0f;
-#pragma unroll
-            for (int r = 0; r < 32; ++r) v[r] *= sc;
-          }
-        } else {
-#pragma unroll
-          for (int r = 0; r < 32; ++r) v[r] = 0.f;
+      for (int r = 0; r < 16; ++r) {
+        const int i = j + r * nb;
+        float2 x = s == 0 ? cur[l * n + i] : cur[l * ld + i + (i >> 4)];
+        if (Ns > 1 && r > 0) {
+          const float2 w = tws[(long long)(r - 1) * Ns + k];
+          const float wy = a.inverse ? -w.y : w.y;
+          x = make_float2(x.x * w.x - x.y * wy, x.x * wy + x.y * w.x);
         }
-        split_row<FP16>(Ah, Al, t, v);
-        tc_proxy_fence();
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        if (t == 0) {
-          const unsigned char* As[2] = {Ah, Al};
-          const unsigned char* Bs[2] = {Fh, Fl};
-          int first = 1;
-          for (int ai = 0; ai < 2; ++ai)
-            for (int bi = 0; bi < 2; ++bi)
-              for (int ks = 0; ks < 2; ++ks) {
-                tc_mma(taddr, umma_desc(As[ai] + ks * 256), umma_desc(Bs[bi] + ks * 256), id, first ? 0u : 1u);
-                first = 0;
-              }
-          tc_commit(&bar);
-        }
-        const bool ok = tc_mbar_wait(&bar, phase);
-        phase ^= 1u;
-        if (__syncthreads_or(!ok)) {
-          if (t == 0) atomicExch(a.err, 1u);
-          failed = true;
-          break;
-        }
-        tc_fence_after();
-        float o[32];
-        tmem_ld32(trow, o);
-        if (have) {
-          const float inv_sc = 1.0f / sc;
-          const int ob = (j - k) * 16 + k;
-#pragma unroll
-          for (int r = 0; r < 16; ++r) {
-            float2 y = make_float2(o[r] * inv_sc, o[16 + r] * inv_sc);
-            if (last) {
-              y.x *= a.scale;
-              y.y *= a.scale;
-              a.out[lane * n + ob + r * Ns] = y;
-            } else {
-              nxt[ob + r * Ns] = y;
-            }
-          }
-        }
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
+        v[r] = x.x;
+        v[16 + r] = x.y;
       }
-      float2* tmp = cur;
-      cur = nxt;
-      nxt = tmp;
+      if (FP16) {  // power-of-two row scale: largest magnitude near 2^11
+        float m = 0.f;
+#pragma unroll
+        for (int r = 0; r < 32; ++r) m = fmaxf(m, fabsf(v[r]));
+        int e = 0;
+        frexpf(m, &e);
+        sc = (m > 0.f && m < 3.0e38f) ? ldexpf(1.0f, 11 - e) : 1.0f;
+#pragma unroll
+        for (int r = 0; r < 32; ++r) v[r] *= sc;
+      }
+      split_row<FP16>(Ah, Al, row, v);
+      tc_proxy_fence();
+      tc_fence_before();
+      __syncthreads();  // every gather of this stage is done: the slot may be overwritten below
+      tc_fence_after();
+      if (t == 0) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const unsigned char* qh = A + q * 16384;
+          const unsigned char* ql = qh + 8192;
+          const uint32_t d = taddr + 32 * q;
+#pragma unroll
+          for (int ks = 0; ks < 2; ++ks) {
+            tc_mma(d, umma_desc(qh + ks * 256), umma_desc(Fh + ks * 256), id, ks);
+            tc_mma(d, umma_desc(qh + ks * 256), umma_desc(Fl + ks * 256), id, 1u);
+            tc_mma(d, umma_desc(ql + ks * 256), umma_desc(Fh + ks * 256), id, 1u);
+          }
+        }
+        tc_commit(&bars[2]);
+      }
+      const bool okm = tc_mbar_wait(&bars[2], mphase);
+      mphase ^= 1u;
+      if (__syncthreads_or(!okm)) {
+        if (t == 0) atomicExch(a.err, 1u);
+        failed = true;
+        break;
+      }
+      tc_fence_after();
+      float o[32];
+      tmem_ld32(trow, o);
+      const float inv_sc = 1.0f / sc;
+      const int ob = (j - k) * 16 + k;
+#pragma unroll
+      for (int r = 0; r < 16; ++r) {
+        const int pos = ob + r * Ns;
+        float2 y = make_float2(o[r] * inv_sc, o[16 + r] * inv_sc);
+        if (last) {
+          y.x *= a.scale;
+          y.y *= a.scale;
+          cur[l * n + pos] = y;
+        } else {
+          cur[l * ld + pos + (pos >> 4)] = y;
+        }
+      }
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
     }
+    if (failed) {
+      if (t == 0 && nxt < a.ntiles) tc_mbar_wait(&bars[cb ^ 1], (unsigned)(((it + 1) >> 1) & 1));
+      break;
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (t == 0) {
+      const long long q0 = tile * a.L;
+      const long long rem = a.lanes - q0;
+      const int here = (int)(rem < a.L ? rem : a.L);
+      tcb_store(a.out + q0 * n, cur, (unsigned)((long long)here * n * sizeof(float2)));
+    }
+    tile = nxt;
+    if (tile >= a.ntiles) break;
   }
+  if (t == 0) tcb_wait0();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (t < 32) tmem_dealloc32(taddr);
+  if (t < 32) tmem_dealloc64(taddr);
 }
 
 cudaError_t launch_tc_selftest(const float* A, const float* B, float* D, unsigned* err, bool fp16, cudaStream_t st) {
@@ -349,9 +420,26 @@ cudaError_t launch_tc_selftest(const float* A, const float* B, float* D, unsigne
   return cudaGetLastError();
 }
 
-size_t tc_fft_smem(int n) { return 1024 + 8192 * 2 + 2048 * 2 + 2 * (size_t)n * sizeof(float2); }
+// Tile geometry for n = 16^s <= 4096: L = 4096 / n lanes (256 butterflies per
+// stage), slots of L x max(ld, n) complex64 (ld = n + n/16 + 1, odd).
+static void tc_geometry(int n, int& L, int& ld, int& slot) {
+  L = 4096 / n;
+  ld = n + (n - 1) / 16 + 1;
+  if ((ld & 1) == 0) ++ld;
+  slot = L * (ld > n ? ld : n);
+  slot = (slot + 15) / 16 * 16;  // 128-byte aligned second slot
+}
+
+size_t tc_fft_smem(int n) {
+  int L, ld, slot;
+  tc_geometry(n, L, ld, slot);
+  return 1024 + 4 * 8192 + 2 * 2048 + 2 * (size_t)slot * sizeof(float2);
+}
 
 cudaError_t launch_tc_fft(const TcLaunch& d, bool fp16, cudaStream_t st) {
+  if (d.lanes <= 0) return cudaSuccess;
+  // bulk copies move whole tiles: both buffers must start on a 16-byte boundary
+  if ((reinterpret_cast<uintptr_t>(d.in) | reinterpret_cast<uintptr_t>(d.out)) & 15) return cudaErrorInvalidValue;
   TcArgs a;
   memset(&a, 0, sizeof(a));
   a.in = static_cast<const float2*>(d.in);
@@ -359,6 +447,8 @@ cudaError_t launch_tc_fft(const TcLaunch& d, bool fp16, cudaStream_t st) {
   a.tw = static_cast<const float2*>(d.tw);
   a.sl = d.sl;
   a.lanes = d.lanes;
+  tc_geometry(d.sl.n, a.L, a.ld, a.slot_elems);
+  a.ntiles = (d.lanes + a.L - 1) / a.L;
   a.scale = (float)d.scale;
   a.inverse = d.inverse;
   a.err = d.err;
@@ -375,19 +465,19 @@ cudaError_t launch_tc_fft(const TcLaunch& d, bool fp16, cudaStream_t st) {
   if (fp16) {
     e = cudaFuncSetAttribute(tc_fft_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tc_fft_kernel<true>, 128, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tc_fft_kernel<true>, 256, smem);
   } else {
     e = cudaFuncSetAttribute(tc_fft_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tc_fft_kernel<false>, 128, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tc_fft_kernel<false>, 256, smem);
   }
   if (per < 1) per = 1;
-  // every resident CTA holds 32 TMEM columns; 512 columns per SM
-  if (per > 16) per = 16;
+  // every resident CTA holds 64 TMEM columns; 512 columns per SM
+  if (per > 8) per = 8;
   long long grid = (long long)sms * per;
-  if (grid > d.lanes) grid = d.lanes;
-  if (fp16) tc_fft_kernel<true><<<(unsigned)grid, 128, smem, st>>>(a);
-  else tc_fft_kernel<false><<<(unsigned)grid, 128, smem, st>>>(a);
+  if (grid > a.ntiles) grid = a.ntiles;
+  if (fp16) tc_fft_kernel<true><<<(unsigned)grid, 256, smem, st>>>(a);
+  else tc_fft_kernel<false><<<(unsigned)grid, 256, smem, st>>>(a);
   count_launch(1);
   return cudaGetLastError();
 }
