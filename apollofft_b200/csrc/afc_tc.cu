@@ -19,7 +19,9 @@
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include "afc_engine.cuh"
 #include "afc_internal.h"
@@ -461,16 +463,28 @@ cudaError_t launch_tc_fft(const TcLaunch& d, bool fp16, cudaStream_t st) {
     if (sms <= 0) sms = 148;
   }
   cudaError_t e;
-  int per = 1;
+  // CTAs per SM from the kernel's registers and shared memory (the occupancy
+  // query reports one CTA for this kernel although two fit)
+  cudaFuncAttributes fa;
   if (fp16) {
     e = cudaFuncSetAttribute(tc_fft_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tc_fft_kernel<true>, 256, smem);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, tc_fft_kernel<true>);
   } else {
     e = cudaFuncSetAttribute(tc_fft_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tc_fft_kernel<false>, 256, smem);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, tc_fft_kernel<false>);
   }
+  if (e != cudaSuccess) return e;
+  static int smem_sm = 0, smem_rsv = 0;
+  if (!smem_sm) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    if (smem_sm <= 0) smem_sm = 228 * 1024;
+  }
+  const int by_regs = fa.numRegs > 0 ? 65536 / (fa.numRegs * 256) : 1;
+  const int by_smem = (int)((size_t)smem_sm / (smem + fa.sharedSizeBytes + (size_t)smem_rsv));
+  int per = std::min(by_regs, by_smem);
   if (per < 1) per = 1;
   // every resident CTA holds 64 TMEM columns; 512 columns per SM
   if (per > 8) per = 8;
