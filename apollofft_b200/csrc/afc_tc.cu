@@ -104,30 +104,38 @@ __device__ __forceinline__ int kmaj_off(int row, int k) {
 template <bool FP16> struct Half;
 template <> struct Half<false> {
   using H = __nv_bfloat16;
+  using H2 = __nv_bfloat162;
   __device__ static H from(float v) { return __float2bfloat16_rn(v); }
   __device__ static float to(H h) { return __bfloat162float(h); }
+  __device__ static H2 from2(float a, float b) { return __floats2bfloat162_rn(a, b); }
+  __device__ static float2 to2(H2 h) { return __bfloat1622float2(h); }
 };
 template <> struct Half<true> {
   using H = __half;
+  using H2 = __half2;
   __device__ static H from(float v) { return __float2half_rn(v); }
   __device__ static float to(H h) { return __half2float(h); }
+  __device__ static H2 from2(float a, float b) { return __floats2half2_rn(a, b); }
+  __device__ static float2 to2(H2 h) { return __half22float2(h); }
 };
 
-// Writes one row (32 values) as hi and lo halves into two K-major tiles.
+// Writes one row (32 values) as hi and lo halves into two K-major tiles
+// (pairs converted together: one conversion per two values and half).
 template <bool FP16>
 __device__ __forceinline__ void split_row(unsigned char* hi, unsigned char* lo, int row, const float* v) {
   using HH = Half<FP16>;
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    alignas(16) typename HH::H h8[8], l8[8];
+    alignas(16) typename HH::H2 h4[4], l4[4];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const float x = v[c * 8 + e];
-      h8[e] = HH::from(x);
-      l8[e] = HH::from(x - HH::to(h8[e]));
+    for (int e = 0; e < 4; ++e) {
+      const float x0 = v[c * 8 + 2 * e], x1 = v[c * 8 + 2 * e + 1];
+      h4[e] = HH::from2(x0, x1);
+      const float2 hf = HH::to2(h4[e]);
+      l4[e] = HH::from2(x0 - hf.x, x1 - hf.y);
     }
-    *reinterpret_cast<uint4*>(hi + kmaj_off(row, c * 8)) = *reinterpret_cast<const uint4*>(h8);
-    *reinterpret_cast<uint4*>(lo + kmaj_off(row, c * 8)) = *reinterpret_cast<const uint4*>(l8);
+    *reinterpret_cast<uint4*>(hi + kmaj_off(row, c * 8)) = *reinterpret_cast<const uint4*>(h4);
+    *reinterpret_cast<uint4*>(lo + kmaj_off(row, c * 8)) = *reinterpret_cast<const uint4*>(l4);
   }
 }
 
