@@ -429,7 +429,10 @@ static afc_status build_fourstep(int64_t n, bool dbl, AxisPlan& ap, cudaStream_t
   if (s != AFC_OK) return s;
   s = build_lenplan(ap.N2, dbl, ap.lp2, st);
   if (s != AFC_OK) return s;
-  int64_t B = (int64_t)std::ceil(std::sqrt((double)n));
+  // two-level twiddle W_n^m = W_n^{B (m / B)} W_n^{m mod B}, B a power of two >= sqrt(n)
+  // so the kernels split m with a shift and a mask
+  int64_t B = 1;
+  while (B * B < n) B <<= 1;
   ap.twB = B;
   int64_t nhi = (n + B - 1) / B;
   AFC_CUDA(dev_alloc(&ap.tw_lo, (size_t)B * csz), "four-step twiddles");

@@ -115,9 +115,11 @@ __device__ __forceinline__ void gstore(const KArgs<T>& a, long long base, long l
       }
       return;
     }
-    case OUT_TW: {  // four-step: multiply by W_N^{col * i}
-      const long long m = (col * (long long)i) % a.twN;
-      const C w = cmul(a.tw_hi[m / a.twB], a.tw_lo[m % a.twB]);
+    case OUT_TW: {  // four-step: multiply by W_N^{col * i}; twB is a power of two
+      unsigned long long m = (unsigned long long)col * (unsigned long long)i;
+      if (m >= (unsigned long long)a.twN) m %= (unsigned long long)a.twN;  // col * i < N in every four-step pass
+      const int sh = __ffsll(a.twB) - 1;
+      const C w = cmul(a.tw_hi[m >> sh], a.tw_lo[m & (unsigned long long)(a.twB - 1)]);
       v = a.tw_conj ? cmulc(v, w) : cmul(v, w);
       static_cast<C*>(a.out)[off] = cscale(v, a.scale);
       return;
@@ -204,7 +206,22 @@ __device__ __forceinline__ void lanes_tile(const KArgs<T>& a, long long q0, unsi
   C* b0 = sm + (long long)l * nbuf * ld;
   C* b1 = b0 + (nbuf > 1 ? ld : 0);
   __syncthreads();
-  if (a.stage_in) {
+  if (a.stage_in && blockDim.x % lanes_here == 0) {
+    // the block covers whole rows: each thread keeps one lane, four loads in flight
+    const int l2 = tid % lanes_here, i0 = tid / lanes_here, di = blockDim.x / lanes_here;
+    const long long ib = lb[l2], colv = lb[2 * L + l2];
+    C* dstl = sm + (long long)l2 * nbuf * ld;
+    int i = i0;
+    for (; i + 3 * di < n; i += 4 * di) {
+      C v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = gload(a, ib, colv, i + u * di);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) dstl[spad(i + u * di)] = v[u];
+    }
+    for (; i < n; i += di) dstl[spad(i)] = gload(a, ib, colv, i);
+    __syncthreads();
+  } else if (a.stage_in) {
     // four independent loads in flight per thread before their shared stores
     const int total = lanes_here * n;
     const int stride = blockDim.x;
@@ -232,7 +249,14 @@ __device__ __forceinline__ void lanes_tile(const KArgs<T>& a, long long q0, unsi
   }
   const Ctx<T> cx{a, lb[l], lb[L + l], active && l < lanes_here};
   C* res = run_stages<INV>(cx, a.sl, a.tw, t, P, b0, b1, a.stage_in != 0, a.stage_out != 0);
-  if (a.stage_out) {
+  if (a.stage_out && blockDim.x % lanes_here == 0) {
+    const long long off = res ? (long long)(res - b0) : 0;
+    const C z = C{(T)0, (T)0};
+    const int l2 = tid % lanes_here, di = blockDim.x / lanes_here;
+    const long long ob = lb[L + l2], colv = lb[2 * L + l2];
+    const C* srcl = sm + (long long)l2 * nbuf * ld + off;
+    for (int i = tid / lanes_here; i < n; i += di) gstore(a, ob, colv, i, srcl[spad(i)], z);
+  } else if (a.stage_out) {
     // every lane ends in the same buffer slot: offset of res within its lane block
     const long long off = res ? (long long)(res - b0) : 0;
     const int total = lanes_here * n;
