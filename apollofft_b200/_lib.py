@@ -91,6 +91,8 @@ SIGNATURES = {
     "afc_last_error_message": (ctypes.c_char_p, []),
     "afc_kernel_launch_count": (_u64, []),
     "afc_execute_1d_no_alloc": (_i32, [_vp, _vp, _vp, _i32, _vp]),
+    "afc_stft_frame_count": (_i32, [_i64, _i64, _i64, _pi64]),
+    "afc_stft_forward": (_i32, [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp]),
 }
 
 _lib = None

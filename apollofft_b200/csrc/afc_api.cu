@@ -1660,6 +1660,67 @@ afc_status afc_execute_ws(afc_plan plan, const void* in, void* out, afc_directio
   return execute(plan, in, out, direction, scale, use_scale != 0, 1.0, workspace, workspace_bytes, false, stream);
 }
 
+// STFT analysis frames of apollo-stft (stft/dimension_1d.rs:96-108): frames
+// centred at m hop, 1 + ceil(signal_len / hop) of them; none when the signal is
+// shorter than a frame.
+static int64_t stft_frames(int64_t frame_len, int64_t hop, int64_t signal_len) {
+  if (signal_len < frame_len) return 0;
+  return 1 + (signal_len + hop - 1) / hop;
+}
+
+afc_status afc_stft_frame_count(int64_t frame_len, int64_t hop, int64_t signal_len, int64_t* frames) {
+  if (!frames) return fail(AFC_ERR_VALIDATION, "validation failed for `frames`: `null` violates `must be non-null`");
+  if (frame_len < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `frame_len`: `%lld` violates `> 0`", (long long)frame_len);
+  if (hop < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `hop_len`: `%lld` violates `> 0`", (long long)hop);
+  *frames = stft_frames(frame_len, hop, signal_len < 0 ? 0 : signal_len);
+  return AFC_OK;
+}
+
+afc_status afc_stft_forward(afc_plan plan, const void* signal, int64_t signal_len, const void* window, int64_t hop,
+                            void* out, int64_t out_elems, void* stream) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (!signal || !window || !out)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  if (plan->rank != 1 || plan->kind != AFC_KIND_C2C || plan->tc)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `rank %d` violates `rank-1 C2C f32/f64 plan`", plan->rank);
+  const int64_t n = plan->dims[0];
+  if (hop < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `hop_len`: `%lld` violates `> 0`", (long long)hop);
+  if (hop > n)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `hop_len`: `%lld` violates `<= frame_len %lld`", (long long)hop,
+                (long long)n);
+  if (signal_len < n)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `signal_len`: `%lld` violates `>= frame_len %lld`",
+                (long long)signal_len, (long long)n);
+  const int64_t frames = stft_frames(n, hop, signal_len);
+  if (out_elems != frames * n)
+    return fail(AFC_ERR_SHAPE_MISMATCH, "shape mismatch: expected %lld output elements (%lld frames x %lld), got %lld",
+                (long long)(frames * n), (long long)frames, (long long)n, (long long)out_elems);
+  const AxisPlan& ap = *plan->axes[0];
+  if (ap.algo != ALGO_SMEM)
+    return fail(AFC_ERR_UNSUPPORTED, "fused STFT frames need a single-CTA frame length (got %lld)", (long long)n);
+  const size_t csz = plan->dbl ? 16 : 8;
+  DeviceGuard g(plan->device);
+  LaunchDesc d;
+  fill_common(d, ap.lp);
+  d.lanes = frames;
+  d.im = LaneMap{1, 1, hop, 0, 0, 1, nullptr};  // frame m: base m hop
+  d.om = LaneMap{1, 1, n, 0, 0, 1, nullptr};
+  d.in = signal;
+  d.out = out;
+  d.in_op = IN_FRAME;
+  d.out_op = OUT_C;
+  d.scale = 1.0;
+  d.nlen = signal_len;
+  d.window = window;
+  d.frame_off = n / 2;
+  d.stage_in = true;
+  d.stage_out = ap.lp.sl.nst <= 1;
+  d.L = choose_L(ap.lp, d.lanes, d.stage_in, d.stage_out, csz);
+  cudaError_t e = launch_lanes(d, plan->dbl, false, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "stft forward");
+  return AFC_OK;
+}
+
 afc_status afc_plan_io_elems(afc_plan plan, afc_direction direction, int64_t* in_elems, int64_t* out_elems) {
   if (!plan || !in_elems || !out_elems)
     return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");

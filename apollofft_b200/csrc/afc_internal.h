@@ -6,7 +6,7 @@
 
 namespace afc {
 
-enum InOpKind { IN_C = 0, IN_R = 1, IN_HERM = 2, IN_CHIRP = 3, IN_CHIRP_R = 4, IN_GATHER = 5, IN_GATHER_R = 6 };
+enum InOpKind { IN_C = 0, IN_R = 1, IN_HERM = 2, IN_CHIRP = 3, IN_CHIRP_R = 4, IN_GATHER = 5, IN_GATHER_R = 6, IN_FRAME = 7 };
 enum OutOpKind {
   OUT_C = 0, OUT_RE = 1, OUT_TRUNC = 2, OUT_TW = 3, OUT_MUL = 4, OUT_CHIRP = 5, OUT_CHIRP_RE = 6,
   OUT_SCATTER = 7, OUT_SCATTER_RE = 8
@@ -39,6 +39,8 @@ struct LaunchDesc {
   const int* scatter = nullptr;
   int lane_minor = 0;
   int in_sel = 0, out_sel = 0;  // batch descriptors: pointer = base[sel] + offset
+  const void* window = nullptr;  // IN_FRAME: analysis window (real, frame length)
+  long long frame_off = 0;       // IN_FRAME: frames start at lane base - frame_off
 };
 
 // A tile of the persistent batch kernel: descriptor index, kind (0 forward lanes

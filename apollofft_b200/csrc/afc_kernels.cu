@@ -52,6 +52,8 @@ template <class T> struct KArgs {
   const int* scatter;      // Rader: scatter[q] = g^{-q} mod p
   int lane_minor;          // tile kernel: consecutive threads take consecutive lanes
   int in_sel, out_sel;     // batch descriptors: 0 absolute pointer, else base[sel] + offset
+  const T* window;         // IN_FRAME: analysis window
+  long long frame_off;     // IN_FRAME: frame q covers signal[q hop - frame_off + i]
 };
 
 template <class T>
@@ -90,6 +92,11 @@ __device__ __forceinline__ typename CT<T>::type gload(const KArgs<T>& a, long lo
       if (i >= a.nlen - 1) return zero;
       const long long off = base + (long long)a.gather[i] * a.im.es;
       return a.in_op == IN_GATHER ? static_cast<const C*>(a.in)[off] : C{static_cast<const T*>(a.in)[off], (T)0};
+    }
+    case IN_FRAME: {  // STFT analysis frame: signal[base - frame_off + i] * window[i], zero outside the signal
+      const long long j = base - a.frame_off + i;
+      if (j < 0 || j >= a.nlen) return zero;
+      return C{static_cast<const T*>(a.in)[j] * a.window[i], (T)0};
     }
   }
   return zero;
@@ -726,6 +733,8 @@ template <class T> static KArgs<T> to_kargs(const LaunchDesc& d) {
   a.tw_lo = static_cast<const C*>(d.tw_lo);
   a.spec = static_cast<const C*>(d.spec);
   a.spec_ld = d.spec_ld;
+  a.window = static_cast<const T*>(d.window);
+  a.frame_off = d.frame_off;
   a.chirp = static_cast<const C*>(d.chirp);
   a.chirp_conj = d.chirp_conj;
   a.gather = d.gather;

@@ -186,6 +186,24 @@ AFC_API const char* afc_last_error_message(void);
 /* Number of kernels this library launched in this process (all devices). */
 AFC_API uint64_t afc_kernel_launch_count(void);
 
+/* ── fused caller operations ──────────────────────────────────────────────── */
+
+/* STFT analysis on the device, frames gathered and windowed inside the FFT's
+ * load: replaces the frame loop of apollo-stft StftPlan::forward_with_window /
+ * forward_f64_slice_into (apollo-stft/.../plan/stft/dimension_1d.rs:132-239),
+ * which copies each frame into a host slice and calls
+ * FftPlan1D::forward_complex_slice_inplace on it.  `plan` is a rank-1 C2C F32 or
+ * F64 plan of length frame_len whose length fits one CTA; `signal` (signal_len
+ * reals) and `window` (frame_len reals) are device arrays of the plan's real
+ * type; frame m covers signal[m hop - frame_len/2 + i] * window[i] (zero
+ * outside the signal), frames = 1 + ceil(signal_len / hop)
+ * (dimension_1d.rs:102-108); `out` receives frames x frame_len complex values,
+ * `out_elems` must equal that count.  Errors as the reference's StftError:
+ * hop 0 or hop > frame_len, signal shorter than a frame -> AFC_ERR_VALIDATION. */
+AFC_API afc_status afc_stft_frame_count(int64_t frame_len, int64_t hop, int64_t signal_len, int64_t* frames);
+AFC_API afc_status afc_stft_forward(afc_plan plan, const void* signal, int64_t signal_len, const void* window,
+                                    int64_t hop, void* out, int64_t out_elems, void* stream);
+
 /* Allocation-free execution of a rank-1 C2C plan whose length runs on the
  * two-pass (four-step) kernels: the intermediate between the passes lives in a
  * 16 MiB static device array instead of a cudaMalloc'd workspace, so the call
