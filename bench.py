@@ -273,7 +273,7 @@ def main():
     ap.add_argument("--shape", default=None, help="override the 3D shape, e.g. 128,256,256 (profiling cases)")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
     ap.add_argument("--quick", action="store_true", help="headline only: no other shapes, e2e or CPU legs")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "stft"],
                     help="c2 (default) is the headline; c1/c3/c4/c5 print their own lines")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -571,6 +571,41 @@ def run_secondary(args):
         line.update({"metric": "ms", "forward_ms": round(tf * 1e3, 3), "forward_backward_ms": round(tb * 1e3, 3),
                      "ratio": round(tb / tf, 3), "forward_gflops_r2c_convention": round(fl / tf / 1e9, 1),
                      "config": "8 x 2048^2 f32 real, full-spectrum R2C (reference contract), loss sum |w X|^2"})
+    elif args.workload == "stft":
+        # apollo-stft's analysis loop (frame copy + window + one FFT per frame) fused
+        # into the FFT load: 2^22 f64 samples, frame 1024, hop 256 (seeded N(0,1))
+        from apollofft_b200.stft import StftPlan
+        n_sig, frame_len, hop = 1 << 22, 1024, 256
+        sig_np = np.random.default_rng(11).standard_normal(n_sig)
+        sig = torch.from_numpy(sig_np).to(dev)
+        plan = StftPlan(frame_len, hop, precision="f64")
+        frames = plan.frame_count(n_sig)
+        out = torch.empty((frames, frame_len), dtype=torch.complex128, device=dev)
+        t = _events_time(lambda: plan.forward(sig, out=out), args.steps, args.warmup, torch)
+        fl = frames * 5 * frame_len * math.log2(frame_len)
+        byts = n_sig * 8 + frames * frame_len * 16
+        line.update({"metric": "GFLOP/s", "value": round(fl / t / 1e9, 1), "ms_per_step": round(t * 1e3, 4),
+                     "frames_per_s": round(frames / t, 1), "hbm_frac": round(byts / t / 1e9 / hbm_peak, 4),
+                     "config": f"STFT analysis f64: {n_sig} samples, frame {frame_len}, hop {hop}, {frames} frames, "
+                               "Hann window, one fused launch"})
+        # the reference's pattern on the host: per frame, window into a slice and
+        # transform it (oracle FftPlan1D<f64>), frames over all threads; bounded sample
+        from oracle import oracle as O
+        sub = min(frames, 4096)
+        win = plan.window
+        fr = np.zeros((sub, frame_len), dtype=np.complex128)
+        for m in range(sub):
+            st0 = m * hop - frame_len // 2
+            lo, hi = max(st0, 0), min(st0 + frame_len, n_sig)
+            fr[m, lo - st0:hi - st0] = sig_np[lo:hi] * win[lo - st0:hi - st0]
+        t0 = time.perf_counter()
+        ref = O.fft1d(fr)
+        tc = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(sub * 5 * frame_len * math.log2(frame_len) / tc / 1e9, 2),
+                                "unit": "GFLOP/s", "cores": O.max_threads(), "kind": "port",
+                                "sample": f"first {sub} frames: window + oracle FFT per frame (frame gather not timed)"}
+        got = out[:sub].cpu().numpy()
+        line["error_vs_oracle_rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
     print(json.dumps(line), flush=True)
     return 0
 
