@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
+#include <complex>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -990,6 +991,24 @@ struct afc_plan_s {
   }
 };
 
+// Chirp z-transform plan (apollo-czt CztPlan, plan/czt/dimension_1d.rs:60-120):
+// input length n, output length m, X_k = sum_j x_j A^-j W^(j k) by Bluestein's
+// identity over a convolution of length L = next_pow2(n + m - 1).
+struct afc_czt_plan_s {
+  int64_t n = 0, m = 0, L = 0;
+  bool dbl = true;
+  int device = 0;
+  afc::LenPlan lp;                 // the length-L convolution in one CTA
+  void* chirp_n = nullptr;         // A^-j W^(j^2/2), j < n
+  void* chirp_k = nullptr;         // W^(k^2/2), k < m
+  void* spec = nullptr;            // FFT of the chirp kernel, scaled by 1/L
+  ~afc_czt_plan_s() {
+    void* ptrs[] = {lp.tw, chirp_n, chirp_k, spec};
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+  }
+};
+
 namespace afc {
 
 struct DeviceGuard {
@@ -1718,6 +1737,121 @@ afc_status afc_stft_forward(afc_plan plan, const void* signal, int64_t signal_le
   d.L = choose_L(ap.lp, d.lanes, d.stage_in, d.stage_out, csz);
   cudaError_t e = launch_lanes(d, plan->dbl, false, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "stft forward");
+  return AFC_OK;
+}
+
+// num-complex powf (polar form): |z|^e exp(i arg(z) e), as the reference's
+// CztPlan builds its chirps (czt/dimension_1d.rs:85-98).
+static std::complex<double> cpowf(std::complex<double> z, double e) {
+  return std::polar(std::pow(std::abs(z), e), std::arg(z) * e);
+}
+
+afc_status afc_czt_plan_create(afc_czt_plan* out, int64_t n, int64_t m, double a_re, double a_im, double w_re,
+                               double w_im, afc_precision prec, int device) {
+  if (!out) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  *out = nullptr;
+  if (n < 1 || m < 1)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `length`: `n=%lld, m=%lld` violates `> 0`", (long long)n,
+                (long long)m);
+  if (!std::isfinite(a_re) || !std::isfinite(a_im) || !std::isfinite(w_re) || !std::isfinite(w_im) ||
+      (a_re == 0.0 && a_im == 0.0) || (w_re == 0.0 && w_im == 0.0))
+    return fail(AFC_ERR_VALIDATION, "validation failed for `a, w`: `non-finite or zero` violates `finite, non-zero`");
+  if (prec != AFC_PREC_F32 && prec != AFC_PREC_F64)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `precision`: `%d` violates `F32|F64`", (int)prec);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(AFC_ERR_BACKEND_UNAVAILABLE, "backend unavailable: cuda (no device)");
+  if (device < 0 || device >= ndev)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `device`: `%d` violates `< %d`", device, ndev);
+  const bool dbl = prec == AFC_PREC_F64;
+  const size_t csz = dbl ? 16 : 8;
+  int64_t L = 1;
+  while (L < n + m - 1) L <<= 1;
+  if (!plannable(L, csz))
+    return fail(AFC_ERR_UNSUPPORTED, "CZT convolution length %lld exceeds one CTA (n + m - 1 too large)", (long long)L);
+  DeviceGuard g(device);
+  std::unique_ptr<afc_czt_plan_s> p(new afc_czt_plan_s());
+  p->n = n;
+  p->m = m;
+  p->L = L;
+  p->dbl = dbl;
+  p->device = device;
+  const std::complex<double> A(a_re, a_im), W(w_re, w_im);
+  std::vector<std::complex<double>> cn(n), ck(m), ker(L, 0.0);
+  for (int64_t j = 0; j < n; ++j) cn[j] = cpowf(A, -(double)j) * cpowf(W, 0.5 * (double)j * (double)j);
+  for (int64_t k = 0; k < m; ++k) ck[k] = cpowf(W, 0.5 * (double)k * (double)k);
+  for (int64_t k = 0; k < m; ++k) ker[k] = cpowf(W, -0.5 * (double)k * (double)k) / (double)L;
+  for (int64_t j = 1; j < n; ++j) ker[L - j] = cpowf(W, -0.5 * (double)j * (double)j) / (double)L;
+  auto upload = [&](const std::vector<std::complex<double>>& v, void** dst) -> cudaError_t {
+    cudaError_t e = dev_alloc(dst, v.size() * csz);
+    if (e != cudaSuccess) return e;
+    if (dbl) return cudaMemcpy(*dst, v.data(), v.size() * csz, cudaMemcpyHostToDevice);
+    std::vector<float> f(2 * v.size());
+    for (size_t i = 0; i < v.size(); ++i) {
+      f[2 * i] = (float)v[i].real();
+      f[2 * i + 1] = (float)v[i].imag();
+    }
+    return cudaMemcpy(*dst, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice);
+  };
+  AFC_CUDA(upload(cn, &p->chirp_n), "CZT chirp");
+  AFC_CUDA(upload(ck, &p->chirp_k), "CZT chirp");
+  AFC_CUDA(upload(ker, &p->spec), "CZT kernel");
+  cudaStream_t st;
+  AFC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+  afc_status s = build_lenplan(L, dbl, p->lp, st);
+  if (s == AFC_OK) {
+    AxisPlan mp;
+    mp.n = L;
+    mp.algo = ALGO_SMEM;
+    mp.lp = p->lp;
+    s = fft_table(mp, dbl, p->spec, st);
+    mp.lp.tw = nullptr;  // owned by the CZT plan
+  }
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  if (s != AFC_OK) return s;
+  *out = p.release();
+  return AFC_OK;
+}
+
+afc_status afc_czt_execute(afc_czt_plan plan, const void* in, void* out, int64_t batch, void* stream) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (!in || !out) return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  if (batch < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `batch`: `%lld` violates `> 0`", (long long)batch);
+  const size_t csz = plan->dbl ? 16 : 8;
+  DeviceGuard g(plan->device);
+  LaunchDesc d;
+  fill_common(d, plan->lp);
+  d.lanes = batch;
+  d.im = LaneMap{1, 1, plan->n, 0, 0, 1, nullptr};
+  d.om = LaneMap{1, 1, plan->m, 0, 0, 1, nullptr};
+  d.in = in;
+  d.out = out;
+  d.in_op = IN_CHIRP;      // x_j A^-j W^(j^2/2) for j < n, zero up to L
+  d.out_op = OUT_CHIRP;    // W^(k^2/2) times the convolution, k < m
+  d.nlen = plan->n;
+  d.nlen_out = plan->m;
+  d.chirp = plan->chirp_n;
+  d.chirp_out = plan->chirp_k;
+  d.chirp_conj = 0;
+  d.spec = plan->spec;
+  d.scale = 1.0;
+  d.L = choose_L(plan->lp, batch, true, true, csz, 2 * csz + 3 * sizeof(long long), 2);
+  cudaError_t e = do_conv(d, plan->dbl, false, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "czt execute");
+  return AFC_OK;
+}
+
+afc_status afc_czt_conv_len(afc_czt_plan plan, int64_t* conv_len) {
+  if (!plan || !conv_len) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  *conv_len = plan->L;
+  return AFC_OK;
+}
+
+afc_status afc_czt_plan_destroy(afc_czt_plan plan) {
+  if (!plan) return AFC_OK;
+  DeviceGuard g(plan->device);
+  delete plan;
   return AFC_OK;
 }
 

@@ -39,6 +39,8 @@ struct LaunchDesc {
   const int* scatter = nullptr;
   int lane_minor = 0;
   int in_sel = 0, out_sel = 0;  // batch descriptors: pointer = base[sel] + offset
+  const void* chirp_out = nullptr;  // OUT_CHIRP: post-multiply table when it differs from `chirp` (CZT)
+  long long nlen_out = 0;          // OUT_CHIRP: outputs kept (j < nlen_out) when > 0, else nlen
   const void* window = nullptr;  // IN_FRAME: analysis window (real, frame length)
   long long frame_off = 0;       // IN_FRAME: frames start at lane base - frame_off
 };

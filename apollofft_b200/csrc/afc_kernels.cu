@@ -52,6 +52,8 @@ template <class T> struct KArgs {
   const int* scatter;      // Rader: scatter[q] = g^{-q} mod p
   int lane_minor;          // tile kernel: consecutive threads take consecutive lanes
   int in_sel, out_sel;     // batch descriptors: 0 absolute pointer, else base[sel] + offset
+  const C* chirp_out;      // OUT_CHIRP: post-multiply table when it differs from chirp (CZT)
+  long long nlen_out;      // OUT_CHIRP: outputs kept when > 0 (else nlen)
   const T* window;         // IN_FRAME: analysis window
   long long frame_off;     // IN_FRAME: frame q covers signal[q hop - frame_off + i]
 };
@@ -137,10 +139,10 @@ __device__ __forceinline__ void gstore(const KArgs<T>& a, long long base, long l
       return;
     }
     case OUT_CHIRP:
-    case OUT_CHIRP_RE: {  // Bluestein post-multiply, keep j < nlen
+    case OUT_CHIRP_RE: {  // Bluestein / CZT post-multiply, keep j < nlen (nlen_out when set)
       const long long j = (long long)i * a.jmul + col;
-      if (j < a.nlen) {
-        const C c = a.chirp[j];
+      if (j < (a.nlen_out > 0 ? a.nlen_out : a.nlen)) {
+        const C c = a.chirp_out ? a.chirp_out[j] : a.chirp[j];
         v = cscale(a.chirp_conj ? cmulc(v, c) : cmul(v, c), a.scale);
         if (a.out_op == OUT_CHIRP) static_cast<C*>(a.out)[off] = v;
         else static_cast<T*>(a.out)[off] = v.x;
@@ -734,6 +736,8 @@ template <class T> static KArgs<T> to_kargs(const LaunchDesc& d) {
   a.spec = static_cast<const C*>(d.spec);
   a.spec_ld = d.spec_ld;
   a.window = static_cast<const T*>(d.window);
+  a.chirp_out = static_cast<const C*>(d.chirp_out);
+  a.nlen_out = d.nlen_out;
   a.frame_off = d.frame_off;
   a.chirp = static_cast<const C*>(d.chirp);
   a.chirp_conj = d.chirp_conj;

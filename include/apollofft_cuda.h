@@ -204,6 +204,26 @@ AFC_API afc_status afc_stft_frame_count(int64_t frame_len, int64_t hop, int64_t 
 AFC_API afc_status afc_stft_forward(afc_plan plan, const void* signal, int64_t signal_len, const void* window,
                                     int64_t hop, void* out, int64_t out_elems, void* stream);
 
+/* Chirp z-transform on the device: X_k = sum_j x_j A^-j W^(j k), j < n, k < m,
+ * by Bluestein's identity in one launch (chirp premultiply fused into the
+ * convolution's load, FFT, product with the kernel spectrum, inverse FFT and
+ * chirp postmultiply fused into its store).  Replaces apollo-czt CztPlan::new /
+ * forward_into (apollo-czt/.../plan/czt/dimension_1d.rs:60-120 and
+ * kernel/bluestein.rs:83-130), which run the premultiply, the two
+ * FftPlan1D slice transforms and the postmultiply on host buffers; same chirp
+ * tables (num-complex powf, polar form) and the same convolution length
+ * L = next_pow2(n + m - 1), which must fit one CTA (AFC_ERR_UNSUPPORTED
+ * otherwise).  n, m > 0 and finite non-zero A, W (CztError::EmptyLength /
+ * InvalidParameters -> AFC_ERR_VALIDATION).  Execute: `batch` contiguous lanes
+ * of n complex inputs -> `batch` lanes of m complex outputs (F32: complex64,
+ * F64: complex128), device pointers, on `stream`. */
+typedef struct afc_czt_plan_s* afc_czt_plan;
+AFC_API afc_status afc_czt_plan_create(afc_czt_plan* out, int64_t n, int64_t m, double a_re, double a_im,
+                                       double w_re, double w_im, afc_precision precision, int device);
+AFC_API afc_status afc_czt_execute(afc_czt_plan plan, const void* in, void* out, int64_t batch, void* stream);
+AFC_API afc_status afc_czt_conv_len(afc_czt_plan plan, int64_t* conv_len);
+AFC_API afc_status afc_czt_plan_destroy(afc_czt_plan plan);
+
 /* Allocation-free execution of a rank-1 C2C plan whose length runs on the
  * two-pass (four-step) kernels: the intermediate between the passes lives in a
  * 16 MiB static device array instead of a cudaMalloc'd workspace, so the call

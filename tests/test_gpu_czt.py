@@ -1,0 +1,93 @@
+"""Device chirp z-transform (afc_czt_*) against a direct evaluation of
+X_k = sum_j x_j A^-j W^(j k) and against the reference's Bluestein path
+(czt/dimension_1d.rs:60-120, kernel/bluestein.rs:83-130) restated in numpy with
+the oracle's FFT."""
+import cmath
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def cpowf(z, e):  # num-complex powf (polar form)
+    return cmath.rect(abs(z) ** e, cmath.phase(z) * e)
+
+
+def czt_direct(x, m, a, w):
+    n = x.shape[-1]
+    j = np.arange(n)
+    out = np.zeros(x.shape[:-1] + (m,), dtype=np.complex128)
+    for k in range(m):
+        coef = np.array([cpowf(a, -jj) * cpowf(w, jj * k) for jj in j])
+        out[..., k] = x @ coef
+    return out
+
+
+def czt_reference(x, m, a, w, oracle):
+    n = x.shape[-1]
+    L = 1
+    while L < n + m - 1:
+        L <<= 1
+    cn = np.array([cpowf(a, -j) * cpowf(w, 0.5 * j * j) for j in range(n)])
+    ck = np.array([cpowf(w, 0.5 * k * k) for k in range(m)])
+    ker = np.zeros(L, dtype=np.complex128)
+    for k in range(m):
+        ker[k] = cpowf(w, -0.5 * k * k)
+    for j in range(1, n):
+        ker[L - j] = cpowf(w, -0.5 * j * j)
+    fk = oracle.fft1d(ker)
+    ws = np.zeros(x.shape[:-1] + (L,), dtype=np.complex128)
+    ws[..., :n] = x * cn
+    ws = oracle.fft1d(ws) * fk
+    ws = oracle.fft1d(ws, inverse=True)
+    return ws[..., :m] * ck
+
+
+CASES = [
+    (64, 64, 1.0, cmath.exp(-2j * cmath.pi / 64)),                      # the DFT
+    (100, 37, cmath.exp(0.3j), cmath.exp(-0.05j)),                      # zoom on an arc
+    (257, 300, cmath.exp(1j), cmath.exp(-2j * cmath.pi / 997)),
+    (1000, 1000, 1.0, cmath.exp(-2j * cmath.pi / 1000)),
+    (50, 80, 1.02 * cmath.exp(0.1j), 0.999 * cmath.exp(-0.03j)),        # a mild spiral
+]
+
+
+@pytest.mark.parametrize("n,m,a,w", CASES)
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_czt_vs_direct_and_reference(afc, oracle, cuda, n, m, a, w, prec):
+    from apollofft_b200.czt import CztPlan
+    rng = np.random.default_rng(n * 7 + m)
+    x = rng.uniform(-1, 1, (3, n)) + 1j * rng.uniform(-1, 1, (3, n))
+    plan = CztPlan(n, m, a, w, precision=prec)
+    dt = np.complex128 if prec == "f64" else np.complex64
+    y = plan.forward(torch.from_numpy(x.astype(dt)).cuda()).cpu().numpy()
+    assert y.shape == (3, m)
+    ref = czt_reference(x.astype(dt).astype(np.complex128), m, a, w, oracle)
+    direct = czt_direct(x.astype(dt).astype(np.complex128), m, a, w)
+    tol = 1e-12 if prec == "f64" else 1e-5
+    assert rel_l2(y, ref) < max(tol, 10 * rel_l2(ref, direct)), (rel_l2(y, ref), rel_l2(ref, direct))
+    assert rel_l2(y, direct) < (1e-9 if prec == "f64" else 1e-4)
+    if abs(a - 1.0) < 1e-15 and n == m and abs(w - cmath.exp(-2j * cmath.pi / n)) < 1e-15:
+        assert rel_l2(y, oracle.fft1d(x.astype(dt).astype(np.complex128))) < (1e-11 if prec == "f64" else 1e-5)
+
+
+def test_czt_two_calls_and_validation(afc, cuda):
+    from apollofft_b200.czt import CztError, CztPlan
+    plan = CztPlan(40, 24, 1.0, cmath.exp(-0.2j))
+    assert plan.convolution_len() == 64
+    x = torch.randn(5, 40, dtype=torch.complex128, device="cuda")
+    a = plan.forward(x).cpu().numpy()
+    b = plan.forward(x).cpu().numpy()
+    assert np.array_equal(a, b)
+    with pytest.raises(CztError):
+        CztPlan(0, 4)
+    with pytest.raises(CztError):
+        CztPlan(4, 4, 0.0, 1.0)
+    with pytest.raises(CztError):
+        CztPlan(4, 4, 1.0, float("nan"))
+    with pytest.raises(afc.AfcError):
+        CztPlan(100000, 100000)  # convolution beyond one CTA
