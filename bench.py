@@ -273,7 +273,7 @@ def main():
     ap.add_argument("--shape", default=None, help="override the 3D shape, e.g. 128,256,256 (profiling cases)")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
     ap.add_argument("--quick", action="store_true", help="headline only: no other shapes, e2e or CPU legs")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "stft"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "stft", "czt"],
                     help="c2 (default) is the headline; c1/c3/c4/c5 print their own lines")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -606,6 +606,46 @@ def run_secondary(args):
                                 "sample": f"first {sub} frames: window + oracle FFT per frame (frame gather not timed)"}
         got = out[:sub].cpu().numpy()
         line["error_vs_oracle_rel_l2"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    elif args.workload == "czt":
+        # apollo-czt's Bluestein path (premultiply, two FFTs, kernel product,
+        # postmultiply) as one launch: 4096 lanes, n = m = 1000, zoom on an arc (f64)
+        import cmath
+        from apollofft_b200.czt import CztPlan
+        lanes, n, m = 4096, 1000, 1000
+        a, w = cmath.exp(0.3j), cmath.exp(-2j * cmath.pi / 4000)
+        rng = np.random.default_rng(12)
+        xn = rng.uniform(-1, 1, (lanes, n)) + 1j * rng.uniform(-1, 1, (lanes, n))
+        x = torch.from_numpy(xn).to(dev)
+        plan = CztPlan(n, m, a, w, precision="f64")
+        out = torch.empty((lanes, m), dtype=torch.complex128, device=dev)
+        t = _events_time(lambda: plan.forward(x, out=out), args.steps, args.warmup, torch)
+        Lc = plan.convolution_len()
+        fl = lanes * 2 * 5 * Lc * math.log2(Lc)  # two length-L FFTs per lane
+        line.update({"metric": "GFLOP/s", "value": round(fl / t / 1e9, 1), "ms_per_step": round(t * 1e3, 4),
+                     "transforms_per_s": round(lanes / t, 1),
+                     "hbm_frac": round(lanes * (n + m) * 16 / t / 1e9 / hbm_peak, 4),
+                     "config": f"CZT f64: {lanes} lanes, n = m = {n}, convolution {Lc}, A = e^0.3i, W = e^(-2 pi i/4000)"})
+        from oracle import oracle as O
+        cn = np.array([cmath.rect(abs(a) ** -j, cmath.phase(a) * -j) * cmath.rect(1.0, cmath.phase(w) * 0.5 * j * j)
+                       for j in range(n)])
+        ck = np.array([cmath.rect(1.0, cmath.phase(w) * 0.5 * k * k) for k in range(m)])
+        ker = np.zeros(Lc, dtype=np.complex128)
+        for k in range(m):
+            ker[k] = cmath.rect(1.0, -cmath.phase(w) * 0.5 * k * k)
+        for j in range(1, n):
+            ker[Lc - j] = cmath.rect(1.0, -cmath.phase(w) * 0.5 * j * j)
+        sub = 512
+        t0 = time.perf_counter()
+        fk = O.fft1d(ker)
+        ws = np.zeros((sub, Lc), dtype=np.complex128)
+        ws[:, :n] = xn[:sub] * cn
+        ws = O.fft1d(O.fft1d(ws) * fk, inverse=True)
+        ref = ws[:, :m] * ck
+        tc = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(sub * 2 * 5 * Lc * math.log2(Lc) / tc / 1e9, 2), "unit": "GFLOP/s",
+                                "cores": O.max_threads(), "kind": "port",
+                                "sample": f"{sub} lanes: premultiply, oracle FFTs, product, postmultiply"}
+        line["error_vs_reference_path_rel_l2"] = float(np.linalg.norm(out[:sub].cpu().numpy() - ref) / np.linalg.norm(ref))
     print(json.dumps(line), flush=True)
     return 0
 
