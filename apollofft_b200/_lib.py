@@ -97,6 +97,10 @@ SIGNATURES = {
     "afc_czt_execute": (_i32, [_vp, _vp, _vp, _i64, _vp]),
     "afc_czt_conv_len": (_i32, [_vp, _pi64]),
     "afc_czt_plan_destroy": (_i32, [_vp]),
+    "afc_nufft1d_plan_create": (_i32, [ctypes.POINTER(_vp), _i64, _dbl, _i64, _i64, _i32]),
+    "afc_nufft1d_type1": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),
+    "afc_nufft1d_type2": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),
+    "afc_nufft_plan_destroy": (_i32, [_vp]),
 }
 
 _lib = None

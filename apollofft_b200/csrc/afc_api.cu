@@ -991,6 +991,20 @@ struct afc_plan_s {
   }
 };
 
+// 1D NUFFT plan (apollo-nufft NufftPlan1D, transform/dimension_1d.rs:101-154):
+// n uniform bins on a periodic domain of length n dx, oversampled grid
+// m = sigma n, Kaiser-Bessel kernel of half width w, beta = pi (1 - 1/(2 sigma)) 2w.
+struct afc_nufft_plan_s {
+  int64_t n = 0, m = 0;
+  int w = 0;
+  double dx = 0, beta = 0, i0b = 1;
+  int device = 0;
+  afc_plan fft = nullptr;          // C2C f64 plan of length m
+  double* deconv = nullptr;        // 1 / kb_ft(k_signed / m), k < n
+  void* grid = nullptr;            // plan-owned oversampled grid (m complex128)
+  ~afc_nufft_plan_s();
+};
+
 // Chirp z-transform plan (apollo-czt CztPlan, plan/czt/dimension_1d.rs:60-120):
 // input length n, output length m, X_k = sum_j x_j A^-j W^(j k) by Bluestein's
 // identity over a convolution of length L = next_pow2(n + m - 1).
@@ -1594,6 +1608,12 @@ static afc_status no_alloc_scratch(int dev, void** ptr) {
 
 using namespace afc;
 
+afc_nufft_plan_s::~afc_nufft_plan_s() {
+  if (fft) afc_plan_destroy(fft);
+  if (deconv) cudaFree(deconv);
+  if (grid) cudaFree(grid);
+}
+
 extern "C" {
 
 afc_status afc_plan_create(afc_plan* out, int rank, const int64_t* dims, afc_precision precision, afc_kind kind,
@@ -1845,6 +1865,114 @@ afc_status afc_czt_execute(afc_czt_plan plan, const void* in, void* out, int64_t
 afc_status afc_czt_conv_len(afc_czt_plan plan, int64_t* conv_len) {
   if (!plan || !conv_len) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
   *conv_len = plan->L;
+  return AFC_OK;
+}
+
+// I0 by the reference's power series (kaiser_bessel.rs:55-69) and the KB
+// kernel's Fourier transform (kaiser_bessel.rs:120-133), host side.
+static double nu_i0_host(double z) {
+  const double scaled = 0.25 * z * z;
+  double sum = 1.0, term = 1.0;
+  for (int k = 1; k <= 256; ++k) {
+    term *= scaled / ((double)k * (double)k);
+    sum += term;
+    if (term <= 2.220446049250313e-16 * sum) break;
+  }
+  return sum;
+}
+static double nu_kb_ft(double xi, int w, double beta, double i0b) {
+  const double twx = 2.0 * M_PI * (double)w * xi;
+  const double z2 = beta * beta - twx * twx;
+  const double pre = 2.0 * (double)w / i0b;
+  if (std::fabs(z2) < 1e-30) return pre;
+  if (z2 > 0.0) {
+    const double sq = std::sqrt(z2);
+    return pre * std::sinh(sq) / sq;
+  }
+  const double sq = std::sqrt(-z2);
+  return pre * std::sin(sq) / sq;
+}
+
+afc_status afc_nufft1d_plan_create(afc_nufft_plan* out, int64_t n, double dx, int64_t sigma, int64_t kernel_width,
+                                   int device) {
+  if (!out) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  *out = nullptr;
+  if (n < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `n`: `%lld` violates `must be > 0`", (long long)n);
+  if (!std::isfinite(dx) || dx <= 0.0)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `dx`: `%g` violates `must be finite and > 0`", dx);
+  if (sigma < 2) return fail(AFC_ERR_VALIDATION, "validation failed for `sigma`: `%lld` violates `>= 2`", (long long)sigma);
+  if (kernel_width < 2 || kernel_width > 32)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `kernel_width`: `%lld` violates `2..32`", (long long)kernel_width);
+  std::unique_ptr<afc_nufft_plan_s> p(new afc_nufft_plan_s());
+  p->n = n;
+  p->m = sigma * n;
+  p->w = (int)kernel_width;
+  p->dx = dx;
+  p->beta = M_PI * (1.0 - 1.0 / (2.0 * (double)sigma)) * (double)(2 * kernel_width);
+  p->i0b = nu_i0_host(p->beta);
+  p->device = device;
+  afc_status s = afc_plan_create(&p->fft, 1, &p->m, AFC_PREC_F64, AFC_KIND_C2C, 1, device);
+  if (s != AFC_OK) return s;
+  DeviceGuard g(device);
+  std::vector<double> dec(n);
+  for (int64_t k = 0; k < n; ++k) {
+    const int64_t ks = k <= n / 2 ? k : k - n;
+    dec[k] = 1.0 / nu_kb_ft((double)ks / (double)p->m, p->w, p->beta, p->i0b);
+  }
+  AFC_CUDA(dev_alloc((void**)&p->deconv, (size_t)n * sizeof(double)), "NUFFT deconvolution");
+  AFC_CUDA(cudaMemcpy(p->deconv, dec.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice), "NUFFT deconvolution");
+  AFC_CUDA(dev_alloc(&p->grid, (size_t)p->m * 16), "NUFFT grid");
+  *out = p.release();
+  return AFC_OK;
+}
+
+static NuLaunch nu_launch(const afc_nufft_plan_s& p) {
+  NuLaunch L;
+  L.m = p.m;
+  L.w = p.w;
+  L.beta = p.beta;
+  L.i0b = p.i0b;
+  L.len = (double)p.n * p.dx;
+  return L;
+}
+
+afc_status afc_nufft1d_type1(afc_nufft_plan plan, const double* positions, const void* values, int64_t npts, void* out,
+                             void* stream) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (npts < 0) return fail(AFC_ERR_VALIDATION, "validation failed for `npts`: `%lld` violates `>= 0`", (long long)npts);
+  if (!out || (npts > 0 && (!positions || !values)))
+    return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  DeviceGuard g(plan->device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  AFC_CUDA(cudaMemsetAsync(plan->grid, 0, (size_t)plan->m * 16, st), "NUFFT grid");
+  AFC_CUDA(nufft_spread_dev(nu_launch(*plan), positions, values, npts, plan->grid, st), "NUFFT spread");
+  afc_status s = afc_execute(plan->fft, plan->grid, plan->grid, AFC_FORWARD, stream);
+  if (s != AFC_OK) return s;
+  AFC_CUDA(nufft_deconv_out_dev(plan->grid, plan->deconv, plan->n, plan->m, out, st), "NUFFT deconvolution");
+  return AFC_OK;
+}
+
+afc_status afc_nufft1d_type2(afc_nufft_plan plan, const void* coeffs, const double* positions, int64_t npts, void* out,
+                             void* stream) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (npts < 0) return fail(AFC_ERR_VALIDATION, "validation failed for `npts`: `%lld` violates `>= 0`", (long long)npts);
+  if (!coeffs || (npts > 0 && (!positions || !out)))
+    return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  DeviceGuard g(plan->device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  AFC_CUDA(cudaMemsetAsync(plan->grid, 0, (size_t)plan->m * 16, st), "NUFFT grid");
+  AFC_CUDA(nufft_place_coeffs_dev(coeffs, plan->deconv, plan->n, plan->m, plan->grid, st), "NUFFT coefficients");
+  // the reference's normalized inverse times m = the unnormalized inverse
+  afc_status s = afc_execute_scaled(plan->fft, plan->grid, plan->grid, AFC_INVERSE, 1.0, stream);
+  if (s != AFC_OK) return s;
+  AFC_CUDA(nufft_interp_dev(nu_launch(*plan), plan->grid, positions, npts, out, st), "NUFFT interpolation");
+  return AFC_OK;
+}
+
+afc_status afc_nufft_plan_destroy(afc_nufft_plan plan) {
+  if (!plan) return AFC_OK;
+  DeviceGuard g(plan->device);
+  delete plan;
   return AFC_OK;
 }
 

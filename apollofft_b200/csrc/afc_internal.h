@@ -102,6 +102,21 @@ struct TcLaunch {
   unsigned* err = nullptr;
 };
 cudaError_t launch_tc_fft(const TcLaunch& d, bool fp16, cudaStream_t st);
+
+// 1D NUFFT spreading / interpolation (afc_nufft.cu), complex128 grids
+struct NuLaunch {
+  long long m = 0;   // oversampled grid length
+  int w = 0;         // kernel half width
+  double beta = 0, i0b = 1, len = 1;
+};
+cudaError_t nufft_spread_dev(const NuLaunch& L, const double* pos, const void* val, long long npts, void* grid,
+                             cudaStream_t st);
+cudaError_t nufft_interp_dev(const NuLaunch& L, const void* grid, const double* pos, long long npts, void* out,
+                             cudaStream_t st);
+cudaError_t nufft_deconv_out_dev(const void* grid, const double* deconv, long long n, long long m, void* out,
+                                 cudaStream_t st);
+cudaError_t nufft_place_coeffs_dev(const void* coeffs, const double* deconv, long long n, long long m, void* grid,
+                                   cudaStream_t st);
 cudaError_t launch_wait_probe(unsigned* err, int polls, cudaStream_t st);
 cudaError_t launch_tc_selftest(const float* A, const float* B, float* D, unsigned* err, bool fp16, cudaStream_t st);
 size_t tc_fft_smem(int n);

@@ -224,6 +224,28 @@ AFC_API afc_status afc_czt_execute(afc_czt_plan plan, const void* in, void* out,
 AFC_API afc_status afc_czt_conv_len(afc_czt_plan plan, int64_t* conv_len);
 AFC_API afc_status afc_czt_plan_destroy(afc_czt_plan plan);
 
+/* 1D non-uniform FFT on the device, apollo-nufft NufftPlan1D
+ * (apollo-nufft/.../transform/dimension_1d.rs:101-272): n uniform bins on the
+ * periodic domain [0, n dx), oversampled grid m = sigma n, Kaiser-Bessel kernel
+ * of half width kernel_width (reference defaults: sigma 2, width 6).  Type 1:
+ * out[k] ~ sum_j values_j exp(-2 pi i k_signed x_j / (n dx)), k < n; type 2:
+ * out[j] ~ sum_k coeffs_k exp(+2 pi i k_signed x_j / (n dx)).  Positions are
+ * float64, values / coeffs / outputs complex128, all device pointers.  The
+ * spreading, the FFT of this library and the deconvolution follow the
+ * reference step by step (type 1 spreads with atomic adds instead of the
+ * reference's bucket sort, so sums differ in rounding only).  Calls on one plan
+ * share its grid: calls on the same stream are ordered, overlapping calls on
+ * different streams race.  Invalid n, dx, sigma < 2 or width outside 2..32 ->
+ * AFC_ERR_VALIDATION. */
+typedef struct afc_nufft_plan_s* afc_nufft_plan;
+AFC_API afc_status afc_nufft1d_plan_create(afc_nufft_plan* out, int64_t n, double dx, int64_t sigma,
+                                           int64_t kernel_width, int device);
+AFC_API afc_status afc_nufft1d_type1(afc_nufft_plan plan, const double* positions, const void* values, int64_t npts,
+                                     void* out, void* stream);
+AFC_API afc_status afc_nufft1d_type2(afc_nufft_plan plan, const void* coeffs, const double* positions, int64_t npts,
+                                     void* out, void* stream);
+AFC_API afc_status afc_nufft_plan_destroy(afc_nufft_plan plan);
+
 /* Allocation-free execution of a rank-1 C2C plan whose length runs on the
  * two-pass (four-step) kernels: the intermediate between the passes lives in a
  * 16 MiB static device array instead of a cudaMalloc'd workspace, so the call
