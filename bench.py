@@ -273,7 +273,7 @@ def main():
     ap.add_argument("--shape", default=None, help="override the 3D shape, e.g. 128,256,256 (profiling cases)")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
     ap.add_argument("--quick", action="store_true", help="headline only: no other shapes, e2e or CPU legs")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "stft", "czt"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "stft", "czt", "nufft"],
                     help="c2 (default) is the headline; c1/c3/c4/c5 print their own lines")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -646,6 +646,28 @@ def run_secondary(args):
                                 "cores": O.max_threads(), "kind": "port",
                                 "sample": f"{sub} lanes: premultiply, oracle FFTs, product, postmultiply"}
         line["error_vs_reference_path_rel_l2"] = float(np.linalg.norm(out[:sub].cpu().numpy() - ref) / np.linalg.norm(ref))
+    elif args.workload == "nufft":
+        # apollo-nufft NufftPlan1D at the reference defaults (sigma 2, width 6):
+        # n = 65536 bins, 2^20 uniform random points; type 1 then type 2 per step (f64)
+        from apollofft_b200.nufft import NufftPlan1D
+        n, npts, dx = 65536, 1 << 20, 1.0 / 65536
+        rng = np.random.default_rng(13)
+        pos_np = rng.uniform(0.0, 1.0, npts)
+        val_np = rng.standard_normal(npts) + 1j * rng.standard_normal(npts)
+        pos = torch.from_numpy(pos_np).to(dev)
+        val = torch.from_numpy(val_np).to(dev)
+        plan = NufftPlan1D(n, dx)
+        f = torch.empty(n, dtype=torch.complex128, device=dev)
+        back = torch.empty(npts, dtype=torch.complex128, device=dev)
+        t = _events_time(lambda: (plan.type1(pos, val, out=f), plan.type2(f, pos, out=back)), args.steps,
+                         args.warmup, torch)
+        line.update({"metric": "points/s", "value": round(2 * npts / t, 1), "ms_per_step": round(t * 1e3, 4),
+                     "config": f"NUFFT 1D f64 type 1 + type 2: n = {n}, {npts} points, sigma 2, kernel width 6"})
+        # error of type 1 against the exact sum on 64 sampled bins
+        ks = np.array([k if k <= n // 2 else k - n for k in range(0, n, n // 64)])
+        exact = np.exp(-2j * np.pi * np.outer(ks, pos_np)) @ val_np
+        got = f.cpu().numpy()[np.arange(0, n, n // 64)]
+        line["type1_rel_l2_vs_exact_sampled_bins"] = float(np.linalg.norm(got - exact) / np.linalg.norm(exact))
     print(json.dumps(line), flush=True)
     return 0
 
