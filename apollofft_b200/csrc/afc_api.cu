@@ -628,11 +628,11 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
       d.herm_n = io.herm_n;
       d.pair_w = io.pair_w;
       const bool rin = io.in_op == IN_R && io.out_op == OUT_C, rout = io.in_op == IN_C && io.out_op == OUT_RE;
-      if (!tl_rec && ((io.in_op == IN_C && io.out_op == OUT_C) || rin || rout) && env_int("AFC_TMA", 1)) {
+      static const int tma_on = env_int("AFC_TMA", 1), tma_lanes = env_int("AFC_TMA_LANES", 0);
+      if (!tl_rec && ((io.in_op == IN_C && io.out_op == OUT_C) || rin || rout) && tma_on) {
         TmaPlan tp;
         unsigned* err = device_err_word();
-        if (err && tma_plan(ap.lp.sl, ap.lp.ld, io.lanes, io.im, io.om, io.in, io.out, dbl, env_int("AFC_TMA_LANES", 0), tp,
-                            rin, rout))
+        if (err && tma_plan(ap.lp.sl, ap.lp.ld, io.lanes, io.im, io.om, io.in, io.out, dbl, tma_lanes, tp, rin, rout))
           return launch_tma(d, tp, err, dbl, inv, st);
       }
       if (!tl_rec && io.in_op == IN_C && plain_out(io.out_op)) {

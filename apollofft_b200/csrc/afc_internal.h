@@ -121,6 +121,12 @@ cudaError_t launch_wait_probe(unsigned* err, int polls, cudaStream_t st);
 cudaError_t launch_tc_selftest(const float* A, const float* B, float* D, unsigned* err, bool fp16, cudaStream_t st);
 size_t tc_fft_smem(int n);
 
+// Launch facts cached per device and kernel (afc_kernels.cu): the dynamic
+// shared memory already granted (cudaFuncSetAttribute only when a launch needs
+// more) and CTAs per SM for a (threads, shared memory) shape, so repeated
+// executions of a plan skip those driver calls.
+cudaError_t kernel_smem_grant(const void* kern, size_t smem);
+int kernel_ctas_per_sm(const void* kern, int threads, size_t smem);
 cudaError_t launch_lanes(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st);
 size_t kargs_size(bool dbl);
 void kargs_pack(const LaunchDesc& d, bool dbl, void* dst);

@@ -13,6 +13,9 @@
 // table kernels    : FP64 generation of stage twiddles, two-level four-step
 //                    twiddles, Bluestein chirps and Rader kernels, narrowed once.
 #include <cuda_runtime.h>
+#include <tuple>
+#include <mutex>
+#include <map>
 #include <cstring>
 #include "afc_engine.cuh"
 #include "afc_internal.h"
@@ -749,9 +752,46 @@ template <class T> static KArgs<T> to_kargs(const LaunchDesc& d) {
   return a;
 }
 
-template <class K> static cudaError_t prep_smem(K kern, size_t smem) {
-  if (smem > 48 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+static std::mutex g_kfact_mu;
+static std::map<std::pair<int, const void*>, size_t> g_kgrant;
+static std::map<std::tuple<int, const void*, int, size_t>, int> g_kper;
+
+cudaError_t kernel_smem_grant(const void* kern, size_t smem) {
+  if (smem <= 48 * 1024) return cudaSuccess;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_pair(dev, kern);
+  {
+    std::lock_guard<std::mutex> lk(g_kfact_mu);
+    auto it = g_kgrant.find(key);
+    if (it != g_kgrant.end() && it->second >= smem) return cudaSuccess;
+  }
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_kfact_mu);
+  size_t& g = g_kgrant[key];
+  if (g < smem) g = smem;
   return cudaSuccess;
+}
+
+int kernel_ctas_per_sm(const void* kern, int threads, size_t smem) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, kern, threads, smem);
+  {
+    std::lock_guard<std::mutex> lk(g_kfact_mu);
+    auto it = g_kper.find(key);
+    if (it != g_kper.end()) return it->second;
+  }
+  int per = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem) != cudaSuccess || per < 1) per = 1;
+  std::lock_guard<std::mutex> lk(g_kfact_mu);
+  g_kper[key] = per;
+  return per;
+}
+
+template <class K> static cudaError_t prep_smem(K kern, size_t smem) {
+  return kernel_smem_grant(reinterpret_cast<const void*>(kern), smem);
 }
 
 template <class T, bool INV> static cudaError_t launch_lanes_t(const LaunchDesc& d, cudaStream_t st) {
@@ -784,9 +824,7 @@ template <class T, bool INV> static cudaError_t launch_tile_t(const LaunchDesc& 
     cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
     if (g_sm_count <= 0) g_sm_count = 148;
   }
-  int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, d.L * d.P, smem);
-  if (per_sm < 1) per_sm = 1;
+  const int per_sm = kernel_ctas_per_sm(reinterpret_cast<const void*>(k), d.L * d.P, smem);
   const long long ntiles = (d.lanes + d.L - 1) / d.L;
   long long grid = (long long)g_sm_count * per_sm;
   if (grid > ntiles) grid = ntiles;

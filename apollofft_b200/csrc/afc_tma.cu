@@ -574,7 +574,7 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
            : tp.variant == 3 ? tma_kernel<T, INV, 3, false>
                              : tma_kernel<T, INV, 0, false>;
   const size_t smem = tma_smem_bytes(tp, sizeof(C));
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = kernel_smem_grant(reinterpret_cast<const void*>(k), smem);
   if (e != cudaSuccess) return e;
   TmaArgs<T> a;
   memset(&a, 0, sizeof(a));
@@ -608,9 +608,7 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
     cudaDeviceGetAttribute(&g_tma_sm, cudaDevAttrMultiProcessorCount, dev);
     if (g_tma_sm <= 0) g_tma_sm = 148;
   }
-  int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, tp.L * tp.P, smem);
-  if (per_sm < 1) per_sm = 1;
+  const int per_sm = kernel_ctas_per_sm(reinterpret_cast<const void*>(k), tp.L * tp.P, smem);
   long long grid = (long long)g_tma_sm * per_sm;
   if (grid > tp.ntiles) grid = tp.ntiles;
   k<<<(unsigned)grid, tp.L * tp.P, smem, st>>>(a);

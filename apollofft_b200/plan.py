@@ -35,6 +35,7 @@ class CudaPlan:
         self.batch = int(batch)
         self.device = int(device)
         self._h = ctypes.c_void_p()
+        self._exec = L.lib().afc_execute
         arr = (ctypes.c_int64 * max(self.rank, 1))(*dims)
         fn = L.lib().afc_plan_get_cached if cached else L.lib().afc_plan_create
         L.check(fn(ctypes.byref(self._h), self.rank, arr, _PREC[precision], _KIND[kind], self.batch, self.device),
@@ -46,9 +47,13 @@ class CudaPlan:
         return int(np.prod(self.dims))
 
     def io_elems(self, inverse: bool = False):
-        a, b = ctypes.c_int64(), ctypes.c_int64()
-        L.check(L.lib().afc_plan_io_elems(self._h, int(inverse), ctypes.byref(a), ctypes.byref(b)), "io_elems")
-        return a.value, b.value
+        inverse = bool(inverse)
+        cache = self.__dict__.setdefault("_io_cache", {})
+        if inverse not in cache:  # fixed per plan: one library call per direction
+            a, b = ctypes.c_int64(), ctypes.c_int64()
+            L.check(L.lib().afc_plan_io_elems(self._h, int(inverse), ctypes.byref(a), ctypes.byref(b)), "io_elems")
+            cache[inverse] = (a.value, b.value)
+        return cache[inverse]
 
     def workspace_size(self) -> int:
         s = ctypes.c_size_t()
@@ -84,13 +89,21 @@ class CudaPlan:
             dims[-1] = dims[-1] // 2 + 1
         return lead + tuple(dims)
 
+    def _io(self, inverse: bool):
+        """(input dtype, output dtype, input elements, output elements), cached per direction."""
+        inverse = bool(inverse)
+        cache = self.__dict__.setdefault("_io_full", {})
+        if inverse not in cache:
+            ie, oe = self.io_elems(inverse)
+            cache[inverse] = (_TORCH_DTYPES[np.dtype(self.in_dtype(inverse))],
+                              _TORCH_DTYPES[np.dtype(self.out_dtype(inverse))], ie, oe)
+        return cache[inverse]
+
     # ── device execution (torch tensors) ──
     def execute(self, x, out=None, inverse: bool = False, scale: Optional[float] = None, stream=None):
         """Runs on torch CUDA tensors; returns `out` (allocated if None)."""
         import torch
-        t_in = _TORCH_DTYPES[np.dtype(self.in_dtype(inverse))]
-        t_out = _TORCH_DTYPES[np.dtype(self.out_dtype(inverse))]
-        ie, oe = self.io_elems(inverse)
+        t_in, t_out, ie, oe = self._io(inverse)
         if x.dtype != t_in:
             raise ValueError(f"expected {t_in} input, got {x.dtype}")
         if not x.is_contiguous():
@@ -102,9 +115,9 @@ class CudaPlan:
                               dtype=t_out, device=x.device)
         if out.numel() != oe or out.dtype != t_out or not out.is_contiguous():
             raise ValueError("output buffer does not match the plan")
-        st = stream if stream is not None else torch.cuda.current_stream(x.device).cuda_stream
+        st = stream if stream is not None else _current_stream(x.device)
         if scale is None:
-            status = L.lib().afc_execute(self._h, x.data_ptr(), out.data_ptr(), int(inverse), st)
+            status = self._exec(self._h, x.data_ptr(), out.data_ptr(), int(inverse), st)
         else:
             status = L.lib().afc_execute_scaled(self._h, x.data_ptr(), out.data_ptr(), int(inverse), float(scale), st)
         L.check(status, "execute")
@@ -150,6 +163,16 @@ class CudaPlan:
             self.close()
         except Exception:
             pass
+
+
+def _current_stream(device):
+    """Raw handle of the current CUDA stream of `device` (torch's fast accessor
+    when present)."""
+    import torch
+    raw = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+    if raw is not None:
+        return raw(device.index if device.index is not None else torch.cuda.current_device())
+    return torch.cuda.current_stream(device).cuda_stream
 
 
 def _torch_dtypes():
