@@ -93,6 +93,8 @@ SIGNATURES = {
     "afc_execute_1d_no_alloc": (_i32, [_vp, _vp, _vp, _i32, _vp]),
     "afc_stft_frame_count": (_i32, [_i64, _i64, _i64, _pi64]),
     "afc_stft_forward": (_i32, [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp]),
+    "afc_stft_inverse_workspace": (_i32, [_vp, _i64, _i64, ctypes.POINTER(_sz)]),
+    "afc_stft_inverse": (_i32, [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _sz, _vp]),
     "afc_czt_plan_create": (_i32, [ctypes.POINTER(_vp), _i64, _i64, _dbl, _dbl, _dbl, _dbl, _i32, _i32]),
     "afc_czt_execute": (_i32, [_vp, _vp, _vp, _i64, _vp]),
     "afc_czt_conv_len": (_i32, [_vp, _pi64]),

@@ -1760,6 +1760,60 @@ afc_status afc_stft_forward(afc_plan plan, const void* signal, int64_t signal_le
   return AFC_OK;
 }
 
+afc_status afc_stft_inverse_workspace(afc_plan plan, int64_t hop, int64_t signal_len, size_t* bytes) {
+  if (!plan || !bytes) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (hop < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `hop_len`: `%lld` violates `> 0`", (long long)hop);
+  const int64_t n = plan->dims[0];
+  *bytes = (size_t)stft_frames(n, hop, signal_len) * (size_t)n * (plan->dbl ? 8 : 4);
+  return AFC_OK;
+}
+
+afc_status afc_stft_inverse(afc_plan plan, const void* spectrum, int64_t spectrum_elems, const void* window, int64_t hop,
+                            void* out, int64_t signal_len, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (!spectrum || !window || !out || !workspace)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  if (plan->rank != 1 || plan->kind != AFC_KIND_C2C || plan->tc)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `rank %d` violates `rank-1 C2C f32/f64 plan`", plan->rank);
+  const int64_t n = plan->dims[0];
+  if (hop < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `hop_len`: `%lld` violates `> 0`", (long long)hop);
+  if (hop > n)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `hop_len`: `%lld` violates `<= frame_len %lld`", (long long)hop,
+                (long long)n);
+  if (signal_len < n)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `signal_len`: `%lld` violates `>= frame_len %lld`",
+                (long long)signal_len, (long long)n);
+  const int64_t frames = stft_frames(n, hop, signal_len);
+  if (spectrum_elems != frames * n)
+    return fail(AFC_ERR_SHAPE_MISMATCH, "shape mismatch: expected %lld spectrum elements (%lld frames x %lld), got %lld",
+                (long long)(frames * n), (long long)frames, (long long)n, (long long)spectrum_elems);
+  const size_t rsz = plan->dbl ? 8 : 4;
+  if (workspace_bytes < (size_t)frames * (size_t)n * rsz)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `workspace_bytes`: `%zu` violates `>= %zu`", workspace_bytes,
+                (size_t)frames * (size_t)n * rsz);
+  const AxisPlan& ap = *plan->axes[0];
+  if (ap.algo != ALGO_SMEM)
+    return fail(AFC_ERR_UNSUPPORTED, "inverse STFT frames need a single-CTA frame length (got %lld)", (long long)n);
+  DeviceGuard g(plan->device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // 1. every frame: normalized inverse FFT, real part, into the workspace
+  AxisIO io;
+  io.in = spectrum;
+  io.out = workspace;
+  io.lanes = frames;
+  io.im = LaneMap{1, 1, n, 0, 0, 1, nullptr};
+  io.om = io.im;
+  io.in_op = IN_C;
+  io.out_op = OUT_RE;
+  io.scale = 1.0 / (double)n;
+  cudaError_t e = exec_axis(ap, plan->dbl, true, io, nullptr, st);
+  if (e != cudaSuccess) return cuda_fail(e, "stft inverse frames");
+  // 2. windowed overlap-add, normalized by the summed squared window
+  e = stft_ola_dev(workspace, window, frames, n, hop, signal_len, out, plan->dbl, st);
+  if (e != cudaSuccess) return cuda_fail(e, "stft overlap-add");
+  return AFC_OK;
+}
+
 // num-complex powf (polar form): |z|^e exp(i arg(z) e), as the reference's
 // CztPlan builds its chirps (czt/dimension_1d.rs:85-98).
 static std::complex<double> cpowf(std::complex<double> z, double e) {

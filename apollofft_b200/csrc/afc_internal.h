@@ -138,6 +138,8 @@ int batch_blocks_per_sm(size_t smem, bool dbl, bool inv);
 cudaError_t launch_tile(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st);
 cudaError_t launch_conv(const LaunchDesc& d, bool dbl, cudaStream_t st);
 
+cudaError_t stft_ola_dev(const void* frames, const void* window, long long nframes, long long flen, long long hop,
+                         long long nsig, void* out, bool dbl, cudaStream_t st);
 cudaError_t gen_row_spectrum_dev(void* dst, const void* src, long long N1, long long N2, bool dbl, cudaStream_t st);
 cudaError_t gen_stage_twiddles_dev(void* tw, const StageList& sl, bool dbl, cudaStream_t st);
 cudaError_t gen_roots_dev(void* out, long long cnt, long long mult, long long N, bool dbl, cudaStream_t st);

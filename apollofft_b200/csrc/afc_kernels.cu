@@ -704,6 +704,31 @@ __global__ void gen_row_spectrum(typename CT<T>::type* dst, const typename CT<T>
   }
 }
 
+// Inverse STFT weighted overlap-add (apollo-stft inverse_complex64_slice_into,
+// stft/dimension_1d.rs:287-345): sample i sums frame[m][i - start_m] * window and
+// window^2 over the frames covering it (start_m = m hop - frame_len / 2) and
+// divides; zero where no frame covers it.  One thread per sample, gathering.
+template <class T>
+__global__ void stft_ola(const T* __restrict__ frames, const T* __restrict__ window, long long nframes, long long flen,
+                         long long hop, long long nsig, T* __restrict__ out) {
+  const long long half = flen / 2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nsig; i += (long long)gridDim.x * blockDim.x) {
+    // frames with start_m <= i < start_m + flen: m hop in (i + half - flen, i + half]
+    long long m_hi = (i + half) / hop;
+    long long lo = i + half - flen + 1;
+    long long m_lo = lo <= 0 ? 0 : (lo + hop - 1) / hop;
+    if (m_hi > nframes - 1) m_hi = nframes - 1;
+    T acc = (T)0, wsum = (T)0;
+    for (long long m = m_lo; m <= m_hi; ++m) {
+      const long long nidx = i - (m * hop - half);
+      const T w = window[nidx];
+      acc += frames[m * flen + nidx] * w;
+      wsum += w * w;
+    }
+    out[i] = wsum > (T)0 ? acc / wsum : (T)0;
+  }
+}
+
 // ─────────────────────────────── launchers ────────────────────────────────
 
 template <class T> static KArgs<T> to_kargs(const LaunchDesc& d) {
@@ -921,6 +946,19 @@ cudaError_t gen_row_spectrum_dev(void* dst, const void* src, long long N1, long 
   else
     gen_row_spectrum<float><<<table_grid(N1 * N2), 256, 0, st>>>(static_cast<float2*>(dst),
                                                                  static_cast<const float2*>(src), N1, N2);
+  count_launch(1);
+  return cudaGetLastError();
+}
+cudaError_t stft_ola_dev(const void* frames, const void* window, long long nframes, long long flen, long long hop,
+                         long long nsig, void* out, bool dbl, cudaStream_t st) {
+  if (dbl)
+    stft_ola<double><<<table_grid(nsig), 256, 0, st>>>(static_cast<const double*>(frames),
+                                                       static_cast<const double*>(window), nframes, flen, hop, nsig,
+                                                       static_cast<double*>(out));
+  else
+    stft_ola<float><<<table_grid(nsig), 256, 0, st>>>(static_cast<const float*>(frames),
+                                                      static_cast<const float*>(window), nframes, flen, hop, nsig,
+                                                      static_cast<float*>(out));
   count_launch(1);
   return cudaGetLastError();
 }

@@ -93,3 +93,36 @@ class StftPlan:
         L.check(L.lib().afc_stft_forward(self.plan._h, signal.data_ptr(), signal.numel(), win.data_ptr(),
                                          self.hop_len, out.data_ptr(), out.numel(), st), "stft forward")
         return out
+
+    def inverse(self, spectrum, signal_len: int, window=None, out=None, stream=None):
+        """Weighted overlap-add inverse (the reference's StftPlan::inverse):
+        spectrum (frames, frame_len) complex -> signal_len reals."""
+        import torch
+        rdt = self._real_dtype()
+        cdt = torch.complex128 if rdt == torch.float64 else torch.complex64
+        if spectrum.dtype != cdt or not spectrum.is_contiguous():
+            raise ValueError(f"expected a contiguous {cdt} spectrum")
+        if signal_len < self.frame_len:
+            raise StftError("input signal shorter than frame length")
+        frames = self.frame_count(signal_len)
+        if spectrum.numel() != frames * self.frame_len:
+            raise StftError("spectrum length does not match the frame count")
+        if window is None:
+            if self._win_dev is None:
+                self._win_dev = torch.from_numpy(self.window).to(device=spectrum.device, dtype=rdt)
+            win = self._win_dev
+        else:
+            win = torch.as_tensor(window, dtype=rdt, device=spectrum.device).contiguous()
+            if win.numel() != self.frame_len:
+                raise StftError("window length does not match frame length")
+        nbytes = ctypes.c_size_t()
+        L.check(L.lib().afc_stft_inverse_workspace(self.plan._h, self.hop_len, int(signal_len), ctypes.byref(nbytes)),
+                "stft inverse workspace")
+        ws = torch.empty(max(nbytes.value // (8 if rdt == torch.float64 else 4), 1), dtype=rdt, device=spectrum.device)
+        if out is None:
+            out = torch.empty(int(signal_len), dtype=rdt, device=spectrum.device)
+        st = stream if stream is not None else torch.cuda.current_stream(spectrum.device).cuda_stream
+        L.check(L.lib().afc_stft_inverse(self.plan._h, spectrum.data_ptr(), spectrum.numel(), win.data_ptr(),
+                                         self.hop_len, out.data_ptr(), int(signal_len), ws.data_ptr(),
+                                         nbytes.value, st), "stft inverse")
+        return out

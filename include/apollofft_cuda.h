@@ -203,6 +203,18 @@ AFC_API uint64_t afc_kernel_launch_count(void);
 AFC_API afc_status afc_stft_frame_count(int64_t frame_len, int64_t hop, int64_t signal_len, int64_t* frames);
 AFC_API afc_status afc_stft_forward(afc_plan plan, const void* signal, int64_t signal_len, const void* window,
                                     int64_t hop, void* out, int64_t out_elems, void* stream);
+/* Inverse STFT by weighted overlap-add, apollo-stft StftPlan::inverse_into
+ * (stft/dimension_1d.rs:250-345): every frame's normalized inverse FFT, real
+ * part, times the window, overlap-added at m hop - frame_len/2 and divided by
+ * the summed squared window (zero where no frame covers a sample).
+ * `spectrum_elems` = frames x frame_len with frames from signal_len as in the
+ * forward; `out` receives signal_len reals.  `workspace` holds the transformed
+ * frames: at least afc_stft_inverse_workspace() bytes (frames x frame_len reals),
+ * caller-owned device memory. */
+AFC_API afc_status afc_stft_inverse_workspace(afc_plan plan, int64_t hop, int64_t signal_len, size_t* bytes);
+AFC_API afc_status afc_stft_inverse(afc_plan plan, const void* spectrum, int64_t spectrum_elems, const void* window,
+                                    int64_t hop, void* out, int64_t signal_len, void* workspace, size_t workspace_bytes,
+                                    void* stream);
 
 /* Chirp z-transform on the device: X_k = sum_j x_j A^-j W^(j k), j < n, k < m,
  * by Bluestein's identity in one launch (chirp premultiply fused into the

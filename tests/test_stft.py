@@ -78,3 +78,44 @@ def test_stft_validation(afc, cuda):
         plan.forward(torch.zeros(63, dtype=torch.float64, device="cuda"))
     with pytest.raises(StftError):
         plan.forward(torch.zeros(100, dtype=torch.float64, device="cuda"), window=np.ones(10))
+
+
+def istft_ref(spec, window, frame_len, hop, n_sig, oracle):
+    frames = spec.shape[0]
+    fr = oracle.fft1d(spec.astype(np.complex128), inverse=True).real * window
+    overlap = np.zeros(n_sig)
+    weight = np.zeros(n_sig)
+    for m in range(frames):
+        start = m * hop - frame_len // 2
+        for i in range(frame_len):
+            j = start + i
+            if 0 <= j < n_sig:
+                overlap[j] += fr[m, i]
+                weight[j] += window[i] * window[i]
+    out = np.where(weight > 0, overlap / np.where(weight > 0, weight, 1.0), 0.0)
+    return out, weight
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("frame_len,hop,n_sig", [(8, 4, 12), (512, 128, 8192), (256, 200, 1000), (1024, 256, 20001),
+                                                 (243, 81, 5000)])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_stft_inverse_vs_reference_and_roundtrip(afc, oracle, cuda, frame_len, hop, n_sig, prec):
+    from apollofft_b200.stft import StftPlan
+    rng = np.random.default_rng(frame_len * 3 + hop + n_sig)
+    sig = rng.standard_normal(n_sig)
+    plan = StftPlan(frame_len, hop, precision=prec)
+    rdt = np.float64 if prec == "f64" else np.float32
+    cdt = np.complex128 if prec == "f64" else np.complex64
+    spec = plan.forward(torch.from_numpy(sig.astype(rdt)).cuda())
+    y = plan.inverse(spec, n_sig).cpu().numpy()
+    ref, weight = istft_ref(spec.cpu().numpy().astype(np.complex128), plan.window.astype(rdt).astype(np.float64),
+                            frame_len, hop, n_sig, oracle)
+    tol = 1e-12 if prec == "f64" else 1e-5
+    assert rel_l2(y, ref) < tol, rel_l2(y, ref)
+    covered = weight > 1e-3
+    assert rel_l2(y[covered], sig[covered]) < (1e-12 if prec == "f64" else 1e-5)
+    # a spectrum of the wrong size is rejected
+    from apollofft_b200.stft import StftError
+    with pytest.raises(StftError):
+        plan.inverse(spec[:-1].contiguous(), n_sig)
