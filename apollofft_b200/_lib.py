@@ -103,6 +103,11 @@ SIGNATURES = {
     "afc_nufft1d_type1": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),
     "afc_nufft1d_type2": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),
     "afc_nufft_plan_destroy": (_i32, [_vp]),
+    "afc_nufft3d_plan_create": (_i32, [ctypes.POINTER(_vp), _i64, _i64, _i64, _dbl, _dbl, _dbl, _i64, _i64, _i32]),
+    "afc_nufft3d_grid_dims": (_i32, [_vp, ctypes.POINTER(_i64)]),
+    "afc_nufft3d_type1": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),
+    "afc_nufft3d_type2": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),
+    "afc_nufft3d_plan_destroy": (_i32, [_vp]),
 }
 
 _lib = None

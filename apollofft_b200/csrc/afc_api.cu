@@ -1005,6 +1005,21 @@ struct afc_nufft_plan_s {
   ~afc_nufft_plan_s();
 };
 
+// 3D NUFFT plan (apollo-nufft NufftPlan3D, transform/dimension_3d.rs:193-230):
+// per axis m = next_pow2(max(sigma n, 2w + 1)), one C2C f64 plan of
+// (mx, my, mz) over the plan-owned grid, deconvolution factors per axis.
+struct afc_nufft3d_plan_s {
+  int64_t n[3] = {0, 0, 0}, m[3] = {0, 0, 0};
+  double d[3] = {0, 0, 0};
+  int w = 0;
+  double beta = 0, i0b = 1;
+  int device = 0;
+  afc_plan fft = nullptr;
+  double* deconv = nullptr;  // nx + ny + nz factors, axis after axis
+  void* grid = nullptr;      // mx my mz complex128, C order
+  ~afc_nufft3d_plan_s();
+};
+
 // Chirp z-transform plan (apollo-czt CztPlan, plan/czt/dimension_1d.rs:60-120):
 // input length n, output length m, X_k = sum_j x_j A^-j W^(j k) by Bluestein's
 // identity over a convolution of length L = next_pow2(n + m - 1).
@@ -1614,6 +1629,12 @@ afc_nufft_plan_s::~afc_nufft_plan_s() {
   if (grid) cudaFree(grid);
 }
 
+afc_nufft3d_plan_s::~afc_nufft3d_plan_s() {
+  if (fft) afc_plan_destroy(fft);
+  if (deconv) cudaFree(deconv);
+  if (grid) cudaFree(grid);
+}
+
 extern "C" {
 
 afc_status afc_plan_create(afc_plan* out, int rank, const int64_t* dims, afc_precision precision, afc_kind kind,
@@ -1816,7 +1837,7 @@ afc_status afc_stft_inverse(afc_plan plan, const void* spectrum, int64_t spectru
 
 // num-complex powf (polar form): |z|^e exp(i arg(z) e), as the reference's
 // CztPlan builds its chirps (czt/dimension_1d.rs:85-98).
-static std::complex<double> cpowf(std::complex<double> z, double e) {
+static std::complex<double> czt_pow(std::complex<double> z, double e) {
   return std::polar(std::pow(std::abs(z), e), std::arg(z) * e);
 }
 
@@ -1852,10 +1873,10 @@ afc_status afc_czt_plan_create(afc_czt_plan* out, int64_t n, int64_t m, double a
   p->device = device;
   const std::complex<double> A(a_re, a_im), W(w_re, w_im);
   std::vector<std::complex<double>> cn(n), ck(m), ker(L, 0.0);
-  for (int64_t j = 0; j < n; ++j) cn[j] = cpowf(A, -(double)j) * cpowf(W, 0.5 * (double)j * (double)j);
-  for (int64_t k = 0; k < m; ++k) ck[k] = cpowf(W, 0.5 * (double)k * (double)k);
-  for (int64_t k = 0; k < m; ++k) ker[k] = cpowf(W, -0.5 * (double)k * (double)k) / (double)L;
-  for (int64_t j = 1; j < n; ++j) ker[L - j] = cpowf(W, -0.5 * (double)j * (double)j) / (double)L;
+  for (int64_t j = 0; j < n; ++j) cn[j] = czt_pow(A, -(double)j) * czt_pow(W, 0.5 * (double)j * (double)j);
+  for (int64_t k = 0; k < m; ++k) ck[k] = czt_pow(W, 0.5 * (double)k * (double)k);
+  for (int64_t k = 0; k < m; ++k) ker[k] = czt_pow(W, -0.5 * (double)k * (double)k) / (double)L;
+  for (int64_t j = 1; j < n; ++j) ker[L - j] = czt_pow(W, -0.5 * (double)j * (double)j) / (double)L;
   auto upload = [&](const std::vector<std::complex<double>>& v, void** dst) -> cudaError_t {
     cudaError_t e = dev_alloc(dst, v.size() * csz);
     if (e != cudaSuccess) return e;
@@ -2024,6 +2045,123 @@ afc_status afc_nufft1d_type2(afc_nufft_plan plan, const void* coeffs, const doub
 }
 
 afc_status afc_nufft_plan_destroy(afc_nufft_plan plan) {
+  if (!plan) return AFC_OK;
+  DeviceGuard g(plan->device);
+  delete plan;
+  return AFC_OK;
+}
+
+afc_status afc_nufft3d_plan_create(afc_nufft3d_plan* out, int64_t nx, int64_t ny, int64_t nz, double dx, double dy,
+                                   double dz, int64_t sigma, int64_t kernel_width, int device) {
+  if (!out) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  *out = nullptr;
+  const int64_t n[3] = {nx, ny, nz};
+  const double d[3] = {dx, dy, dz};
+  static const char* nname[3] = {"nx", "ny", "nz"};
+  static const char* dname[3] = {"dx", "dy", "dz"};
+  for (int a = 0; a < 3; ++a) {
+    if (n[a] < 1)
+      return fail(AFC_ERR_VALIDATION, "validation failed for `%s`: `%lld` violates `must be > 0`", nname[a],
+                  (long long)n[a]);
+    if (!std::isfinite(d[a]) || d[a] <= 0.0)
+      return fail(AFC_ERR_VALIDATION, "validation failed for `%s`: `%g` violates `must be finite and > 0`", dname[a],
+                  d[a]);
+  }
+  if (sigma < 2) return fail(AFC_ERR_VALIDATION, "validation failed for `sigma`: `%lld` violates `>= 2`", (long long)sigma);
+  if (kernel_width < 2 || kernel_width > 32)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `kernel_width`: `%lld` violates `2..32`", (long long)kernel_width);
+  std::unique_ptr<afc_nufft3d_plan_s> p(new afc_nufft3d_plan_s());
+  p->w = (int)kernel_width;
+  p->beta = M_PI * (1.0 - 1.0 / (2.0 * (double)sigma)) * (double)(2 * kernel_width);
+  p->i0b = nu_i0_host(p->beta);
+  p->device = device;
+  int64_t total_n = 0;
+  for (int a = 0; a < 3; ++a) {
+    p->n[a] = n[a];
+    p->d[a] = d[a];
+    if (n[a] > (int64_t(1) << 40) / sigma)
+      return fail(AFC_ERR_VALIDATION, "validation failed for `%s`: `%lld` violates `oversampled length overflow`",
+                  nname[a], (long long)n[a]);
+    int64_t lower = std::max<int64_t>(n[a] * sigma, 2 * kernel_width + 1), m = 1;
+    while (m < lower) m <<= 1;
+    p->m[a] = m;
+    total_n += n[a];
+  }
+  afc_status s = afc_plan_create(&p->fft, 3, p->m, AFC_PREC_F64, AFC_KIND_C2C, 1, device);
+  if (s != AFC_OK) return s;
+  DeviceGuard g(device);
+  std::vector<double> dec;
+  dec.reserve((size_t)total_n);
+  for (int a = 0; a < 3; ++a)
+    for (int64_t k = 0; k < n[a]; ++k) {
+      const int64_t ks = k <= n[a] / 2 ? k : k - n[a];
+      dec.push_back(1.0 / nu_kb_ft((double)ks / (double)p->m[a], p->w, p->beta, p->i0b));
+    }
+  AFC_CUDA(dev_alloc((void**)&p->deconv, (size_t)total_n * sizeof(double)), "NUFFT deconvolution");
+  AFC_CUDA(cudaMemcpy(p->deconv, dec.data(), (size_t)total_n * sizeof(double), cudaMemcpyHostToDevice),
+           "NUFFT deconvolution");
+  AFC_CUDA(dev_alloc(&p->grid, (size_t)(p->m[0] * p->m[1] * p->m[2]) * 16), "NUFFT grid");
+  *out = p.release();
+  return AFC_OK;
+}
+
+afc_status afc_nufft3d_grid_dims(afc_nufft3d_plan plan, int64_t* m) {
+  if (!plan || !m) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  for (int a = 0; a < 3; ++a) m[a] = plan->m[a];
+  return AFC_OK;
+}
+
+static NuLaunch3 nu_launch3(const afc_nufft3d_plan_s& p) {
+  NuLaunch3 L;
+  L.nx = p.n[0], L.ny = p.n[1], L.nz = p.n[2];
+  L.mx = p.m[0], L.my = p.m[1], L.mz = p.m[2];
+  L.w = p.w;
+  L.beta = p.beta;
+  L.i0b = p.i0b;
+  L.lx = (double)p.n[0] * p.d[0];
+  L.ly = (double)p.n[1] * p.d[1];
+  L.lz = (double)p.n[2] * p.d[2];
+  return L;
+}
+
+afc_status afc_nufft3d_type1(afc_nufft3d_plan plan, const double* positions, const void* values, int64_t npts,
+                             void* out, void* stream) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (npts < 0) return fail(AFC_ERR_VALIDATION, "validation failed for `npts`: `%lld` violates `>= 0`", (long long)npts);
+  if (!out || (npts > 0 && (!positions || !values)))
+    return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  DeviceGuard g(plan->device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const NuLaunch3 L = nu_launch3(*plan);
+  AFC_CUDA(cudaMemsetAsync(plan->grid, 0, (size_t)(L.mx * L.my * L.mz) * 16, st), "NUFFT grid");
+  AFC_CUDA(nufft3_spread_dev(L, positions, values, npts, plan->grid, st), "NUFFT spread");
+  afc_status s = afc_execute(plan->fft, plan->grid, plan->grid, AFC_FORWARD, stream);
+  if (s != AFC_OK) return s;
+  const double* dc = plan->deconv;
+  AFC_CUDA(nufft3_modes_dev(L, dc, dc + L.nx, dc + L.nx + L.ny, plan->grid, out, false, st), "NUFFT deconvolution");
+  return AFC_OK;
+}
+
+afc_status afc_nufft3d_type2(afc_nufft3d_plan plan, const void* modes, const double* positions, int64_t npts,
+                             void* out, void* stream) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (npts < 0) return fail(AFC_ERR_VALIDATION, "validation failed for `npts`: `%lld` violates `>= 0`", (long long)npts);
+  if (!modes || (npts > 0 && (!positions || !out)))
+    return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  DeviceGuard g(plan->device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const NuLaunch3 L = nu_launch3(*plan);
+  AFC_CUDA(cudaMemsetAsync(plan->grid, 0, (size_t)(L.mx * L.my * L.mz) * 16, st), "NUFFT grid");
+  const double* dc = plan->deconv;
+  AFC_CUDA(nufft3_modes_dev(L, dc, dc + L.nx, dc + L.nx + L.ny, modes, plan->grid, true, st), "NUFFT modes");
+  // the reference's three normalized inverse axis passes: scale 1/(mx my mz)
+  afc_status s = afc_execute(plan->fft, plan->grid, plan->grid, AFC_INVERSE, stream);
+  if (s != AFC_OK) return s;
+  AFC_CUDA(nufft3_interp_dev(L, plan->grid, positions, npts, out, st), "NUFFT interpolation");
+  return AFC_OK;
+}
+
+afc_status afc_nufft3d_plan_destroy(afc_nufft3d_plan plan) {
   if (!plan) return AFC_OK;
   DeviceGuard g(plan->device);
   delete plan;

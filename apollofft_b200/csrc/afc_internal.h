@@ -115,6 +115,17 @@ cudaError_t nufft_interp_dev(const NuLaunch& L, const void* grid, const double* 
                              cudaStream_t st);
 cudaError_t nufft_deconv_out_dev(const void* grid, const double* deconv, long long n, long long m, void* out,
                                  cudaStream_t st);
+struct NuLaunch3 {
+  long long nx = 0, ny = 0, nz = 0, mx = 0, my = 0, mz = 0;
+  int w = 0;
+  double beta = 0, i0b = 1, lx = 1, ly = 1, lz = 1;
+};
+cudaError_t nufft3_spread_dev(const NuLaunch3& L, const double* pos, const void* val, long long npts, void* grid,
+                              cudaStream_t st);
+cudaError_t nufft3_interp_dev(const NuLaunch3& L, const void* grid, const double* pos, long long npts, void* out,
+                              cudaStream_t st);
+cudaError_t nufft3_modes_dev(const NuLaunch3& L, const double* dcx, const double* dcy, const double* dcz,
+                             const void* src, void* dst, bool to_grid, cudaStream_t st);
 cudaError_t nufft_place_coeffs_dev(const void* coeffs, const double* deconv, long long n, long long m, void* grid,
                                    cudaStream_t st);
 cudaError_t launch_wait_probe(unsigned* err, int polls, cudaStream_t st);

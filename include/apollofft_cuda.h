@@ -258,6 +258,30 @@ AFC_API afc_status afc_nufft1d_type2(afc_nufft_plan plan, const void* coeffs, co
                                      void* out, void* stream);
 AFC_API afc_status afc_nufft_plan_destroy(afc_nufft_plan plan);
 
+/* 3D non-uniform FFT on the device, apollo-nufft NufftPlan3D
+ * (apollo-nufft/.../transform/dimension_3d.rs:193-620): nx x ny x nz modes on
+ * the periodic box [0, nx dx) x [0, ny dy) x [0, nz dz); per axis the
+ * oversampled length is next_pow2(max(sigma n, 2 kernel_width + 1))
+ * (dimension_3d.rs:48-54); separable Kaiser-Bessel weights over
+ * (2 kernel_width + 1)^3 cells.  Positions are npts x 3 float64 (x, y, z per
+ * point), values / modes / outputs complex128, modes and type-1 outputs C order
+ * [kx][ky][kz]; all device pointers.  Type 1: out[kx,ky,kz] ~ sum_j values_j
+ * exp(-2 pi i (kx_s x_j / Lx + ky_s y_j / Ly + kz_s z_j / Lz)).  Type 2 follows
+ * the reference's normalized inverse axis passes (dimension_3d.rs:548-551):
+ * out[j] ~ sum_k modes_k exp(+2 pi i (...)) / (mx my mz).  Spreading uses
+ * atomic adds instead of the reference's bucket sort (rounding differs only).
+ * One grid per plan: overlapping calls on different streams race.
+ * afc_nufft3d_grid_dims writes (mx, my, mz). */
+typedef struct afc_nufft3d_plan_s* afc_nufft3d_plan;
+AFC_API afc_status afc_nufft3d_plan_create(afc_nufft3d_plan* out, int64_t nx, int64_t ny, int64_t nz, double dx,
+                                           double dy, double dz, int64_t sigma, int64_t kernel_width, int device);
+AFC_API afc_status afc_nufft3d_grid_dims(afc_nufft3d_plan plan, int64_t* m);
+AFC_API afc_status afc_nufft3d_type1(afc_nufft3d_plan plan, const double* positions, const void* values, int64_t npts,
+                                     void* out, void* stream);
+AFC_API afc_status afc_nufft3d_type2(afc_nufft3d_plan plan, const void* modes, const double* positions, int64_t npts,
+                                     void* out, void* stream);
+AFC_API afc_status afc_nufft3d_plan_destroy(afc_nufft3d_plan plan);
+
 /* Allocation-free execution of a rank-1 C2C plan whose length runs on the
  * two-pass (four-step) kernels: the intermediate between the passes lives in a
  * 16 MiB static device array instead of a cudaMalloc'd workspace, so the call
