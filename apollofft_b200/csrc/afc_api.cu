@@ -1017,6 +1017,8 @@ struct afc_nufft3d_plan_s {
   afc_plan fft = nullptr;
   double* deconv = nullptr;  // nx + ny + nz factors, axis after axis
   void* grid = nullptr;      // mx my mz complex128, C order
+  afc::NuTileLaunch tiles;   // B = 0: per-point kernels
+  int64_t pts_cap = 0;       // points the tile / rank / index buffers hold
   ~afc_nufft3d_plan_s();
 };
 
@@ -1630,6 +1632,8 @@ afc_nufft_plan_s::~afc_nufft_plan_s() {
 }
 
 afc_nufft3d_plan_s::~afc_nufft3d_plan_s() {
+  for (int* b : {tiles.cnt, tiles.off, tiles.tile, tiles.rank, tiles.idx})
+    if (b) cudaFree(b);
   if (fft) afc_plan_destroy(fft);
   if (deconv) cudaFree(deconv);
   if (grid) cudaFree(grid);
@@ -2101,7 +2105,33 @@ afc_status afc_nufft3d_plan_create(afc_nufft3d_plan* out, int64_t nx, int64_t ny
   AFC_CUDA(cudaMemcpy(p->deconv, dec.data(), (size_t)total_n * sizeof(double), cudaMemcpyHostToDevice),
            "NUFFT deconvolution");
   AFC_CUDA(dev_alloc(&p->grid, (size_t)(p->m[0] * p->m[1] * p->m[2]) * 16), "NUFFT grid");
+  const int B = nufft3_tile_size(p->w);
+  const int64_t ntiles = B ? (p->m[0] / B) * (p->m[1] / B) * (p->m[2] / B) : 0;
+  if (B && ntiles < (int64_t(1) << 30)) {
+    p->tiles.B = B;
+    p->tiles.ntx = (int)(p->m[0] / B);
+    p->tiles.nty = (int)(p->m[1] / B);
+    p->tiles.ntz = (int)(p->m[2] / B);
+    AFC_CUDA(dev_alloc((void**)&p->tiles.cnt, (size_t)ntiles * sizeof(int)), "NUFFT tiles");
+    AFC_CUDA(dev_alloc((void**)&p->tiles.off, (size_t)(ntiles + 1) * sizeof(int)), "NUFFT tiles");
+  }
   *out = p.release();
+  return AFC_OK;
+}
+
+// Grows the per-point tile buffers (synchronous allocation) when a call brings
+// more points than any call before it; false -> the per-point kernels run.
+static afc_status nu3_reserve(afc_nufft3d_plan_s& p, int64_t npts, bool* tiled) {
+  *tiled = p.tiles.B != 0 && npts > 0 && npts <= INT32_MAX;
+  if (!*tiled || npts <= p.pts_cap) return AFC_OK;
+  for (int** b : {&p.tiles.tile, &p.tiles.rank, &p.tiles.idx}) {
+    if (*b) cudaFree(*b);
+    *b = nullptr;
+  }
+  p.pts_cap = 0;
+  for (int** b : {&p.tiles.tile, &p.tiles.rank, &p.tiles.idx})
+    AFC_CUDA(dev_alloc((void**)b, (size_t)npts * sizeof(int)), "NUFFT point buckets");
+  p.pts_cap = npts;
   return AFC_OK;
 }
 
@@ -2134,7 +2164,13 @@ afc_status afc_nufft3d_type1(afc_nufft3d_plan plan, const double* positions, con
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const NuLaunch3 L = nu_launch3(*plan);
   AFC_CUDA(cudaMemsetAsync(plan->grid, 0, (size_t)(L.mx * L.my * L.mz) * 16, st), "NUFFT grid");
-  AFC_CUDA(nufft3_spread_dev(L, positions, values, npts, plan->grid, st), "NUFFT spread");
+  bool tiled = false;
+  afc_status r = nu3_reserve(*plan, npts, &tiled);
+  if (r != AFC_OK) return r;
+  if (tiled)
+    AFC_CUDA(nufft3_tiled_dev(L, plan->tiles, true, positions, values, npts, plan->grid, st), "NUFFT spread");
+  else
+    AFC_CUDA(nufft3_spread_dev(L, positions, values, npts, plan->grid, st), "NUFFT spread");
   afc_status s = afc_execute(plan->fft, plan->grid, plan->grid, AFC_FORWARD, stream);
   if (s != AFC_OK) return s;
   const double* dc = plan->deconv;
@@ -2157,7 +2193,13 @@ afc_status afc_nufft3d_type2(afc_nufft3d_plan plan, const void* modes, const dou
   // the reference's three normalized inverse axis passes: scale 1/(mx my mz)
   afc_status s = afc_execute(plan->fft, plan->grid, plan->grid, AFC_INVERSE, stream);
   if (s != AFC_OK) return s;
-  AFC_CUDA(nufft3_interp_dev(L, plan->grid, positions, npts, out, st), "NUFFT interpolation");
+  bool tiled = false;
+  s = nu3_reserve(*plan, npts, &tiled);
+  if (s != AFC_OK) return s;
+  if (tiled)
+    AFC_CUDA(nufft3_tiled_dev(L, plan->tiles, false, positions, plan->grid, npts, out, st), "NUFFT interpolation");
+  else
+    AFC_CUDA(nufft3_interp_dev(L, plan->grid, positions, npts, out, st), "NUFFT interpolation");
   return AFC_OK;
 }
 

@@ -124,6 +124,20 @@ cudaError_t nufft3_spread_dev(const NuLaunch3& L, const double* pos, const void*
                               cudaStream_t st);
 cudaError_t nufft3_interp_dev(const NuLaunch3& L, const void* grid, const double* pos, long long npts, void* out,
                               cudaStream_t st);
+// Tiled spreading / interpolation: tile edge B (8 or 4; 0 = the kernel is too
+// wide for a shared-memory tile and the per-point kernels run instead).
+struct NuTileLaunch {
+  int B = 0, ntx = 0, nty = 0, ntz = 0;
+  int* cnt = nullptr;   // ntiles
+  int* off = nullptr;   // ntiles + 1
+  int* tile = nullptr;  // npts
+  int* rank = nullptr;  // npts
+  int* idx = nullptr;   // npts
+};
+int nufft3_tile_size(int w);
+size_t nufft3_tile_smem(int B, int w);
+cudaError_t nufft3_tiled_dev(const NuLaunch3& L, const NuTileLaunch& TL, bool spread, const double* pos,
+                             const void* src, long long npts, void* dst, cudaStream_t st);
 cudaError_t nufft3_modes_dev(const NuLaunch3& L, const double* dcx, const double* dcy, const double* dcz,
                              const void* src, void* dst, bool to_grid, cudaStream_t st);
 cudaError_t nufft_place_coeffs_dev(const void* coeffs, const double* deconv, long long n, long long m, void* grid,

@@ -15,14 +15,32 @@
 
 namespace afc {
 
-// I0(z) = sum_k ((z/2)^2)^k / (k!)^2, summed until the term drops below
-// epsilon of the sum (at most 256 terms).
+// I0(z) = sum_k ((z/2)^2)^k / (k!)^2: term_k = term_{k-1} (z/2)^2 / k^2, the
+// ratios from a table of 1/k^2 (so the running product is a chain of
+// multiplies, not divides), summed four terms at a time until the last of them
+// drops below epsilon of the sum (at most 256 terms).  The terms the reference
+// would not add are below epsilon of the sum.
+struct NuInvSquares {
+  double v[257];
+  constexpr NuInvSquares() : v() {
+    for (int k = 1; k <= 256; ++k) v[k] = 1.0 / ((double)k * (double)k);
+  }
+};
+__constant__ NuInvSquares c_nu_inv_k2 = NuInvSquares();
+
 __device__ __forceinline__ double nu_i0(double z) {
   const double scaled = 0.25 * z * z;
   double sum = 1.0, term = 1.0;
-  for (int k = 1; k <= 256; ++k) {
-    const double kf = (double)k;
-    term *= scaled / (kf * kf);
+  for (int k = 1; k <= 256; k += 4) {
+    const double q0 = scaled * c_nu_inv_k2.v[k], q1 = scaled * c_nu_inv_k2.v[k + 1];
+    const double q2 = scaled * c_nu_inv_k2.v[k + 2], q3 = scaled * c_nu_inv_k2.v[k + 3];
+    term *= q0;
+    sum += term;
+    term *= q1;
+    sum += term;
+    term *= q2;
+    sum += term;
+    term *= q3;
     sum += term;
     if (term <= 2.220446049250313e-16 * sum) break;
   }
@@ -121,8 +139,12 @@ __global__ void nu_place_coeffs(const double2* __restrict__ coeffs, const double
 }
 
 // ─── 3D (apollo-nufft NufftPlan3D, transform/dimension_3d.rs:193-620) ───
-// Separable kernel: weight = phi_x phi_y phi_z over (2w+1)^3 taps; grid C-order
-// [ix][iy][iz] of size mx x my x mz.
+// Separable kernel: weight = phi_x phi_y phi_z over T^3 taps, T = 2w + 1; grid
+// C-order [ix][iy][iz] of size mx x my x mz, every m a power of two.
+// One warp per point: the lanes evaluate the 3T axis weights into shared
+// memory, then walk the T x T (py, pz) plane flattened over the 32 lanes for
+// every px, so one warp instruction touches two or three contiguous runs of T
+// cells (T = 13: 6 instructions per plane) instead of 32 scattered cells.
 struct NuGeom3 {
   long long mx, my, mz;
   int w;
@@ -130,15 +152,8 @@ struct NuGeom3 {
   double lx, ly, lz;
 };
 
-constexpr int kNuMaxTaps = 65;  // 2 w + 1 for w <= 32
-
-__device__ __forceinline__ void nu_weights(double t, long long m, const NuGeom3& g, long long& m0, double* wt) {
-  const double rt = round(t);
-  m0 = (long long)rt;
-  const double d = t - rt;
-  for (int p = -g.w; p <= g.w; ++p) wt[p + g.w] = nu_kb((double)p - d, (double)g.w, g.beta, g.i0b);
-  (void)m;
-}
+constexpr int kNuMaxTaps = 65;       // T for w <= 32
+constexpr int kNuWarps = 8;          // warps (points in flight) per 256-thread CTA
 
 __device__ __forceinline__ double nu_axis_t(double x, double len, long long m) {
   double r = fmod(x, len);
@@ -146,64 +161,355 @@ __device__ __forceinline__ double nu_axis_t(double x, double len, long long m) {
   return (double)m * r / len;
 }
 
-__global__ void nu_spread3(NuGeom3 g, const double* __restrict__ pos, const double2* __restrict__ val, long long npts,
-                           double2* grid) {
-  double wx[kNuMaxTaps], wy[kNuMaxTaps], wz[kNuMaxTaps];
-  const int taps = 2 * g.w + 1;
-  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < npts; j += (long long)gridDim.x * blockDim.x) {
-    long long m0x, m0y, m0z;
-    nu_weights(nu_axis_t(pos[3 * j], g.lx, g.mx), g.mx, g, m0x, wx);
-    nu_weights(nu_axis_t(pos[3 * j + 1], g.ly, g.my), g.my, g, m0y, wy);
-    nu_weights(nu_axis_t(pos[3 * j + 2], g.lz, g.mz), g.mz, g, m0z, wz);
+// Lanes fill wt[0..T) for one axis and return m0 (the same in every lane).
+__device__ __forceinline__ long long nu_axis_weights(double x, double len, long long m, const NuGeom3& g, int lane,
+                                                     double* wt) {
+  const double t = nu_axis_t(x, len, m);
+  const double rt = round(t);
+  const double d = t - rt;
+  for (int p = lane; p <= 2 * g.w; p += 32) wt[p] = nu_kb((double)(p - g.w) - d, (double)g.w, g.beta, g.i0b);
+  return (long long)rt;
+}
+
+struct NuPlaneWalk {  // lane's (py, pz) start and the constant stride of 32 flattened cells
+  int py0, pz0, dpy, dpz, iters;
+  __device__ NuPlaneWalk(int T, int lane)
+      : py0(lane / T), pz0(lane % T), dpy(32 / T), dpz(32 % T), iters((T * T + 31) / 32) {}
+};
+
+__global__ void __launch_bounds__(32 * kNuWarps) nu_spread3(NuGeom3 g, const double* __restrict__ pos,
+                                                              const double2* __restrict__ val, long long npts,
+                                                              double2* grid) {
+  __shared__ double sw[kNuWarps][3][kNuMaxTaps];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int T = 2 * g.w + 1;
+  const NuPlaneWalk pw(T, lane);
+  const long long mxm = g.mx - 1, mym = g.my - 1, mzm = g.mz - 1;
+  double* wx = sw[wid][0];
+  double* wy = sw[wid][1];
+  double* wz = sw[wid][2];
+  const long long warps = (long long)gridDim.x * kNuWarps;
+  for (long long j = (long long)blockIdx.x * kNuWarps + wid; j < npts; j += warps) {
+    const long long m0x = nu_axis_weights(pos[3 * j], g.lx, g.mx, g, lane, wx);
+    const long long m0y = nu_axis_weights(pos[3 * j + 1], g.ly, g.my, g, lane, wy);
+    const long long m0z = nu_axis_weights(pos[3 * j + 2], g.lz, g.mz, g, lane, wz);
     const double2 v = val[j];
-    for (int px = 0; px < taps; ++px) {
-      if (wx[px] == 0.0) continue;
-      const long long ix = nu_wrap(m0x + px - g.w, g.mx);
-      for (int py = 0; py < taps; ++py) {
-        if (wy[py] == 0.0) continue;
-        const long long iy = nu_wrap(m0y + py - g.w, g.my);
-        const double wxy = wx[px] * wy[py];
-        double2* row = grid + (ix * g.my + iy) * g.mz;
-        for (int pz = 0; pz < taps; ++pz) {
-          if (wz[pz] == 0.0) continue;
-          const double wt = wxy * wz[pz];
-          double2* c = row + nu_wrap(m0z + pz - g.w, g.mz);
-          atomicAdd(&c->x, v.x * wt);
-          atomicAdd(&c->y, v.y * wt);
+    __syncwarp();
+    for (int px = 0; px < T; ++px) {
+      const double wxv = wx[px];
+      if (wxv == 0.0) continue;
+      double2* plane = grid + ((m0x + px - g.w) & mxm) * g.my * g.mz;
+      int py = pw.py0, pz = pw.pz0;
+      for (int it = 0; it < pw.iters; ++it) {
+        if (py < T) {
+          const double wt = wxv * wy[py] * wz[pz];
+          if (wt != 0.0) {
+            double2* c = plane + ((m0y + py - g.w) & mym) * g.mz + ((m0z + pz - g.w) & mzm);
+            atomicAdd(&c->x, v.x * wt);
+            atomicAdd(&c->y, v.y * wt);
+          }
         }
+        py += pw.dpy;
+        pz += pw.dpz;
+        if (pz >= T) pz -= T, ++py;
       }
     }
+    __syncwarp();
   }
 }
 
-__global__ void nu_interp3(NuGeom3 g, const double2* __restrict__ grid, const double* __restrict__ pos, long long npts,
-                           double2* out) {
-  double wx[kNuMaxTaps], wy[kNuMaxTaps], wz[kNuMaxTaps];
-  const int taps = 2 * g.w + 1;
+__global__ void __launch_bounds__(32 * kNuWarps) nu_interp3(NuGeom3 g, const double2* __restrict__ grid,
+                                                              const double* __restrict__ pos, long long npts,
+                                                              double2* out) {
+  __shared__ double sw[kNuWarps][3][kNuMaxTaps];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int T = 2 * g.w + 1;
+  const NuPlaneWalk pw(T, lane);
+  const long long mxm = g.mx - 1, mym = g.my - 1, mzm = g.mz - 1;
+  double* wx = sw[wid][0];
+  double* wy = sw[wid][1];
+  double* wz = sw[wid][2];
+  const long long warps = (long long)gridDim.x * kNuWarps;
+  for (long long j = (long long)blockIdx.x * kNuWarps + wid; j < npts; j += warps) {
+    const long long m0x = nu_axis_weights(pos[3 * j], g.lx, g.mx, g, lane, wx);
+    const long long m0y = nu_axis_weights(pos[3 * j + 1], g.ly, g.my, g, lane, wy);
+    const long long m0z = nu_axis_weights(pos[3 * j + 2], g.lz, g.mz, g, lane, wz);
+    __syncwarp();
+    double ax = 0.0, ay = 0.0;
+    for (int px = 0; px < T; ++px) {
+      const double wxv = wx[px];
+      if (wxv == 0.0) continue;
+      const double2* plane = grid + ((m0x + px - g.w) & mxm) * g.my * g.mz;
+      int py = pw.py0, pz = pw.pz0;
+      for (int it = 0; it < pw.iters; ++it) {
+        if (py < T) {
+          const double wt = wxv * wy[py] * wz[pz];
+          if (wt != 0.0) {
+            const double2 c = plane[((m0y + py - g.w) & mym) * g.mz + ((m0z + pz - g.w) & mzm)];
+            ax += c.x * wt;
+            ay += c.y * wt;
+          }
+        }
+        py += pw.dpy;
+        pz += pw.dpz;
+        if (pz >= T) pz -= T, ++py;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      ax += __shfl_xor_sync(0xffffffffu, ax, o);
+      ay += __shfl_xor_sync(0xffffffffu, ay, o);
+    }
+    if (lane == 0) out[j] = make_double2(ax, ay);
+    __syncwarp();
+  }
+}
+
+// ─── tiled 3D spreading / interpolation ───
+// Points are bucketed by the B^3 tile of cells that holds their centre cell
+// round(t) mod m (the reference bucket-sorts its points too, sort_points_3d,
+// dimension_3d.rs:74-117); one CTA per tile keeps the tile and its w-cell halo,
+// E^3 cells with E = B + 2w, in shared memory.  Spreading: warp k owns the
+// x-planes lx = k mod 16 of the tile and adds every point's taps on its planes
+// with plain shared-memory read-modify-writes (no two warps share a cell),
+// then the CTA adds its E^3 cells to the grid with coalesced atomics (tiles'
+// halos overlap); grid atomics drop from (2w+1)^3 per point to E^3 per tile.
+// Interpolation: the CTA loads its E^3 cells once, one warp per point gathers
+// from shared memory.
+constexpr int kNuTileThreads = 512;
+constexpr int kNuTileWarps = kNuTileThreads / 32;
+constexpr int kNuChunk = 32;  // points whose weights the spreading CTA stages at once
+
+struct NuTiles {
+  int B, E, nty, ntz;
+  const int* off;  // ntiles + 1 offsets into idx
+  const int* idx;  // point indices grouped by tile
+};
+
+__device__ __forceinline__ int nu_centre(double x, double len, long long m) {
+  return (int)((long long)round(nu_axis_t(x, len, m)) & (m - 1));
+}
+
+__global__ void nu3_bin(NuGeom3 g, int B, int nty, int ntz, const double* __restrict__ pos, long long npts,
+                        int* __restrict__ cnt, int* __restrict__ tile, int* __restrict__ rank) {
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < npts; j += (long long)gridDim.x * blockDim.x) {
-    long long m0x, m0y, m0z;
-    nu_weights(nu_axis_t(pos[3 * j], g.lx, g.mx), g.mx, g, m0x, wx);
-    nu_weights(nu_axis_t(pos[3 * j + 1], g.ly, g.my), g.my, g, m0y, wy);
-    nu_weights(nu_axis_t(pos[3 * j + 2], g.lz, g.mz), g.mz, g, m0z, wz);
-    double2 acc = make_double2(0.0, 0.0);
-    for (int px = 0; px < taps; ++px) {
-      if (wx[px] == 0.0) continue;
-      const long long ix = nu_wrap(m0x + px - g.w, g.mx);
-      for (int py = 0; py < taps; ++py) {
-        if (wy[py] == 0.0) continue;
-        const long long iy = nu_wrap(m0y + py - g.w, g.my);
-        const double wxy = wx[px] * wy[py];
-        const double2* row = grid + (ix * g.my + iy) * g.mz;
-        for (int pz = 0; pz < taps; ++pz) {
-          if (wz[pz] == 0.0) continue;
-          const double wt = wxy * wz[pz];
-          const double2 c = row[nu_wrap(m0z + pz - g.w, g.mz)];
-          acc.x += c.x * wt;
-          acc.y += c.y * wt;
+    const int cx = nu_centre(pos[3 * j], g.lx, g.mx);
+    const int cy = nu_centre(pos[3 * j + 1], g.ly, g.my);
+    const int cz = nu_centre(pos[3 * j + 2], g.lz, g.mz);
+    const int t = ((cx / B) * nty + cy / B) * ntz + cz / B;
+    tile[j] = t;
+    rank[j] = atomicAdd(&cnt[t], 1);
+  }
+}
+
+// Exclusive prefix sum of cnt[0..n) into off[0..n], one CTA of 1024 threads,
+// each over a contiguous chunk.
+__global__ void __launch_bounds__(1024) nu3_scan(const int* __restrict__ cnt, int* __restrict__ off, int n) {
+  __shared__ int wsum[32];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int per = (n + 1023) / 1024;
+  const int lo = min(n, tid * per), hi = min(n, lo + per);
+  int s = 0;
+  for (int i = lo; i < hi; ++i) s += cnt[i];
+  int v = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  if (lane == 31) wsum[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    int w = wsum[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    wsum[lane] = w;
+  }
+  __syncthreads();
+  int ex = v - s + (wid > 0 ? wsum[wid - 1] : 0);
+  for (int i = lo; i < hi; ++i) {
+    off[i] = ex;
+    ex += cnt[i];
+  }
+  if (tid == 1023) off[n] = ex;
+}
+
+__global__ void nu3_scatter(const int* __restrict__ tile, const int* __restrict__ rank, const int* __restrict__ off,
+                            long long npts, int* __restrict__ idx) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < npts; j += (long long)gridDim.x * blockDim.x)
+    idx[off[tile[j]] + rank[j]] = (int)j;
+}
+
+struct NuTileCoord {
+  int tx, ty, tz;
+  __device__ NuTileCoord(int tile, const NuTiles& tl)
+      : tx(tile / (tl.nty * tl.ntz)), ty((tile / tl.ntz) % tl.nty), tz(tile % tl.ntz) {}
+};
+
+// Axis-a weight of tap `tap` for the point at pos, and (lc non-null) the
+// point's centre cell relative to the tile origin, in [0, B).
+__device__ __forceinline__ double nu_tile_weight(const NuGeom3& g, const NuTiles& tl, const NuTileCoord& tc,
+                                                 const double* pos, int a, int tap, int* lc) {
+  const double len = a == 0 ? g.lx : a == 1 ? g.ly : g.lz;
+  const long long m = a == 0 ? g.mx : a == 1 ? g.my : g.mz;
+  const int t0 = a == 0 ? tc.tx : a == 1 ? tc.ty : tc.tz;
+  const double t = nu_axis_t(pos[a], len, m);
+  const double rt = round(t);
+  if (lc) *lc = (int)((long long)rt & (m - 1)) - t0 * tl.B;
+  return nu_kb((double)(tap - g.w) - (t - rt), (double)g.w, g.beta, g.i0b);
+}
+
+__device__ __forceinline__ int nu_tile_centre(const NuGeom3& g, const NuTiles& tl, const NuTileCoord& tc,
+                                              const double* pos, int a) {
+  const double len = a == 0 ? g.lx : a == 1 ? g.ly : g.lz;
+  const long long m = a == 0 ? g.mx : a == 1 ? g.my : g.mz;
+  const int t0 = a == 0 ? tc.tx : a == 1 ? tc.ty : tc.tz;
+  return nu_centre(pos[a], len, m) - t0 * tl.B;
+}
+
+// The lane's cells of a T x T (py, pz) plane: at most kNuTileIters, packed
+// py << 8 | pz (-1 past the plane), fixed for the whole kernel.
+constexpr int kNuTileIters = 12;  // ceil(T^2 / 32) for T <= 19 (w <= 9)
+
+struct NuLaneCells {
+  int pyz[kNuTileIters];
+  __device__ NuLaneCells(int T, int lane) {
+#pragma unroll
+    for (int it = 0; it < kNuTileIters; ++it) {
+      const int f = it * 32 + lane;
+      pyz[it] = f < T * T ? ((f / T) << 8) | (f % T) : -1;
+    }
+  }
+};
+
+__global__ void __launch_bounds__(kNuTileThreads) nu3_spread_tiles(NuGeom3 g, NuTiles tl,
+                                                                    const double* __restrict__ pos,
+                                                                    const double2* __restrict__ val, double2* grid) {
+  extern __shared__ __align__(16) unsigned char nu_smem[];
+  const int tile = blockIdx.x;
+  const int start = tl.off[tile], end = tl.off[tile + 1];
+  if (start == end) return;
+  const int T = 2 * g.w + 1, E = tl.E, E2 = E * E, E3 = E2 * E;
+  double2* acc = reinterpret_cast<double2*>(nu_smem);
+  double* wts = reinterpret_cast<double*>(acc + E3);       // kNuChunk x 3 x T
+  int* loc = reinterpret_cast<int*>(wts + kNuChunk * 3 * T);  // kNuChunk x 3
+  for (int c = threadIdx.x; c < E3; c += kNuTileThreads) acc[c] = make_double2(0.0, 0.0);
+  const NuTileCoord tc(tile, tl);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const NuLaneCells lc(T, lane);
+  int coff[kNuTileIters];
+#pragma unroll
+  for (int it = 0; it < kNuTileIters; ++it) coff[it] = lc.pyz[it] >= 0 ? (lc.pyz[it] >> 8) * E + (lc.pyz[it] & 255) : 0;
+  for (int base = start; base < end; base += kNuChunk) {
+    const int cnt = min(kNuChunk, end - base);
+    __syncthreads();  // zeroing done / previous chunk's weights consumed
+    for (int e = threadIdx.x; e < cnt * 3 * T; e += kNuTileThreads) {
+      const int p = e / (3 * T), r = e - p * 3 * T, a = r / T, tap = r - a * T;
+      const long long j = tl.idx[base + p];
+      wts[e] = nu_tile_weight(g, tl, tc, pos + 3 * j, a, tap, tap == 0 ? &loc[p * 3 + a] : nullptr);
+    }
+    __syncthreads();
+    for (int p = 0; p < cnt; ++p) {
+      const int lx0 = loc[p * 3], ly0 = loc[p * 3 + 1], lz0 = loc[p * 3 + 2];
+      int px = (wid - lx0) % kNuTileWarps;
+      if (px < 0) px += kNuTileWarps;
+      if (px >= T) continue;  // warp-uniform: none of this point's planes is ours
+      const double* wx = wts + p * 3 * T;
+      const double* wy = wx + T;
+      const double* wz = wy + T;
+      const double2 v = val[tl.idx[base + p]];
+      for (; px < T; px += kNuTileWarps) {
+        const double wxv = wx[px];
+        double2* plane = acc + (lx0 + px) * E2 + ly0 * E + lz0;
+#pragma unroll
+        for (int it = 0; it < kNuTileIters; ++it) {
+          if (lc.pyz[it] >= 0) {
+            const double wt = wxv * wy[lc.pyz[it] >> 8] * wz[lc.pyz[it] & 255];
+            double2* c = plane + coff[it];
+            double2 o = *c;
+            o.x += v.x * wt;
+            o.y += v.y * wt;
+            *c = o;
+          }
+        }
+      }
+      __syncwarp();  // the next point's lanes may touch the cells written here
+    }
+  }
+  __syncthreads();
+  const long long mxm = g.mx - 1, mym = g.my - 1, mzm = g.mz - 1;
+  const long long gx0 = (long long)tc.tx * tl.B - g.w, gy0 = (long long)tc.ty * tl.B - g.w,
+                  gz0 = (long long)tc.tz * tl.B - g.w;
+  for (int c = threadIdx.x; c < E3; c += kNuTileThreads) {
+    const double2 a = acc[c];
+    if (a.x == 0.0 && a.y == 0.0) continue;
+    const int cx = c / E2, cy = (c / E) % E, cz = c % E;
+    double2* d = grid + (((gx0 + cx) & mxm) * g.my + ((gy0 + cy) & mym)) * g.mz + ((gz0 + cz) & mzm);
+    atomicAdd(&d->x, a.x);
+    atomicAdd(&d->y, a.y);
+  }
+}
+
+__global__ void __launch_bounds__(kNuTileThreads) nu3_interp_tiles(NuGeom3 g, NuTiles tl,
+                                                                    const double2* __restrict__ grid,
+                                                                    const double* __restrict__ pos, double2* out) {
+  extern __shared__ __align__(16) unsigned char nu_smem[];
+  const int tile = blockIdx.x;
+  const int start = tl.off[tile], end = tl.off[tile + 1];
+  if (start == end) return;
+  const int T = 2 * g.w + 1, E = tl.E, E2 = E * E, E3 = E2 * E;
+  double2* cells = reinterpret_cast<double2*>(nu_smem);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double* wx = reinterpret_cast<double*>(cells + E3) + wid * 3 * T;
+  double* wy = wx + T;
+  double* wz = wy + T;
+  const NuTileCoord tc(tile, tl);
+  const long long mxm = g.mx - 1, mym = g.my - 1, mzm = g.mz - 1;
+  const long long gx0 = (long long)tc.tx * tl.B - g.w, gy0 = (long long)tc.ty * tl.B - g.w,
+                  gz0 = (long long)tc.tz * tl.B - g.w;
+  for (int c = threadIdx.x; c < E3; c += kNuTileThreads) {
+    const int cx = c / E2, cy = (c / E) % E, cz = c % E;
+    cells[c] = grid[(((gx0 + cx) & mxm) * g.my + ((gy0 + cy) & mym)) * g.mz + ((gz0 + cz) & mzm)];
+  }
+  const NuLaneCells lc(T, lane);
+  int coff[kNuTileIters];
+#pragma unroll
+  for (int it = 0; it < kNuTileIters; ++it) coff[it] = lc.pyz[it] >= 0 ? (lc.pyz[it] >> 8) * E + (lc.pyz[it] & 255) : 0;
+  __syncthreads();
+  for (int q = start + wid; q < end; q += kNuTileWarps) {
+    const long long j = tl.idx[q];
+    for (int e = lane; e < 3 * T; e += 32) {  // all 3T axis weights over the 32 lanes
+      const int a = e / T;
+      wx[e] = nu_tile_weight(g, tl, tc, pos + 3 * j, a, e - a * T, nullptr);
+    }
+    const int l0x = nu_tile_centre(g, tl, tc, pos + 3 * j, 0);
+    const int l0y = nu_tile_centre(g, tl, tc, pos + 3 * j, 1);
+    const int l0z = nu_tile_centre(g, tl, tc, pos + 3 * j, 2);
+    __syncwarp();
+    double wyz[kNuTileIters];
+#pragma unroll
+    for (int it = 0; it < kNuTileIters; ++it)
+      wyz[it] = lc.pyz[it] >= 0 ? wy[lc.pyz[it] >> 8] * wz[lc.pyz[it] & 255] : 0.0;
+    double ax = 0.0, ay = 0.0;
+    const double2* plane = cells + l0x * E2 + l0y * E + l0z;
+    for (int px = 0; px < T; ++px, plane += E2) {
+      const double wxv = wx[px];
+#pragma unroll
+      for (int it = 0; it < kNuTileIters; ++it) {
+        if (lc.pyz[it] >= 0) {
+          const double wt = wxv * wyz[it];
+          const double2 c = plane[coff[it]];
+          ax += c.x * wt;
+          ay += c.y * wt;
         }
       }
     }
-    out[j] = acc;
+    for (int o = 16; o > 0; o >>= 1) {
+      ax += __shfl_xor_sync(0xffffffffu, ax, o);
+      ay += __shfl_xor_sync(0xffffffffu, ay, o);
+    }
+    if (lane == 0) out[j] = make_double2(ax, ay);
+    __syncwarp();
   }
 }
 
@@ -270,10 +576,15 @@ static NuGeom3 geom3(const NuLaunch3& L) {
   return NuGeom3{L.mx, L.my, L.mz, L.w, L.beta, L.i0b, L.lx, L.ly, L.lz};
 }
 
+static unsigned nu_warp_grid(long long npts) {
+  long long b = (npts + kNuWarps - 1) / kNuWarps;
+  return (unsigned)(b < 148 * 8 ? b : 148 * 8);
+}
+
 cudaError_t nufft3_spread_dev(const NuLaunch3& L, const double* pos, const void* val, long long npts, void* grid,
                               cudaStream_t st) {
   if (npts <= 0) return cudaSuccess;
-  nu_spread3<<<nu_grid(npts), 128, 0, st>>>(geom3(L), pos, static_cast<const double2*>(val), npts,
+  nu_spread3<<<nu_warp_grid(npts), 32 * kNuWarps, 0, st>>>(geom3(L), pos, static_cast<const double2*>(val), npts,
                                             static_cast<double2*>(grid));
   count_launch(1);
   return cudaGetLastError();
@@ -282,7 +593,7 @@ cudaError_t nufft3_spread_dev(const NuLaunch3& L, const double* pos, const void*
 cudaError_t nufft3_interp_dev(const NuLaunch3& L, const void* grid, const double* pos, long long npts, void* out,
                               cudaStream_t st) {
   if (npts <= 0) return cudaSuccess;
-  nu_interp3<<<nu_grid(npts), 128, 0, st>>>(geom3(L), static_cast<const double2*>(grid), pos, npts,
+  nu_interp3<<<nu_warp_grid(npts), 32 * kNuWarps, 0, st>>>(geom3(L), static_cast<const double2*>(grid), pos, npts,
                                             static_cast<double2*>(out));
   count_launch(1);
   return cudaGetLastError();
@@ -294,6 +605,48 @@ cudaError_t nufft3_modes_dev(const NuLaunch3& L, const double* dcx, const double
                                                          static_cast<const double2*>(src), static_cast<double2*>(dst),
                                                          to_grid ? 1 : 0);
   count_launch(1);
+  return cudaGetLastError();
+}
+
+int nufft3_tile_size(int w) {
+  if ((2 * w + 1) * (2 * w + 1) > 32 * kNuTileIters) return 0;  // more plane cells than a lane's list holds
+  for (int B : {8, 4})
+    if (nufft3_tile_smem(B, w) <= 220 * 1024) return B;
+  return 0;
+}
+
+size_t nufft3_tile_smem(int B, int w) {
+  const size_t E = (size_t)(B + 2 * w), T = (size_t)(2 * w + 1);
+  const size_t cells = E * E * E * sizeof(double2);
+  const size_t spread = cells + kNuChunk * 3 * T * sizeof(double) + kNuChunk * 3 * sizeof(int);
+  const size_t interp = cells + kNuTileWarps * 3 * T * sizeof(double);
+  return spread > interp ? spread : interp;
+}
+
+cudaError_t nufft3_tiled_dev(const NuLaunch3& L, const NuTileLaunch& TL, bool spread, const double* pos,
+                             const void* src, long long npts, void* dst, cudaStream_t st) {
+  if (npts <= 0) return cudaSuccess;
+  const NuGeom3 g = geom3(L);
+  const int ntiles = TL.ntx * TL.nty * TL.ntz;
+  cudaError_t e = cudaMemsetAsync(TL.cnt, 0, (size_t)ntiles * sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  nu3_bin<<<nu_grid(npts), 256, 0, st>>>(g, TL.B, TL.nty, TL.ntz, pos, npts, TL.cnt, TL.tile, TL.rank);
+  nu3_scan<<<1, 1024, 0, st>>>(TL.cnt, TL.off, ntiles);
+  nu3_scatter<<<nu_grid(npts), 256, 0, st>>>(TL.tile, TL.rank, TL.off, npts, TL.idx);
+  const NuTiles tl{TL.B, TL.B + 2 * L.w, TL.nty, TL.ntz, TL.off, TL.idx};
+  const size_t smem = nufft3_tile_smem(TL.B, L.w);
+  if (spread) {
+    e = kernel_smem_grant(reinterpret_cast<const void*>(nu3_spread_tiles), smem);
+    if (e != cudaSuccess) return e;
+    nu3_spread_tiles<<<ntiles, kNuTileThreads, smem, st>>>(g, tl, pos, static_cast<const double2*>(src),
+                                                           static_cast<double2*>(dst));
+  } else {
+    e = kernel_smem_grant(reinterpret_cast<const void*>(nu3_interp_tiles), smem);
+    if (e != cudaSuccess) return e;
+    nu3_interp_tiles<<<ntiles, kNuTileThreads, smem, st>>>(g, tl, static_cast<const double2*>(src), pos,
+                                                           static_cast<double2*>(dst));
+  }
+  count_launch(4);
   return cudaGetLastError();
 }
 

@@ -273,7 +273,7 @@ def main():
     ap.add_argument("--shape", default=None, help="override the 3D shape, e.g. 128,256,256 (profiling cases)")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
     ap.add_argument("--quick", action="store_true", help="headline only: no other shapes, e2e or CPU legs")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "stft", "czt", "nufft"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "stft", "czt", "nufft", "nufft3d"],
                     help="c2 (default) is the headline; c1/c3/c4/c5 print their own lines")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -668,6 +668,35 @@ def run_secondary(args):
         exact = np.exp(-2j * np.pi * np.outer(ks, pos_np)) @ val_np
         got = f.cpu().numpy()[np.arange(0, n, n // 64)]
         line["type1_rel_l2_vs_exact_sampled_bins"] = float(np.linalg.norm(got - exact) / np.linalg.norm(exact))
+    elif args.workload == "nufft3d":
+        # apollo-nufft NufftPlan3D at the reference defaults (sigma 2, width 6):
+        # 64^3 modes on the unit cube (oversampled 128^3), 2^18 uniform random
+        # points; type 1 then type 2 per step (f64)
+        from apollofft_b200.nufft import NufftPlan3D
+        nb, npts = 64, 1 << 18
+        rng = np.random.default_rng(14)
+        pos_np = rng.uniform(0.0, 1.0, (npts, 3))
+        val_np = rng.standard_normal(npts) + 1j * rng.standard_normal(npts)
+        pos = torch.from_numpy(pos_np).to(dev)
+        val = torch.from_numpy(val_np).to(dev)
+        plan = NufftPlan3D((nb, nb, nb), (1.0 / nb,) * 3)
+        f = torch.empty((nb, nb, nb), dtype=torch.complex128, device=dev)
+        back = torch.empty(npts, dtype=torch.complex128, device=dev)
+        t1 = _events_time(lambda: plan.type1(pos, val, out=f), args.steps, args.warmup, torch)
+        t2 = _events_time(lambda: plan.type2(f, pos, out=back), args.steps, args.warmup, torch)
+        t = t1 + t2
+        line.update({"metric": "points/s", "value": round(2 * npts / t, 1), "ms_per_step": round(t * 1e3, 4),
+                     "type1_ms": round(t1 * 1e3, 4), "type2_ms": round(t2 * 1e3, 4),
+                     "config": f"NUFFT 3D f64 type 1 + type 2: {nb}^3 modes, grid {plan.oversampled}, {npts} points, "
+                               "sigma 2, kernel width 6"})
+        # error of type 1 against the exact sum on 64 sampled modes
+        rs = np.random.default_rng(15)
+        idx = rs.integers(0, nb, (64, 3))
+        ks = np.where(idx <= nb // 2, idx, idx - nb)
+        exact = np.exp(-2j * np.pi * ks @ pos_np.T) @ val_np
+        fc = f.cpu().numpy()
+        got = fc[idx[:, 0], idx[:, 1], idx[:, 2]]
+        line["type1_rel_l2_vs_exact_sampled_modes"] = float(np.linalg.norm(got - exact) / np.linalg.norm(exact))
     print(json.dumps(line), flush=True)
     return 0
 

@@ -86,7 +86,10 @@ def exact2(modes, pos, shape, L):
 CASES = [((4, 4, 4), (0.1, 0.1, 0.1), 2, 6, 3),
          ((8, 6, 5), (0.25, 0.5, 0.2), 2, 6, 150),
          ((16, 12, 10), (1.0, 0.1, 0.3), 2, 4, 300),
-         ((3, 2, 2), (0.5, 0.75, 1.0), 3, 6, 40)]
+         ((3, 2, 2), (0.5, 0.75, 1.0), 3, 6, 40),
+         ((16, 16, 16), (0.0625, 0.0625, 0.0625), 2, 6, 2000),   # shared-memory tiles, B = 8
+         ((6, 5, 4), (1.0, 1.0, 1.0), 2, 8, 60),                 # B = 4 tiles
+         ((4, 4, 4), (1.0, 1.0, 1.0), 2, 10, 30)]                # too wide for a tile: per-point kernels
 
 
 @pytest.mark.parametrize("shape,spacing,sigma,w,npts", CASES)
@@ -150,3 +153,23 @@ def test_nufft3d_empty_and_validation(afc, cuda):
                 dict(shape=(2, 2, 2), spacing=(1, 1, 1), kernel_width=40)]:
         with pytest.raises(ValueError):
             NufftPlan3D(**bad)
+
+
+def test_nufft3d_growing_and_clustered_points(afc, oracle, cuda):
+    """Point buffers grow between calls; every point in one tile; repeat calls agree."""
+    from apollofft_b200.nufft import NufftPlan3D
+    shape, spacing = (8, 8, 8), (0.125, 0.125, 0.125)
+    ref = RefPlan3(shape, spacing, 2, 6)
+    plan = NufftPlan3D(shape, spacing)
+    rng = np.random.default_rng(5)
+    for npts, spread in [(10, 1.0), (400, 1.0), (300, 0.01), (600, 1.0)]:
+        pos = rng.uniform(0.0, spread, (npts, 3))
+        val = rng.standard_normal(npts) + 1j * rng.standard_normal(npts)
+        p_t = torch.from_numpy(pos).cuda()
+        y1 = plan.type1(p_t, torch.from_numpy(val).cuda()).cpu().numpy()
+        assert rel_l2(y1, ref.type1(pos, val, oracle)) < 1e-12
+        y1b = plan.type1(p_t, torch.from_numpy(val).cuda()).cpu().numpy()
+        assert rel_l2(y1b, y1) < 1e-14
+        modes = torch.from_numpy(np.ascontiguousarray(y1)).cuda()
+        y2 = plan.type2(modes, p_t).cpu().numpy()
+        assert rel_l2(y2, ref.type2(y1, pos, oracle)) < 1e-12
