@@ -668,6 +668,17 @@ def run_secondary(args):
         exact = np.exp(-2j * np.pi * np.outer(ks, pos_np)) @ val_np
         got = f.cpu().numpy()[np.arange(0, n, n // 64)]
         line["type1_rel_l2_vs_exact_sampled_bins"] = float(np.linalg.norm(got - exact) / np.linalg.norm(exact))
+        # the reference's algorithm restated (numpy spreading + oracle FFT) on a bounded sample
+        from oracle import nufft as ON, oracle as O
+        sub = 8192
+        ref = ON.RefPlan(n, dx, 2, 6)
+        t0 = time.perf_counter()
+        fr = ref.type1(pos_np[:sub], val_np[:sub])
+        ref.type2(fr, pos_np[:sub])
+        tc = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(2 * sub / tc, 1), "unit": "points/s", "cores": O.max_threads(),
+                                "kind": "port", "sample": f"type 1 + type 2 of the first {sub} points, same plan "
+                                "(spreading one thread in numpy, oracle FFT on all threads)"}
     elif args.workload == "nufft3d":
         # apollo-nufft NufftPlan3D at the reference defaults (sigma 2, width 6):
         # 64^3 modes on the unit cube (oversampled 128^3), 2^18 uniform random
@@ -697,6 +708,16 @@ def run_secondary(args):
         fc = f.cpu().numpy()
         got = fc[idx[:, 0], idx[:, 1], idx[:, 2]]
         line["type1_rel_l2_vs_exact_sampled_modes"] = float(np.linalg.norm(got - exact) / np.linalg.norm(exact))
+        from oracle import nufft as ON, oracle as O
+        sub = 2048
+        ref = ON.RefPlan3((nb, nb, nb), (1.0 / nb,) * 3, 2, 6)
+        t0 = time.perf_counter()
+        fr = ref.type1(pos_np[:sub], val_np[:sub])
+        ref.type2(fr, pos_np[:sub])
+        tc = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(2 * sub / tc, 1), "unit": "points/s", "cores": O.max_threads(),
+                                "kind": "port", "sample": f"type 1 + type 2 of the first {sub} points, same plan "
+                                "(spreading one thread in numpy, oracle 3D FFT on all threads)"}
     print(json.dumps(line), flush=True)
     return 0
 

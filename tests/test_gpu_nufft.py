@@ -1,102 +1,16 @@
 """Device 1D NUFFT (afc_nufft1d_*) against the reference's algorithm restated in
-numpy (transform/dimension_1d.rs:156-272: Kaiser-Bessel spreading with the
-power-series I0 of kaiser_bessel.rs:55-116, the oracle's FFT, deconvolution by
-the kernel's Fourier transform) and against the exact sums of
-verification/mod.rs:97-98 within the reference's own accuracy bound."""
-import math
-
+numpy (oracle/nufft.py: transform/dimension_1d.rs:156-272, Kaiser-Bessel
+spreading with the power-series I0 of kaiser_bessel.rs:55-116, the oracle's
+FFT, deconvolution by the kernel's Fourier transform) and against the exact
+sums of verification/mod.rs:97-98 within the reference's own accuracy bound."""
 import numpy as np
 import pytest
 import torch
 
 from conftest import rel_l2
+from oracle.nufft import RefPlan, exact1_1d as exact1, exact2_1d as exact2
 
 pytestmark = pytest.mark.gpu
-
-
-def i0(z):
-    scaled = 0.25 * z * z
-    s, term = 1.0, 1.0
-    for k in range(1, 257):
-        term *= scaled / (k * k)
-        s += term
-        if term <= np.finfo(float).eps * s:
-            break
-    return s
-
-
-def kb(x, w, beta, i0b):
-    u2 = (x / w) ** 2
-    return 0.0 if u2 >= 1.0 else i0(beta * math.sqrt(1.0 - u2)) / i0b
-
-
-def kb_ft(xi, w, beta, i0b):
-    t = 2.0 * math.pi * w * xi
-    z2 = beta * beta - t * t
-    pre = 2.0 * w / i0b
-    if abs(z2) < 1e-30:
-        return pre
-    if z2 > 0:
-        s = math.sqrt(z2)
-        return pre * math.sinh(s) / s
-    s = math.sqrt(-z2)
-    return pre * math.sin(s) / s
-
-
-def signed(k, n):
-    return k if k <= n // 2 else k - n
-
-
-class RefPlan:
-    def __init__(self, n, dx, sigma, w):
-        self.n, self.dx, self.m, self.w = n, dx, sigma * n, w
-        self.beta = math.pi * (1.0 - 1.0 / (2.0 * sigma)) * (2 * w)
-        self.i0b = i0(self.beta)
-        self.deconv = np.array([1.0 / kb_ft(signed(k, n) / self.m, w, self.beta, self.i0b) for k in range(n)])
-        self.L = n * dx
-
-    def place(self, x):
-        r = math.fmod(x, self.L)
-        if r < 0:
-            r += self.L
-        t = self.m * r / self.L
-        m0 = math.floor(t + 0.5) if t >= 0 else math.ceil(t - 0.5)
-        return int(m0), t - m0
-
-    def type1(self, pos, val, oracle):
-        grid = np.zeros(self.m, dtype=np.complex128)
-        for x, v in zip(pos, val):
-            m0, d = self.place(x)
-            for p in range(-self.w, self.w + 1):
-                wt = kb(p - d, self.w, self.beta, self.i0b)
-                if wt != 0.0:
-                    grid[(m0 + p) % self.m] += v * wt
-        spec = oracle.fft1d(grid)
-        return np.array([spec[signed(k, self.n) % self.m] * self.deconv[k] for k in range(self.n)])
-
-    def type2(self, coeffs, pos, oracle):
-        grid = np.zeros(self.m, dtype=np.complex128)
-        for k in range(self.n):
-            grid[signed(k, self.n) % self.m] = coeffs[k] * self.deconv[k]
-        grid = oracle.fft1d(grid, inverse=True) * self.m
-        out = np.zeros(len(pos), dtype=np.complex128)
-        for j, x in enumerate(pos):
-            m0, d = self.place(x)
-            for p in range(-self.w, self.w + 1):
-                wt = kb(p - d, self.w, self.beta, self.i0b)
-                if wt != 0.0:
-                    out[j] += grid[(m0 + p) % self.m] * wt
-        return out
-
-
-def exact1(pos, val, n, L):
-    ks = np.array([signed(k, n) for k in range(n)])
-    return np.exp(-2j * np.pi * np.outer(ks, pos) / L) @ val
-
-
-def exact2(coeffs, pos, n, L):
-    ks = np.array([signed(k, n) for k in range(n)])
-    return np.exp(2j * np.pi * np.outer(pos, ks) / L) @ coeffs
 
 
 @pytest.mark.parametrize("n,dx,sigma,w,npts", [(32, 0.25, 2, 6, 200), (64, 0.05, 2, 4, 300), (128, 1.0, 3, 6, 500),

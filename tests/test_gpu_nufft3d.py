@@ -1,86 +1,18 @@
 """Device 3D NUFFT (afc_nufft3d_*) against the reference's algorithm restated in
-numpy (transform/dimension_3d.rs:256-330 and 496-603: per-axis oversampled
+numpy (oracle/nufft.py: transform/dimension_3d.rs:256-330 and 496-603: per-axis oversampled
 length next_pow2(max(sigma n, 2w + 1)), separable Kaiser-Bessel weights over
 (2w + 1)^3 cells, the oracle's 3D FFT, per-axis deconvolution; type 2 through
 the normalized inverse passes) and against the exact sums of
 dimension_3d.rs:679-739 within the reference's own bound (fast_3d_tracks_exact:
 max error / max magnitude < 1e-6)."""
-import math
-
 import numpy as np
 import pytest
 import torch
 
 from conftest import rel_l2
-from test_gpu_nufft import i0, kb, kb_ft, signed
+from oracle.nufft import RefPlan3, exact1_3d as exact1, exact2_3d as exact2
 
 pytestmark = pytest.mark.gpu
-
-
-def over_len(n, sigma, w):
-    lower = max(n * sigma, 2 * w + 1)
-    m = 1
-    while m < lower:
-        m <<= 1
-    return m
-
-
-class RefPlan3:
-    def __init__(self, shape, spacing, sigma, w):
-        self.n = shape
-        self.L = [n * d for n, d in zip(shape, spacing)]
-        self.m = [over_len(n, sigma, w) for n in shape]
-        self.w = w
-        self.beta = math.pi * (1.0 - 1.0 / (2.0 * sigma)) * (2 * w)
-        self.i0b = i0(self.beta)
-        self.deconv = [np.array([1.0 / kb_ft(signed(k, n) / m, w, self.beta, self.i0b) for k in range(n)])
-                       for n, m in zip(shape, self.m)]
-        self.bins = [np.array([signed(k, n) % m for k in range(n)]) for n, m in zip(shape, self.m)]
-
-    def taps(self, x, a):
-        r = math.fmod(x, self.L[a])
-        if r < 0:
-            r += self.L[a]
-        t = self.m[a] * r / self.L[a]
-        m0 = math.floor(t + 0.5) if t >= 0 else math.ceil(t - 0.5)
-        d = t - m0
-        idx = np.array([(m0 + p) % self.m[a] for p in range(-self.w, self.w + 1)])
-        wt = np.array([kb(p - d, self.w, self.beta, self.i0b) for p in range(-self.w, self.w + 1)])
-        return idx, wt
-
-    def dec(self):
-        return self.deconv[0][:, None, None] * self.deconv[1][None, :, None] * self.deconv[2][None, None, :]
-
-    def type1(self, pos, val, oracle):
-        grid = np.zeros(self.m, dtype=np.complex128)
-        for (x, y, z), v in zip(pos, val):
-            (ix, wx), (iy, wy), (iz, wz) = self.taps(x, 0), self.taps(y, 1), self.taps(z, 2)
-            grid[np.ix_(ix, iy, iz)] += v * (wx[:, None, None] * wy[None, :, None] * wz[None, None, :])
-        spec = oracle.fft3d(grid)
-        return spec[np.ix_(*self.bins)] * self.dec()
-
-    def type2(self, modes, pos, oracle):
-        grid = np.zeros(self.m, dtype=np.complex128)
-        grid[np.ix_(*self.bins)] = modes * self.dec()
-        grid = oracle.fft3d(grid, inverse=True)  # normalized, as the reference's axis passes
-        out = np.zeros(len(pos), dtype=np.complex128)
-        for j, (x, y, z) in enumerate(pos):
-            (ix, wx), (iy, wy), (iz, wz) = self.taps(x, 0), self.taps(y, 1), self.taps(z, 2)
-            out[j] = np.sum(grid[np.ix_(ix, iy, iz)] * (wx[:, None, None] * wy[None, :, None] * wz[None, None, :]))
-        return out
-
-
-def kgrid(shape, L):
-    ks = [np.array([signed(k, n) for k in range(n)]) / l for n, l in zip(shape, L)]
-    return np.stack(np.meshgrid(*ks, indexing="ij"), -1).reshape(-1, 3)
-
-
-def exact1(pos, val, shape, L):
-    return (np.exp(-2j * np.pi * kgrid(shape, L) @ pos.T) @ val).reshape(shape)
-
-
-def exact2(modes, pos, shape, L):
-    return np.exp(2j * np.pi * pos @ kgrid(shape, L).T) @ modes.reshape(-1)
 
 
 CASES = [((4, 4, 4), (0.1, 0.1, 0.1), 2, 6, 3),

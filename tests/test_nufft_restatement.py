@@ -1,4 +1,4 @@
-"""Pins the NUFFT restatements the device tests compare against (1D:
+"""Pins the NUFFT restatements of oracle/nufft.py, which the device tests compare against (1D:
 transform/dimension_1d.rs, 3D: transform/dimension_3d.rs) on the CPU: the
 reference's own known answers (DC mode = sum of values, type 2 at the origin =
 sum of modes) and its accuracy bound against the exact sums
@@ -7,8 +7,7 @@ import numpy as np
 import pytest
 
 from conftest import rel_l2
-from test_gpu_nufft import RefPlan, exact1 as exact1_1d, exact2 as exact2_1d
-from test_gpu_nufft3d import RefPlan3, exact1, exact2
+from oracle.nufft import RefPlan, RefPlan3, exact1_1d, exact2_1d, exact1_3d as exact1, exact2_3d as exact2
 
 
 def test_restatement_1d_tracks_exact(oracle):
