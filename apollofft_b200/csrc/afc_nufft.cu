@@ -397,9 +397,6 @@ __global__ void __launch_bounds__(kNuTileThreads) nu3_spread_tiles(NuGeom3 g, Nu
   const NuTileCoord tc(tile, tl);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const NuLaneCells lc(T, lane);
-  int coff[kNuTileIters];
-#pragma unroll
-  for (int it = 0; it < kNuTileIters; ++it) coff[it] = lc.pyz[it] >= 0 ? (lc.pyz[it] >> 8) * E + (lc.pyz[it] & 255) : 0;
   for (int base = start; base < end; base += kNuChunk) {
     const int cnt = min(kNuChunk, end - base);
     __syncthreads();  // zeroing done / previous chunk's weights consumed
@@ -421,15 +418,27 @@ __global__ void __launch_bounds__(kNuTileThreads) nu3_spread_tiles(NuGeom3 g, Nu
       for (; px < T; px += kNuTileWarps) {
         const double wxv = wx[px];
         double2* plane = acc + (lx0 + px) * E2 + ly0 * E + lz0;
+        // six of the lane's cells at a time: all loads first, then the adds and
+        // stores (the lane's cells are distinct, and so are different lanes'),
+        // so six shared-memory loads are in flight instead of one
 #pragma unroll
-        for (int it = 0; it < kNuTileIters; ++it) {
-          if (lc.pyz[it] >= 0) {
-            const double wt = wxv * wy[lc.pyz[it] >> 8] * wz[lc.pyz[it] & 255];
-            double2* c = plane + coff[it];
-            double2 o = *c;
-            o.x += v.x * wt;
-            o.y += v.y * wt;
-            *c = o;
+        for (int h = 0; h < kNuTileIters; h += 6) {
+          if (h * 32 >= T * T) break;
+          double2 cv[6];
+#pragma unroll
+          for (int i = 0; i < 6; ++i) {
+            const int f = lc.pyz[h + i];
+            if (f >= 0) cv[i] = plane[(f >> 8) * E + (f & 255)];
+          }
+#pragma unroll
+          for (int i = 0; i < 6; ++i) {
+            const int f = lc.pyz[h + i];
+            if (f >= 0) {
+              const double wt = wxv * wy[f >> 8] * wz[f & 255];
+              cv[i].x += v.x * wt;
+              cv[i].y += v.y * wt;
+              plane[(f >> 8) * E + (f & 255)] = cv[i];
+            }
           }
         }
       }
