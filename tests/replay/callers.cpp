@@ -16,6 +16,18 @@
 //     length-n DFT, which the oracle computes directly.
 //   * apollo-nufft NufftPlan1D (transform/dimension_1d.rs:110-150): one plan of
 //     the oversampled length sigma * n, forward and inverse on the spread grid.
+//   * apollo-dctdst dct2_dst2_fast / dct3_fast / dst3_fast
+//     (infrastructure/kernel/fast.rs:144-345): one 2N-point fft_1d_complex of
+//     the zero-padded signal for DCT-II and DST-II, a 2N-point normalized
+//     ifft_1d_complex of the Hermitian pre-twiddled spectrum for DCT-III, a
+//     2N-point forward FFT of the pre-twiddled signal for DST-III; checked
+//     against the definitions summed in long double.
+//   * apollo-dht   dht_fast_with_scratch (infrastructure/kernel/fast.rs:10-27):
+//     H_k = Re X_k - Im X_k of one forward FFT; checked against the cas sum.
+//   * apollo-hilbert analytic_signal_into (infrastructure/kernel/direct.rs:85-106):
+//     forward, the analytic mask (1 at DC and Nyquist, 2 on positive bins, 0 on
+//     negative), normalized inverse, real part reset to the input; checked
+//     against the same steps on the oracle.
 // A device-resident batch of all STFT frames (one afc_execute over `frames`
 // lanes) is checked too: the fused form a caller moves to.
 //
@@ -184,11 +196,141 @@ static void replay_nufft() {
   }
 }
 
+// cos / sin of 2 pi m / period in long double, m reduced mod period first
+static long double cos_frac(long long m, long long period) {
+  return std::cos(2.0L * 3.141592653589793238462643383279502884L * (long double)(m % period) / (long double)period);
+}
+static long double sin_frac(long long m, long long period) {
+  return std::sin(2.0L * 3.141592653589793238462643383279502884L * (long double)(m % period) / (long double)period);
+}
+
+static double rel_l2_real(const std::vector<double>& a, const std::vector<long double>& b) {
+  long double num = 0, den = 0;
+  for (size_t i = 0; i < a.size(); ++i) {
+    num += ((long double)a[i] - b[i]) * ((long double)a[i] - b[i]);
+    den += b[i] * b[i];
+  }
+  return (double)std::sqrt(num / den);
+}
+
+static void replay_dctdst() {
+  const long long n = 1000, two_n = 2 * n;
+  std::mt19937_64 rng(17);
+  std::normal_distribution<double> nd;
+  std::vector<double> x(n);
+  for (auto& v : x) v = nd(rng);
+  const double half_cycle = M_PI / (double)two_n;
+  CudaPlan1D plan(two_n);
+  // DCT-II and DST-II from one forward FFT of the zero-padded signal
+  std::vector<C> f(two_n);
+  for (long long i = 0; i < n; ++i) f[i] = C(x[i], 0.0);
+  plan.forward_complex_slice_inplace(f.data(), f.size());
+  std::vector<double> dct2(n), dst2(n);
+  for (long long k = 0; k < n; ++k) {
+    dct2[k] = (std::polar(1.0, -half_cycle * (double)k) * f[k]).real();
+    dst2[k] = -(std::polar(1.0, -half_cycle * (double)(k + 1)) * f[k + 1]).imag();
+  }
+  std::vector<long double> dct2_ref(n, 0.0L), dst2_ref(n, 0.0L);
+  for (long long k = 0; k < n; ++k)
+    for (long long i = 0; i < n; ++i) {
+      dct2_ref[k] += (long double)x[i] * cos_frac((2 * i + 1) * k, 2 * two_n);
+      dst2_ref[k] += (long double)x[i] * sin_frac((2 * i + 1) * (k + 1), 2 * two_n);
+    }
+  expect("dctdst: DCT-II via 2N forward (n = 1000)", rel_l2_real(dct2, dct2_ref));
+  expect("dctdst: DST-II via 2N forward (n = 1000)", rel_l2_real(dst2, dst2_ref));
+  // DCT-III: Hermitian pre-twiddled spectrum, normalized 2N inverse, N Re(y)
+  std::vector<C> g(two_n);
+  g[0] = C(x[0], 0.0);
+  for (long long k = 1; k < n; ++k) g[k] = C(x[k], 0.0) * std::polar(1.0, half_cycle * (double)k);
+  for (long long k = 1; k < n; ++k) g[two_n - k] = std::conj(g[k]);
+  plan.inverse_complex_slice_inplace(g.data(), g.size());
+  std::vector<double> dct3(n);
+  for (long long i = 0; i < n; ++i) dct3[i] = (double)n * g[i].real();
+  std::vector<long double> dct3_ref(n);
+  for (long long i = 0; i < n; ++i) {
+    long double acc = 0.5L * x[0];
+    for (long long k = 1; k < n; ++k) acc += (long double)x[k] * cos_frac((2 * i + 1) * k, 2 * two_n);
+    dct3_ref[i] = acc;
+  }
+  expect("dctdst: DCT-III via 2N normalized inverse", rel_l2_real(dct3, dct3_ref));
+  // DST-III: pre-twiddled signal with the half boundary term, 2N forward
+  std::vector<C> v(two_n);
+  for (long long i = 0; i < n; ++i)
+    v[i] = C(i < n - 1 ? x[i] : 0.5 * x[i], 0.0) * std::polar(1.0, -half_cycle * (double)i);
+  plan.forward_complex_slice_inplace(v.data(), v.size());
+  std::vector<double> dst3(n);
+  for (long long k = 0; k < n; ++k)
+    dst3[k] = (std::polar(1.0, half_cycle * (double)(2 * k + 1)) * std::conj(v[k])).imag();
+  std::vector<long double> dst3_ref(n);
+  for (long long k = 0; k < n; ++k) {
+    long double acc = (k % 2 ? -0.5L : 0.5L) * x[n - 1];
+    for (long long i = 0; i + 1 < n; ++i) acc += (long double)x[i] * sin_frac((i + 1) * (2 * k + 1), 2 * two_n);
+    dst3_ref[k] = acc;
+  }
+  expect("dctdst: DST-III via 2N forward", rel_l2_real(dst3, dst3_ref));
+}
+
+static void replay_dht() {
+  for (long long n : {1000LL, 1009LL, 4096LL}) {
+    std::mt19937_64 rng(19 + n);
+    std::normal_distribution<double> nd;
+    std::vector<double> x(n);
+    for (auto& v : x) v = nd(rng);
+    CudaPlan1D plan(n);
+    std::vector<C> scratch(n);
+    for (long long i = 0; i < n; ++i) scratch[i] = C(x[i], 0.0);
+    plan.forward_complex_slice_inplace(scratch.data(), scratch.size());
+    std::vector<double> h(n);
+    for (long long k = 0; k < n; ++k) h[k] = scratch[k].real() - scratch[k].imag();
+    std::vector<long double> ref(n, 0.0L);
+    for (long long k = 0; k < n; ++k)
+      for (long long i = 0; i < n; ++i) ref[k] += (long double)x[i] * (cos_frac(k * i, n) + sin_frac(k * i, n));
+    char what[64];
+    std::snprintf(what, sizeof what, "dht: Re X - Im X (n = %lld)", n);
+    expect(what, rel_l2_real(h, ref));
+  }
+}
+
+static void analytic_mask(std::vector<C>& s) {
+  const size_t len = s.size(), positive_end = (len + 1) / 2;
+  for (size_t k = 0; k < len; ++k) {
+    const double scale = (k == 0 || (len % 2 == 0 && k == len / 2)) ? 1.0 : (k < positive_end ? 2.0 : 0.0);
+    s[k] *= scale;
+  }
+}
+
+static void replay_hilbert() {
+  for (long long n : {1000LL, 1001LL}) {
+    std::mt19937_64 rng(23 + n);
+    std::normal_distribution<double> nd;
+    std::vector<double> x(n);
+    for (auto& v : x) v = nd(rng);
+    CudaPlan1D plan(n);
+    std::vector<C> a(n);
+    for (long long i = 0; i < n; ++i) a[i] = C(x[i], 0.0);
+    std::vector<C> ref = a;
+    plan.forward_complex_slice_inplace(a.data(), a.size());
+    analytic_mask(a);
+    plan.inverse_complex_slice_inplace(a.data(), a.size());
+    for (long long i = 0; i < n; ++i) a[i] = C(x[i], a[i].imag());
+    ref = oracle_fft(ref, false);
+    analytic_mask(ref);
+    ref = oracle_fft(ref, true);
+    for (long long i = 0; i < n; ++i) ref[i] = C(x[i], ref[i].imag());
+    char what[64];
+    std::snprintf(what, sizeof what, "hilbert: analytic signal (n = %lld)", n);
+    expect(what, rel_l2(a, ref));
+  }
+}
+
 int main() {
   try {
     replay_stft();
     replay_czt();
     replay_nufft();
+    replay_dctdst();
+    replay_dht();
+    replay_hilbert();
   } catch (const std::exception& e) {
     std::fprintf(stderr, "error: %s\n", e.what());
     return 2;

@@ -1,6 +1,8 @@
 """Caller call patterns (apollo-stft frames, apollo-czt Bluestein workspace,
-apollo-nufft oversampled grid) replayed by a C++ program through the C ABI and
-checked against the oracle; see tests/replay/callers.cpp."""
+apollo-nufft oversampled grid, apollo-dctdst 2N-point DCT/DST, apollo-dht,
+apollo-hilbert analytic signal) replayed by a C++ program through the C ABI
+and checked against the oracle or the definitions; see
+tests/replay/callers.cpp."""
 import os
 import subprocess
 
