@@ -273,8 +273,9 @@ __global__ void __launch_bounds__(32 * kNuWarps) nu_interp3(NuGeom3 g, const dou
 // with plain shared-memory read-modify-writes (no two warps share a cell),
 // then the CTA adds its E^3 cells to the grid with coalesced atomics (tiles'
 // halos overlap); grid atomics drop from (2w+1)^3 per point to E^3 per tile.
-// Interpolation: the CTA loads its E^3 cells once, one warp per point gathers
-// from shared memory.
+// Interpolation: the CTA loads its E^3 cells once, stages the weights of 32
+// points at a time with all its threads, and one warp per point gathers from
+// shared memory.
 constexpr int kNuTileThreads = 512;
 constexpr int kNuTileWarps = kNuTileThreads / 32;
 constexpr int kNuChunk = 32;  // points whose weights the spreading CTA stages at once
@@ -468,10 +469,9 @@ __global__ void __launch_bounds__(kNuTileThreads) nu3_interp_tiles(NuGeom3 g, Nu
   if (start == end) return;
   const int T = 2 * g.w + 1, E = tl.E, E2 = E * E, E3 = E2 * E;
   double2* cells = reinterpret_cast<double2*>(nu_smem);
+  double* wts = reinterpret_cast<double*>(cells + E3);       // kNuChunk x 3 x T
+  int* loc = reinterpret_cast<int*>(wts + kNuChunk * 3 * T);  // kNuChunk x 3
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double* wx = reinterpret_cast<double*>(cells + E3) + wid * 3 * T;
-  double* wy = wx + T;
-  double* wz = wy + T;
   const NuTileCoord tc(tile, tl);
   const long long mxm = g.mx - 1, mym = g.my - 1, mzm = g.mz - 1;
   const long long gx0 = (long long)tc.tx * tl.B - g.w, gy0 = (long long)tc.ty * tl.B - g.w,
@@ -484,41 +484,44 @@ __global__ void __launch_bounds__(kNuTileThreads) nu3_interp_tiles(NuGeom3 g, Nu
   int coff[kNuTileIters];
 #pragma unroll
   for (int it = 0; it < kNuTileIters; ++it) coff[it] = lc.pyz[it] >= 0 ? (lc.pyz[it] >> 8) * E + (lc.pyz[it] & 255) : 0;
-  __syncthreads();
-  for (int q = start + wid; q < end; q += kNuTileWarps) {
-    const long long j = tl.idx[q];
-    for (int e = lane; e < 3 * T; e += 32) {  // all 3T axis weights over the 32 lanes
-      const int a = e / T;
-      wx[e] = nu_tile_weight(g, tl, tc, pos + 3 * j, a, e - a * T, nullptr);
+  for (int base = start; base < end; base += kNuChunk) {
+    const int cnt = min(kNuChunk, end - base);
+    __syncthreads();  // cells loaded / previous chunk's weights consumed
+    // the chunk's 3T axis weights per point over all threads of the CTA
+    for (int e = threadIdx.x; e < cnt * 3 * T; e += kNuTileThreads) {
+      const int p = e / (3 * T), r = e - p * 3 * T, a = r / T, tap = r - a * T;
+      const long long j = tl.idx[base + p];
+      wts[e] = nu_tile_weight(g, tl, tc, pos + 3 * j, a, tap, tap == 0 ? &loc[p * 3 + a] : nullptr);
     }
-    const int l0x = nu_tile_centre(g, tl, tc, pos + 3 * j, 0);
-    const int l0y = nu_tile_centre(g, tl, tc, pos + 3 * j, 1);
-    const int l0z = nu_tile_centre(g, tl, tc, pos + 3 * j, 2);
-    __syncwarp();
-    double wyz[kNuTileIters];
+    __syncthreads();
+    for (int p = wid; p < cnt; p += kNuTileWarps) {
+      const double* wx = wts + p * 3 * T;
+      const double* wy = wx + T;
+      const double* wz = wy + T;
+      double wyz[kNuTileIters];
 #pragma unroll
-    for (int it = 0; it < kNuTileIters; ++it)
-      wyz[it] = lc.pyz[it] >= 0 ? wy[lc.pyz[it] >> 8] * wz[lc.pyz[it] & 255] : 0.0;
-    double ax = 0.0, ay = 0.0;
-    const double2* plane = cells + l0x * E2 + l0y * E + l0z;
-    for (int px = 0; px < T; ++px, plane += E2) {
-      const double wxv = wx[px];
+      for (int it = 0; it < kNuTileIters; ++it)
+        wyz[it] = lc.pyz[it] >= 0 ? wy[lc.pyz[it] >> 8] * wz[lc.pyz[it] & 255] : 0.0;
+      double ax = 0.0, ay = 0.0;
+      const double2* plane = cells + loc[p * 3] * E2 + loc[p * 3 + 1] * E + loc[p * 3 + 2];
+      for (int px = 0; px < T; ++px, plane += E2) {
+        const double wxv = wx[px];
 #pragma unroll
-      for (int it = 0; it < kNuTileIters; ++it) {
-        if (lc.pyz[it] >= 0) {
-          const double wt = wxv * wyz[it];
-          const double2 c = plane[coff[it]];
-          ax += c.x * wt;
-          ay += c.y * wt;
+        for (int it = 0; it < kNuTileIters; ++it) {
+          if (lc.pyz[it] >= 0) {
+            const double wt = wxv * wyz[it];
+            const double2 c = plane[coff[it]];
+            ax += c.x * wt;
+            ay += c.y * wt;
+          }
         }
       }
+      for (int o = 16; o > 0; o >>= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+      }
+      if (lane == 0) out[tl.idx[base + p]] = make_double2(ax, ay);
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      ax += __shfl_xor_sync(0xffffffffu, ax, o);
-      ay += __shfl_xor_sync(0xffffffffu, ay, o);
-    }
-    if (lane == 0) out[j] = make_double2(ax, ay);
-    __syncwarp();
   }
 }
 
@@ -627,9 +630,8 @@ int nufft3_tile_size(int w) {
 size_t nufft3_tile_smem(int B, int w) {
   const size_t E = (size_t)(B + 2 * w), T = (size_t)(2 * w + 1);
   const size_t cells = E * E * E * sizeof(double2);
-  const size_t spread = cells + kNuChunk * 3 * T * sizeof(double) + kNuChunk * 3 * sizeof(int);
-  const size_t interp = cells + kNuTileWarps * 3 * T * sizeof(double);
-  return spread > interp ? spread : interp;
+  // both kernels stage the axis weights and centre cells of kNuChunk points
+  return cells + kNuChunk * 3 * T * sizeof(double) + kNuChunk * 3 * sizeof(int);
 }
 
 cudaError_t nufft3_tiled_dev(const NuLaunch3& L, const NuTileLaunch& TL, bool spread, const double* pos,
