@@ -273,12 +273,12 @@ __global__ void __launch_bounds__(32 * kNuWarps) nu_interp3(NuGeom3 g, const dou
 // with plain shared-memory read-modify-writes (no two warps share a cell),
 // then the CTA adds its E^3 cells to the grid with coalesced atomics (tiles'
 // halos overlap); grid atomics drop from (2w+1)^3 per point to E^3 per tile.
-// Interpolation: the CTA loads its E^3 cells once, stages the weights of 32
+// Interpolation: the CTA loads its E^3 cells once, stages the weights of 64
 // points at a time with all its threads, and one warp per point gathers from
 // shared memory.
 constexpr int kNuTileThreads = 512;
 constexpr int kNuTileWarps = kNuTileThreads / 32;
-constexpr int kNuChunk = 32;  // points whose weights the spreading CTA stages at once
+constexpr int kNuChunk = 64;  // points whose weights a tile CTA stages at once
 
 struct NuTiles {
   int B, E, nty, ntz;
@@ -502,7 +502,8 @@ __global__ void __launch_bounds__(kNuTileThreads) nu3_interp_tiles(NuGeom3 g, Nu
 #pragma unroll
       for (int it = 0; it < kNuTileIters; ++it)
         wyz[it] = lc.pyz[it] >= 0 ? wy[lc.pyz[it] >> 8] * wz[lc.pyz[it] & 255] : 0.0;
-      double ax = 0.0, ay = 0.0;
+      // two accumulator pairs (even / odd cells) halve the dependent FMA chain
+      double ax0 = 0.0, ay0 = 0.0, ax1 = 0.0, ay1 = 0.0;
       const double2* plane = cells + loc[p * 3] * E2 + loc[p * 3 + 1] * E + loc[p * 3 + 2];
       for (int px = 0; px < T; ++px, plane += E2) {
         const double wxv = wx[px];
@@ -511,11 +512,17 @@ __global__ void __launch_bounds__(kNuTileThreads) nu3_interp_tiles(NuGeom3 g, Nu
           if (lc.pyz[it] >= 0) {
             const double wt = wxv * wyz[it];
             const double2 c = plane[coff[it]];
-            ax += c.x * wt;
-            ay += c.y * wt;
+            if (it & 1) {
+              ax1 += c.x * wt;
+              ay1 += c.y * wt;
+            } else {
+              ax0 += c.x * wt;
+              ay0 += c.y * wt;
+            }
           }
         }
       }
+      double ax = ax0 + ax1, ay = ay0 + ay1;
       for (int o = 16; o > 0; o >>= 1) {
         ax += __shfl_xor_sync(0xffffffffu, ax, o);
         ay += __shfl_xor_sync(0xffffffffu, ay, o);
