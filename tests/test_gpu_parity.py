@@ -1,6 +1,6 @@
 """CUDA kernels vs the f64 oracle (the reference's high_accuracy plan restated).
 
-Bars (stated in the north star): f64 relative L2 <= 1e-12, f32 <= 1e-5 against
+Bars: f64 relative L2 <= 1e-12, f32 <= 1e-5 against
 the f64 oracle on the same seeded inputs.  Integer maps are checked bit-exactly
 in test_oracle_integer.py."""
 import os

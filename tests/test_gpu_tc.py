@@ -3,7 +3,7 @@
 * one tensor-core tile D = A B^T with hi/lo operands against numpy (checks the
   UMMA descriptors and the TMEM read-back);
 * 16^s-point transforms against the exact DFT, per row: FP16 split <= 1e-5
-  relative L2 (the north-star bar), BF16 split measured and bounded;
+  relative L2 (the accuracy bar of the split forms), BF16 split measured and bounded;
 * high-dynamic-range rows (scaled by 10^k, k in [-6, 6]) keep the FP16 bar
   thanks to the per-butterfly power-of-two scaling.
 """
