@@ -99,6 +99,9 @@ SIGNATURES = {
     "afc_czt_execute": (_i32, [_vp, _vp, _vp, _i64, _vp]),
     "afc_czt_conv_len": (_i32, [_vp, _pi64]),
     "afc_czt_plan_destroy": (_i32, [_vp]),
+    "afc_hilbert_plan_create": (_i32, [ctypes.POINTER(_vp), _i64, _i32, _i32]),
+    "afc_hilbert_analytic": (_i32, [_vp, _vp, _vp, _i64, _vp]),
+    "afc_hilbert_plan_destroy": (_i32, [_vp]),
     "afc_nufft1d_plan_create": (_i32, [ctypes.POINTER(_vp), _i64, _dbl, _i64, _i64, _i32]),
     "afc_nufft1d_type1": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),
     "afc_nufft1d_type2": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),

@@ -1040,6 +1040,23 @@ struct afc_czt_plan_s {
   }
 };
 
+// Analytic-signal plan (apollo-hilbert HilbertPlan, application/execution/plan/
+// hilbert.rs:21-75, over analytic_signal_into, infrastructure/kernel/direct.rs:
+// 85-106): forward FFT of the real signal, the analytic mask, inverse FFT, all
+// in one convolution tile per lane.
+struct afc_hilbert_plan_s {
+  int64_t n = 0;
+  bool dbl = true;
+  int device = 0;
+  afc::LenPlan lp;        // the length-n transform in one CTA (n >= 2)
+  void* mask = nullptr;   // mask(k) / n as complex: 1 at DC (and n/2 for even n), 2 below (n+1)/2, 0 above
+  ~afc_hilbert_plan_s() {
+    void* ptrs[] = {lp.tw, mask};
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+  }
+};
+
 namespace afc {
 
 struct DeviceGuard {
@@ -1938,6 +1955,93 @@ afc_status afc_czt_execute(afc_czt_plan plan, const void* in, void* out, int64_t
   d.L = choose_L(plan->lp, batch, true, true, csz, 2 * csz + 3 * sizeof(long long), 2);
   cudaError_t e = do_conv(d, plan->dbl, false, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "czt execute");
+  return AFC_OK;
+}
+
+afc_status afc_hilbert_plan_create(afc_hilbert_plan* out, int64_t n, afc_precision prec, int device) {
+  if (!out) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  *out = nullptr;
+  if (n < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `len`: `%lld` violates `> 0`", (long long)n);
+  if (prec != AFC_PREC_F32 && prec != AFC_PREC_F64)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `precision`: `%d` violates `F32|F64`", (int)prec);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(AFC_ERR_BACKEND_UNAVAILABLE, "backend unavailable: cuda (no device)");
+  if (device < 0 || device >= ndev)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `device`: `%d` violates `< %d`", device, ndev);
+  const bool dbl = prec == AFC_PREC_F64;
+  const size_t csz = dbl ? 16 : 8;
+  if (n >= 2 && !plannable(n, csz))
+    return fail(AFC_ERR_UNSUPPORTED, "analytic signal of length %lld needs a smooth length that fits one CTA",
+                (long long)n);
+  DeviceGuard g(device);
+  std::unique_ptr<afc_hilbert_plan_s> p(new afc_hilbert_plan_s());
+  p->n = n;
+  p->dbl = dbl;
+  p->device = device;
+  if (n == 1) {  // x + 0i: no transform
+    *out = p.release();
+    return AFC_OK;
+  }
+  // the reference's apply_analytic_mask (direct.rs:130-143), with the inverse's 1/n folded in
+  std::vector<double> mk(2 * n, 0.0);
+  const int64_t positive_end = (n + 1) / 2;
+  for (int64_t k = 0; k < n; ++k) {
+    const double sc = (k == 0 || (n % 2 == 0 && k == n / 2)) ? 1.0 : (k < positive_end ? 2.0 : 0.0);
+    mk[2 * k] = sc / (double)n;
+  }
+  if (dbl) {
+    AFC_CUDA(dev_alloc(&p->mask, (size_t)n * csz), "analytic mask");
+    AFC_CUDA(cudaMemcpy(p->mask, mk.data(), (size_t)n * csz, cudaMemcpyHostToDevice), "analytic mask");
+  } else {
+    std::vector<float> f(mk.begin(), mk.end());
+    AFC_CUDA(dev_alloc(&p->mask, (size_t)n * csz), "analytic mask");
+    AFC_CUDA(cudaMemcpy(p->mask, f.data(), (size_t)n * csz, cudaMemcpyHostToDevice), "analytic mask");
+  }
+  cudaStream_t st;
+  AFC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+  afc_status s = build_lenplan(n, dbl, p->lp, st);
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  if (s != AFC_OK) return s;
+  *out = p.release();
+  return AFC_OK;
+}
+
+afc_status afc_hilbert_analytic(afc_hilbert_plan plan, const void* signal, void* out, int64_t batch, void* stream) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (!signal || !out) return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  if (batch < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `batch`: `%lld` violates `> 0`", (long long)batch);
+  const size_t rsz = plan->dbl ? 8 : 4, csz = 2 * rsz;
+  DeviceGuard g(plan->device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (plan->n == 1) {  // (x, 0) per lane
+    AFC_CUDA(cudaMemsetAsync(out, 0, (size_t)batch * csz, st), "analytic signal");
+    AFC_CUDA(cudaMemcpy2DAsync(out, csz, signal, rsz, rsz, (size_t)batch, cudaMemcpyDeviceToDevice, st),
+             "analytic signal");
+    return AFC_OK;
+  }
+  LaunchDesc d;
+  fill_common(d, plan->lp);
+  d.lanes = batch;
+  d.im = LaneMap{1, 1, plan->n, 0, 0, 1, nullptr};
+  d.om = LaneMap{1, 1, plan->n, 0, 0, 1, nullptr};
+  d.in = signal;
+  d.out = out;
+  d.in_op = IN_R;     // real signal widened
+  d.out_op = OUT_C;   // analytic signal
+  d.spec = plan->mask;
+  d.scale = 1.0;
+  d.L = choose_L(plan->lp, batch, true, true, csz, 2 * csz + 3 * sizeof(long long), 2);
+  cudaError_t e = do_conv(d, plan->dbl, false, st);
+  if (e != cudaSuccess) return cuda_fail(e, "analytic signal");
+  return AFC_OK;
+}
+
+afc_status afc_hilbert_plan_destroy(afc_hilbert_plan plan) {
+  if (!plan) return AFC_OK;
+  DeviceGuard g(plan->device);
+  delete plan;
   return AFC_OK;
 }
 

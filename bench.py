@@ -273,7 +273,7 @@ def main():
     ap.add_argument("--shape", default=None, help="override the 3D shape, e.g. 128,256,256 (profiling cases)")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
     ap.add_argument("--quick", action="store_true", help="headline only: no other shapes, e2e or CPU legs")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "stft", "czt", "nufft", "nufft3d"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "stft", "czt", "nufft", "nufft3d", "hilbert"],
                     help="c2 (default) is the headline; c1/c3/c4/c5 print their own lines")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -477,6 +477,26 @@ def run_secondary(args):
                                 "kind": "port", "sample": f"{reps} x (64 x 4096 fwd+inv)"}
         line["error_vs_oracle_rel_l2"] = float(np.linalg.norm(p.execute(torch.from_numpy(xin).to(dev)).cpu().numpy()
                                                               - yy) / np.linalg.norm(yy))
+        # the same two calls captured once in a CUDA graph and replayed: the device
+        # time without the per-call host work (Python checks, C ABI, launch)
+        try:
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(side):
+                for _ in range(3):
+                    p.execute(x, out=y)
+                    p.execute(y, out=x, inverse=True)
+            torch.cuda.current_stream().wait_stream(side)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                p.execute(x, out=y)
+                p.execute(y, out=x, inverse=True)
+            tg = _events_time(g.replay, args.steps, args.warmup, torch)
+            line["graph_us_per_step"] = round(tg * 1e6, 2)
+            line["graph_hbm_frac"] = round(2 * 2 * 64 * 4096 * 16 / tg / 1e9 / hbm_peak, 4)
+        except Exception as exc:  # capture refused: report the host-driven figure only
+            line["graph_us_per_step"] = None
+            line["graph_error"] = str(exc)[:200]
     elif args.workload == "c3":
         lens = W.c3_lengths()
         xv = W.c3_values(lens)
@@ -679,6 +699,35 @@ def run_secondary(args):
         line["cpu_baseline"] = {"value": round(2 * sub / tc, 1), "unit": "points/s", "cores": O.max_threads(),
                                 "kind": "port", "sample": f"type 1 + type 2 of the first {sub} points, same plan "
                                 "(spreading one thread in numpy, oracle FFT on all threads)"}
+    elif args.workload == "hilbert":
+        # apollo-hilbert's analytic_signal_into (forward, mask, normalized inverse)
+        # as one fused launch: 4096 lanes of 4096 f64 samples (seeded N(0,1))
+        from apollofft_b200.hilbert import HilbertPlan
+        lanes, n = 4096, 4096
+        xn = np.random.default_rng(16).standard_normal((lanes, n))
+        x = torch.from_numpy(xn).to(dev)
+        plan = HilbertPlan(n)
+        out = torch.empty((lanes, n), dtype=torch.complex128, device=dev)
+        t = _events_time(lambda: plan.analytic_signal(x, out=out), args.steps, args.warmup, torch)
+        fl = lanes * 2 * 5 * n * math.log2(n)  # two length-n transforms per lane
+        byts = lanes * n * (8 + 16)
+        line.update({"metric": "GFLOP/s", "value": round(fl / t / 1e9, 1), "ms_per_step": round(t * 1e3, 4),
+                     "signals_per_s": round(lanes / t, 1), "hbm_frac": round(byts / t / 1e9 / hbm_peak, 4),
+                     "config": f"analytic signal f64: {lanes} lanes x {n}, one fused launch"})
+        from oracle import oracle as O
+        sub = 512
+        k = np.arange(n)
+        mask = np.where(k < (n + 1) // 2, 2.0, 0.0)
+        mask[0] = 1.0
+        mask[n // 2] = 1.0
+        t0 = time.perf_counter()
+        ref = O.fft1d(O.fft1d(xn[:sub].astype(np.complex128)) * mask, inverse=True)
+        tc = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(sub * 2 * 5 * n * math.log2(n) / tc / 1e9, 2), "unit": "GFLOP/s",
+                                "cores": O.max_threads(), "kind": "port",
+                                "sample": f"{sub} lanes: oracle forward, mask, oracle inverse"}
+        line["quadrature_rel_l2_vs_reference_path"] = float(
+            np.linalg.norm(out[:sub].cpu().numpy().imag - ref.imag) / np.linalg.norm(ref.imag))
     elif args.workload == "nufft3d":
         # apollo-nufft NufftPlan3D at the reference defaults (sigma 2, width 6):
         # 64^3 modes on the unit cube (oversampled 128^3), 2^18 uniform random

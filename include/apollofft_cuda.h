@@ -236,6 +236,22 @@ AFC_API afc_status afc_czt_execute(afc_czt_plan plan, const void* in, void* out,
 AFC_API afc_status afc_czt_conv_len(afc_czt_plan plan, int64_t* conv_len);
 AFC_API afc_status afc_czt_plan_destroy(afc_czt_plan plan);
 
+/* Analytic signal on the device, apollo-hilbert HilbertPlan::analytic_signal_into
+ * (apollo-hilbert/.../plan/hilbert.rs:52-75 over infrastructure/kernel/direct.rs:
+ * 85-143): forward FFT of each real lane, the analytic mask (1 at DC and, for
+ * even n, at n/2; 2 on bins 1..(n+1)/2-1; 0 above), normalized inverse FFT,
+ * as one fused launch (one shared-memory tile per lane).  `signal` is
+ * batch x n real (float64 for F64, float32 for F32), `out` batch x n complex,
+ * device pointers.  The quadrature H{x} is the imaginary part; the real part
+ * is the inverse FFT's value (the reference then overwrites it with x; here it
+ * equals x to rounding).  n must be smooth (2, 3, 5, 7, 11, 13 factors) and fit
+ * one CTA, else AFC_ERR_UNSUPPORTED; n = 1 gives x + 0i. */
+typedef struct afc_hilbert_plan_s* afc_hilbert_plan;
+AFC_API afc_status afc_hilbert_plan_create(afc_hilbert_plan* out, int64_t n, afc_precision precision, int device);
+AFC_API afc_status afc_hilbert_analytic(afc_hilbert_plan plan, const void* signal, void* out, int64_t batch,
+                                        void* stream);
+AFC_API afc_status afc_hilbert_plan_destroy(afc_hilbert_plan plan);
+
 /* 1D non-uniform FFT on the device, apollo-nufft NufftPlan1D
  * (apollo-nufft/.../transform/dimension_1d.rs:101-272): n uniform bins on the
  * periodic domain [0, n dx), oversampled grid m = sigma n, Kaiser-Bessel kernel
