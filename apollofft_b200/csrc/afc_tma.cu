@@ -42,6 +42,7 @@ template <class T> struct TmaArgs {
   int real_in;      // contiguous in-place mode: input lanes are real (widened to complex in stage 0)
   int real_out;     // contiguous in-place mode: output lanes are the real parts
   int nbx, bn;      // boxes along the transformed axis, rows per box
+  unsigned tw_bytes;  // > 0: one tile per CTA, the twiddle table is copied into the idle second slot
   T scale;
   unsigned* err;
 };
@@ -217,24 +218,27 @@ __device__ __forceinline__ void tma_stage_inplace(TView<C> src, TView<C> dst, in
 }
 
 template <class T>
+// tw_dst non-null: the twiddle table (a.tw_bytes) rides on the same barrier.
 __device__ __forceinline__ void tma_issue_load(const TmaArgs<T>& a, long long tile, typename CT<T>::type* slot,
-                                               unsigned long long* bar) {
+                                               unsigned long long* bar, typename CT<T>::type* tw_dst = nullptr) {
   using C = typename CT<T>::type;
+  const unsigned extra = tw_dst ? a.tw_bytes : 0u;
   if (a.mode == 0) {
     const long long q0 = tile * a.L;
     const long long rem = a.lanes - q0;
     const int lanes_here = (int)(rem < a.L ? rem : a.L);
     const size_t es = a.real_in ? sizeof(T) : sizeof(C);
     const unsigned bytes = (unsigned)((long long)lanes_here * a.sl.n * es);
-    mbar_expect_tx(bar, bytes);
+    mbar_expect_tx(bar, bytes + extra);
     bulk_load(slot, reinterpret_cast<const char*>(a.in) + q0 * a.sl.n * es, bytes, bar);
   } else {
     const int o = (int)(tile / a.kb), kb = (int)(tile % a.kb);
     const unsigned box_bytes = (unsigned)(2 * a.L * a.bn * sizeof(T));
-    mbar_expect_tx(bar, box_bytes * a.nbx);
+    mbar_expect_tx(bar, box_bytes * a.nbx + extra);
     for (int b = 0; b < a.nbx; ++b)
       tma_load_3d(slot + (long long)b * a.bn * a.L, &a.tmi, 2 * kb * a.L, b * a.bn, o, bar);
   }
+  if (extra) bulk_load(tw_dst, a.tw, extra, bar);
 }
 
 template <class T>
@@ -293,7 +297,11 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
     fence_proxy_async();
   }
   __syncthreads();
-  if (tid == 0) tma_issue_load(a, tile, slots[0], &bars[0]);
+  // a CTA with a single tile never prefetches into the second slot: the
+  // twiddle table is staged there with the tile (stage twiddles then come from
+  // shared memory instead of L1 misses to L2)
+  if (tid == 0) tma_issue_load(a, tile, slots[0], &bars[0], a.tw_bytes ? slots[1] : nullptr);
+  const C* twb = a.tw_bytes ? slots[1] : a.tw;
   const TView<C> wv{work, ld, 1, 1};
   const int nst = a.sl.nst;
   for (int it = 0;; ++it) {
@@ -324,7 +332,7 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
       const bool last = s == nst - 1;
       const TView<C> src = s == 0 ? lin : cpad;
       const TView<C> dst = last ? olin : cpad;
-      const C* twi = a.tw + sd.twoff;
+      const C* twi = twb + sd.twoff;
       const T* rsrc = (s == 0 && a.real_in) ? reinterpret_cast<const T*>(cur) : nullptr;
       T* rdst = (last && a.real_out) ? reinterpret_cast<T*>(cur) : nullptr;
 #define AFC_TI(R) tma_stage_inplace<R, INV, (V == 4 ? 1 : 0)>(src, dst, l, n, sd.Ns, twi, t, P, last, a.scale, rsrc, rdst)
@@ -358,7 +366,7 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
       const bool last = s == nst - 1;
       const TView<C> src = s == 0 ? lin : ((s & 1) ? wv : cpad);
       const TView<C> dst = last ? olin : ((s & 1) ? cpad : wv);
-      const C* twi = a.tw + sd.twoff;
+      const C* twi = twb + sd.twoff;
 #define AFC_TM(R) tma_stage<R, INV>(src, dst, l, n, sd.Ns, twi, t, P, last, a.scale)
       if constexpr (P2) {
         switch (sd.R) {
@@ -610,6 +618,16 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
   }
   const int per_sm = kernel_ctas_per_sm(reinterpret_cast<const void*>(k), tp.L * tp.P, smem);
   long long grid = (long long)g_tma_sm * per_sm;
+  if (grid >= tp.ntiles) {
+    // one tile per CTA: stage the twiddle table (r-major, twoff + (R - 1) Ns
+    // entries per stage) in the second slot when it fits and can be bulk-copied
+    long long twc = 0;
+    for (int s = 0; s < d.sl.nst; ++s)
+      if (d.sl.st[s].Ns > 1) twc = std::max<long long>(twc, d.sl.st[s].twoff + (long long)(d.sl.st[s].R - 1) * d.sl.st[s].Ns);
+    const long long twb = twc * (long long)sizeof(C);
+    if (twc > 0 && twb % 16 == 0 && twc <= tp.slot_elems && (reinterpret_cast<uintptr_t>(d.tw) & 15) == 0)
+      a.tw_bytes = (unsigned)twb;
+  }
   if (grid > tp.ntiles) grid = tp.ntiles;
   k<<<(unsigned)grid, tp.L * tp.P, smem, st>>>(a);
   count_launch(1);
