@@ -102,25 +102,32 @@ class CudaPlan:
     # ── device execution (torch tensors) ──
     def execute(self, x, out=None, inverse: bool = False, scale: Optional[float] = None, stream=None):
         """Runs on torch CUDA tensors; returns `out` (allocated if None)."""
-        import torch
-        t_in, t_out, ie, oe = self._io(inverse)
+        io = self.__dict__.get("_io_inv" if inverse else "_io_fwd")
+        if io is None:  # fixed per plan and direction: looked up once
+            io = self._io(inverse)
+            self.__dict__["_io_inv" if inverse else "_io_fwd"] = io
+        t_in, t_out, ie, oe = io
         if x.dtype != t_in:
             raise ValueError(f"expected {t_in} input, got {x.dtype}")
         if not x.is_contiguous():
             raise ValueError("input must be C-contiguous")
         if x.numel() != ie:
             raise ValueError(f"shape mismatch: expected {ie} elements, got {x.numel()}")
+        if not x.is_cuda:
+            raise ValueError("input must be a CUDA tensor (use execute_host for host arrays)")
         if out is None:
+            import torch
             out = torch.empty(self.out_shape(inverse) if oe == int(np.prod(self.out_shape(inverse))) else (oe,),
                               dtype=t_out, device=x.device)
-        if out.numel() != oe or out.dtype != t_out or not out.is_contiguous():
+        if out.numel() != oe or out.dtype != t_out or not out.is_contiguous() or not out.is_cuda:
             raise ValueError("output buffer does not match the plan")
-        st = stream if stream is not None else _current_stream(x.device)
+        st = stream if stream is not None else _stream_of(x)
         if scale is None:
-            status = self._exec(self._h, x.data_ptr(), out.data_ptr(), int(inverse), st)
+            status = self._exec(self._h, x.data_ptr(), out.data_ptr(), 1 if inverse else 0, st)
         else:
             status = L.lib().afc_execute_scaled(self._h, x.data_ptr(), out.data_ptr(), int(inverse), float(scale), st)
-        L.check(status, "execute")
+        if status:
+            L.check(status, "execute")
         return out
 
     def adjoint(self, g, inverse: bool = False, stream=None):
@@ -165,14 +172,18 @@ class CudaPlan:
             pass
 
 
-def _current_stream(device):
-    """Raw handle of the current CUDA stream of `device` (torch's fast accessor
-    when present)."""
-    import torch
-    raw = getattr(torch._C, "_cuda_getCurrentRawStream", None)
-    if raw is not None:
-        return raw(device.index if device.index is not None else torch.cuda.current_device())
-    return torch.cuda.current_stream(device).cuda_stream
+_RAW_STREAM = None
+
+
+def _stream_of(x):
+    """Raw handle of the current CUDA stream of tensor x's device (torch's
+    fast accessor, looked up once)."""
+    global _RAW_STREAM
+    if _RAW_STREAM is None:
+        import torch
+        _RAW_STREAM = getattr(torch._C, "_cuda_getCurrentRawStream", None) or \
+            (lambda idx: torch.cuda.current_stream(idx).cuda_stream)
+    return _RAW_STREAM(x.get_device())
 
 
 def _torch_dtypes():
