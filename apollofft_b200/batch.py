@@ -30,10 +30,12 @@ class BatchPlan:
     def execute(self, x, out=None, inverse: bool = False, mode: int = 0, stream=None):
         import torch
         want = torch.complex128 if self.precision == "f64" else torch.complex64
-        if x.dtype != want or not x.is_contiguous() or x.numel() != self.total:
+        if x.dtype != want or not x.is_contiguous() or x.numel() != self.total or not x.is_cuda:
             raise ValueError(f"expected a contiguous {want} tensor of {self.total} elements")
         if out is None:
             out = torch.empty_like(x)
+        if out.dtype != want or not out.is_contiguous() or out.numel() != self.total or not out.is_cuda:
+            raise ValueError("output buffer does not match the plan")
         st = stream if stream is not None else torch.cuda.current_stream(x.device).cuda_stream
         L.check(L.lib().afc_batch_execute(self._h, x.data_ptr(), out.data_ptr(), int(inverse), int(mode), st),
                 "batch execute")

@@ -53,12 +53,12 @@ class CztPlan:
         leading batch); returns the (..., m) transform."""
         import torch
         cdt = torch.complex128 if self.precision == "f64" else torch.complex64
-        if x.dtype != cdt or not x.is_contiguous() or x.shape[-1] != self.n:
+        if x.dtype != cdt or not x.is_contiguous() or x.shape[-1] != self.n or not x.is_cuda:
             raise ValueError(f"expected a contiguous {cdt} tensor with last dimension {self.n}")
         batch = x.numel() // self.n
         if out is None:
             out = torch.empty(tuple(x.shape[:-1]) + (self.m,), dtype=cdt, device=x.device)
-        if out.dtype != cdt or not out.is_contiguous() or out.numel() != batch * self.m:
+        if out.dtype != cdt or not out.is_contiguous() or out.numel() != batch * self.m or not out.is_cuda:
             raise ValueError("output buffer does not match the plan")
         st = stream if stream is not None else torch.cuda.current_stream(x.device).cuda_stream
         L.check(L.lib().afc_czt_execute(self._h, x.data_ptr(), out.data_ptr(), batch, st), "czt execute")

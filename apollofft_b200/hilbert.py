@@ -34,12 +34,12 @@ class HilbertPlan:
         import torch
         rt = torch.float64 if self.precision == "f64" else torch.float32
         ct = torch.complex128 if self.precision == "f64" else torch.complex64
-        if x.dtype != rt or not x.is_contiguous() or x.dim() < 1 or x.shape[-1] != self.n:
+        if x.dtype != rt or not x.is_contiguous() or x.dim() < 1 or x.shape[-1] != self.n or not x.is_cuda:
             raise ValueError(f"signal: expected a contiguous {rt} tensor whose last dimension is {self.n}")
         lanes = x.numel() // self.n
         if out is None:
             out = torch.empty(x.shape, dtype=ct, device=x.device)
-        if out.dtype != ct or not out.is_contiguous() or out.numel() != x.numel():
+        if out.dtype != ct or not out.is_contiguous() or out.numel() != x.numel() or not out.is_cuda:
             raise ValueError("output buffer does not match the signal")
         if lanes == 0:
             return out

@@ -39,7 +39,7 @@ class NufftPlan1D:
 
     @staticmethod
     def _check(t, dtype, what):
-        if t.dtype != dtype or not t.is_contiguous() or t.dim() != 1:
+        if t.dtype != dtype or not t.is_contiguous() or t.dim() != 1 or not t.is_cuda:
             raise ValueError(f"{what}: expected a contiguous 1D {dtype} tensor")
 
     def type1(self, positions, values, out=None, stream=None):
@@ -103,7 +103,7 @@ class NufftPlan3D:
 
     @staticmethod
     def _check(t, dtype, what, shape=None):
-        if t.dtype != dtype or not t.is_contiguous():
+        if t.dtype != dtype or not t.is_contiguous() or not t.is_cuda:
             raise ValueError(f"{what}: expected a contiguous {dtype} tensor")
         if shape is not None and tuple(t.shape) != tuple(shape):
             raise ValueError(f"{what}: expected shape {tuple(shape)}, got {tuple(t.shape)}")

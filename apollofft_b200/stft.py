@@ -71,7 +71,7 @@ class StftPlan:
         frames x spectrum_len array, reshaped)."""
         import torch
         rdt = self._real_dtype()
-        if signal.dtype != rdt or signal.dim() != 1 or not signal.is_contiguous():
+        if signal.dtype != rdt or signal.dim() != 1 or not signal.is_contiguous() or not signal.is_cuda:
             raise ValueError(f"expected a contiguous 1D {rdt} signal")
         if signal.numel() < self.frame_len:
             raise StftError("input signal shorter than frame length")
@@ -87,7 +87,7 @@ class StftPlan:
         cdt = torch.complex128 if rdt == torch.float64 else torch.complex64
         if out is None:
             out = torch.empty((frames, self.frame_len), dtype=cdt, device=signal.device)
-        if out.dtype != cdt or not out.is_contiguous():
+        if out.dtype != cdt or not out.is_contiguous() or not out.is_cuda:
             raise ValueError("output buffer does not match the plan")
         st = stream if stream is not None else torch.cuda.current_stream(signal.device).cuda_stream
         L.check(L.lib().afc_stft_forward(self.plan._h, signal.data_ptr(), signal.numel(), win.data_ptr(),
@@ -100,7 +100,7 @@ class StftPlan:
         import torch
         rdt = self._real_dtype()
         cdt = torch.complex128 if rdt == torch.float64 else torch.complex64
-        if spectrum.dtype != cdt or not spectrum.is_contiguous():
+        if spectrum.dtype != cdt or not spectrum.is_contiguous() or not spectrum.is_cuda:
             raise ValueError(f"expected a contiguous {cdt} spectrum")
         if signal_len < self.frame_len:
             raise StftError("input signal shorter than frame length")
@@ -121,6 +121,8 @@ class StftPlan:
         ws = torch.empty(max(nbytes.value // (8 if rdt == torch.float64 else 4), 1), dtype=rdt, device=spectrum.device)
         if out is None:
             out = torch.empty(int(signal_len), dtype=rdt, device=spectrum.device)
+        if out.dtype != rdt or not out.is_contiguous() or out.numel() != int(signal_len) or not out.is_cuda:
+            raise ValueError("output buffer does not match the signal length")
         st = stream if stream is not None else torch.cuda.current_stream(spectrum.device).cuda_stream
         L.check(L.lib().afc_stft_inverse(self.plan._h, spectrum.data_ptr(), spectrum.numel(), win.data_ptr(),
                                          self.hop_len, out.data_ptr(), int(signal_len), ws.data_ptr(),
