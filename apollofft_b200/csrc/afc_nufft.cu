@@ -360,14 +360,6 @@ __device__ __forceinline__ double nu_tile_weight(const NuGeom3& g, const NuTiles
   return nu_kb((double)(tap - g.w) - (t - rt), (double)g.w, g.beta, g.i0b);
 }
 
-__device__ __forceinline__ int nu_tile_centre(const NuGeom3& g, const NuTiles& tl, const NuTileCoord& tc,
-                                              const double* pos, int a) {
-  const double len = a == 0 ? g.lx : a == 1 ? g.ly : g.lz;
-  const long long m = a == 0 ? g.mx : a == 1 ? g.my : g.mz;
-  const int t0 = a == 0 ? tc.tx : a == 1 ? tc.ty : tc.tz;
-  return nu_centre(pos[a], len, m) - t0 * tl.B;
-}
-
 // The lane's cells of a T x T (py, pz) plane: at most kNuTileIters, packed
 // py << 8 | pz (-1 past the plane), fixed for the whole kernel.
 constexpr int kNuTileIters = 12;  // ceil(T^2 / 32) for T <= 19 (w <= 9)
