@@ -81,3 +81,44 @@ def test_length_one_validation_and_unsupported(afc, cuda):
     plan = HilbertPlan(64)
     with pytest.raises(ValueError):
         plan.analytic_signal(torch.zeros(63, dtype=torch.float64, device="cuda"))
+
+
+def _kat_signals():
+    """The reference's own known answers (apollo-hilbert verification/mod.rs:11-135)."""
+    t16, t32, t64 = np.arange(16), np.arange(32), np.arange(64)
+    return {
+        "cos16": np.cos(2 * np.pi * t16 / 16),
+        "cos3_32": np.cos(2 * np.pi * 3 * t32 / 32),
+        "const9": np.full(9, 4.0),
+        "alt10": np.array([1.0 if i % 2 == 0 else -1.0 for i in range(10)]),
+        "sin3_32": np.sin(2 * np.pi * 3 * t32 / 32),
+        "cos5_64": np.cos(2 * np.pi * 5 * t64 / 64),
+    }
+
+
+def test_reference_known_answers(afc, cuda):
+    from apollofft_b200.hilbert import HilbertPlan
+    s = _kat_signals()
+
+    def z_of(x):
+        return HilbertPlan(len(x)).analytic_signal(torch.from_numpy(x).cuda()).cpu().numpy()
+
+    # cosine -> sine quadrature (:11-25)
+    assert np.abs(z_of(s["cos16"]).imag - np.sin(2 * np.pi * np.arange(16) / 16)).max() < 1e-11
+    # real part kept, unit envelope (:28-46)
+    z = z_of(s["cos3_32"])
+    assert np.abs(z.real - s["cos3_32"]).max() < 1e-12 and np.abs(np.abs(z) - 1.0).max() < 1e-11
+    # constant: zero quadrature, constant envelope (:49-59)
+    z = z_of(s["const9"])
+    assert np.abs(z.real - 4.0).max() < 1e-12 and np.abs(z.imag).max() < 1e-12
+    # even-length Nyquist tone has zero quadrature (:62-72)
+    assert np.abs(z_of(s["alt10"]).imag).max() < 1e-12
+    # H{H{x}} = -x for a zero-mean tone (:124-137)
+    p = HilbertPlan(32)
+    h1 = p.transform(torch.from_numpy(s["sin3_32"]).cuda())
+    h2 = p.transform(h1).cpu().numpy()
+    assert np.abs(h2 + s["sin3_32"]).max() < 1e-10
+    # constant instantaneous frequency k / n of a tone (:104-121)
+    z = z_of(s["cos5_64"])
+    f = np.diff(np.unwrap(np.angle(z))) / (2 * np.pi)
+    assert np.abs(f - 5 / 64).max() < 1e-10
