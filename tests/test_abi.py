@@ -75,3 +75,35 @@ def test_python_api_validation_messages(afc):
         afc.irfft3(np.ones((2, 2, 3), dtype=np.complex128), 4)
     with pytest.raises(ValueError, match="unsupported precision"):
         afc.fft1(np.zeros(4), precision="bogus")
+
+
+def test_caller_entry_points_validate_without_device(afc):
+    """Argument checks of the fused caller entry points run before any device
+    work (null handles, empty lengths, invalid spacing / oversampling / width /
+    precision)."""
+    L = afc._lib
+    lib = L.lib()
+    h = ctypes.c_void_p()
+    # 3D NUFFT (apollo-nufft NufftPlan3D::new / UniformGrid3D::new contracts)
+    for args, field in [((0, 4, 4, 1.0, 1.0, 1.0, 2, 6), "nx"), ((4, 4, 0, 1.0, 1.0, 1.0, 2, 6), "nz"),
+                        ((4, 4, 4, 1.0, 0.0, 1.0, 2, 6), "dy"), ((4, 4, 4, 1.0, 1.0, float("inf"), 2, 6), "dz"),
+                        ((4, 4, 4, 1.0, 1.0, 1.0, 1, 6), "sigma"), ((4, 4, 4, 1.0, 1.0, 1.0, 2, 1), "kernel_width"),
+                        ((4, 4, 4, 1.0, 1.0, 1.0, 2, 33), "kernel_width")]:
+        assert lib.afc_nufft3d_plan_create(ctypes.byref(h), *args, 0) == L.AFC_ERR_VALIDATION
+        assert field in L.last_error()
+    assert lib.afc_nufft3d_plan_create(None, 4, 4, 4, 1.0, 1.0, 1.0, 2, 6, 0) == L.AFC_ERR_VALIDATION
+    assert lib.afc_nufft3d_type1(None, None, None, 0, None, None) == L.AFC_ERR_VALIDATION
+    assert lib.afc_nufft3d_type2(None, None, None, 0, None, None) == L.AFC_ERR_VALIDATION
+    m = (ctypes.c_int64 * 3)()
+    assert lib.afc_nufft3d_grid_dims(None, m) == L.AFC_ERR_VALIDATION
+    assert lib.afc_nufft3d_plan_destroy(None) == L.AFC_OK
+    # 1D NUFFT
+    assert lib.afc_nufft1d_plan_create(ctypes.byref(h), 0, 1.0, 2, 6, 0) == L.AFC_ERR_VALIDATION
+    assert lib.afc_nufft1d_plan_create(ctypes.byref(h), 8, -1.0, 2, 6, 0) == L.AFC_ERR_VALIDATION
+    # analytic signal (apollo-hilbert HilbertPlan::new rejects an empty signal)
+    assert lib.afc_hilbert_plan_create(ctypes.byref(h), 0, L.PREC_F64, 0) == L.AFC_ERR_VALIDATION
+    assert "len" in L.last_error()
+    assert lib.afc_hilbert_plan_create(ctypes.byref(h), 16, 7, 0) == L.AFC_ERR_VALIDATION
+    assert lib.afc_hilbert_plan_create(None, 16, L.PREC_F64, 0) == L.AFC_ERR_VALIDATION
+    assert lib.afc_hilbert_analytic(None, None, None, 1, None) == L.AFC_ERR_VALIDATION
+    assert lib.afc_hilbert_plan_destroy(None) == L.AFC_OK
