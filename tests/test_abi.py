@@ -107,3 +107,19 @@ def test_caller_entry_points_validate_without_device(afc):
     assert lib.afc_hilbert_plan_create(None, 16, L.PREC_F64, 0) == L.AFC_ERR_VALIDATION
     assert lib.afc_hilbert_analytic(None, None, None, 1, None) == L.AFC_ERR_VALIDATION
     assert lib.afc_hilbert_plan_destroy(None) == L.AFC_OK
+
+
+def test_czt_entry_points_validate_without_device(afc):
+    """apollo-czt CztPlan::new contracts (czt/dimension_1d.rs:61-75): positive
+    lengths, finite non-zero A and W."""
+    L = afc._lib
+    lib = L.lib()
+    h = ctypes.c_void_p()
+    for args in [(0, 8, 1.0, 0.0, 0.0, 1.0), (8, 0, 1.0, 0.0, 0.0, 1.0), (8, 8, 0.0, 0.0, 0.0, 1.0),
+                 (8, 8, 1.0, 0.0, 0.0, 0.0), (8, 8, float("nan"), 0.0, 0.0, 1.0)]:
+        assert lib.afc_czt_plan_create(ctypes.byref(h), *args, L.PREC_F64, 0) == L.AFC_ERR_VALIDATION
+    assert lib.afc_czt_plan_create(ctypes.byref(h), 8, 8, 1.0, 0.0, 0.0, 1.0, 9, 0) == L.AFC_ERR_VALIDATION
+    assert lib.afc_czt_execute(None, None, None, 1, None) == L.AFC_ERR_VALIDATION
+    v = ctypes.c_int64()
+    assert lib.afc_czt_conv_len(None, ctypes.byref(v)) == L.AFC_ERR_VALIDATION
+    assert lib.afc_czt_plan_destroy(None) == L.AFC_OK
