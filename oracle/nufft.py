@@ -181,3 +181,39 @@ def exact1_3d(pos, val, shape, L):
 
 def exact2_3d(modes, pos, shape, L):
     return np.exp(2j * np.pi * np.asarray(pos) @ _kgrid(shape, L).T) @ modes.reshape(-1)
+
+
+# ── the same plans in C++ (oracle/nufft_oracle.cpp), one thread: the timed CPU
+# baseline of the device NUFFT and a second restatement the tests pin ──
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def c_type1_1d(n, dx, sigma, w, pos, val):
+    pos, val = _c(pos, np.float64), _c(val, np.complex128)
+    out = np.empty(n, dtype=np.complex128)
+    O.lib().or_nufft1d_type1(n, dx, sigma, w, pos.ctypes.data, val.ctypes.data, len(pos), out.ctypes.data)
+    return out
+
+
+def c_type2_1d(n, dx, sigma, w, coeffs, pos):
+    pos, coeffs = _c(pos, np.float64), _c(coeffs, np.complex128)
+    out = np.empty(len(pos), dtype=np.complex128)
+    O.lib().or_nufft1d_type2(n, dx, sigma, w, coeffs.ctypes.data, pos.ctypes.data, len(pos), out.ctypes.data)
+    return out
+
+
+def c_type1_3d(shape, spacing, sigma, w, pos, val):
+    pos, val = _c(pos, np.float64), _c(val, np.complex128)
+    out = np.empty(shape, dtype=np.complex128)
+    O.lib().or_nufft3d_type1(*shape, *spacing, sigma, w, pos.ctypes.data, val.ctypes.data, len(val), out.ctypes.data)
+    return out
+
+
+def c_type2_3d(shape, spacing, sigma, w, modes, pos):
+    pos, modes = _c(pos, np.float64), _c(modes, np.complex128)
+    out = np.empty(len(pos), dtype=np.complex128)
+    O.lib().or_nufft3d_type2(*shape, *spacing, sigma, w, modes.ctypes.data, pos.ctypes.data, len(pos),
+                             out.ctypes.data)
+    return out

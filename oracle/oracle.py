@@ -37,7 +37,7 @@ def lib():
         if not os.path.exists(_LIB_PATH):
             build()
         L = ctypes.CDLL(_LIB_PATH)
-        u64, i32, dbl = ctypes.c_uint64, ctypes.c_int, ctypes.c_double
+        u64, i32, dbl, i64 = ctypes.c_uint64, ctypes.c_int, ctypes.c_double, ctypes.c_int64
         pu64 = ctypes.POINTER(ctypes.c_uint64)
         vp = ctypes.c_void_p
         sig = {
@@ -72,6 +72,10 @@ def lib():
             "or_fft_uneven_c128": (None, [vp, pu64, pu64, u64, i32, i32]),
             "or_direct_dft": (None, [vp, vp, u64, i32]),
             "or_max_threads": (i32, []),
+            "or_nufft1d_type1": (None, [i64, dbl, i64, i64, vp, vp, i64, vp]),
+            "or_nufft1d_type2": (None, [i64, dbl, i64, i64, vp, vp, i64, vp]),
+            "or_nufft3d_type1": (None, [i64, i64, i64, dbl, dbl, dbl, i64, i64, vp, vp, i64, vp]),
+            "or_nufft3d_type2": (None, [i64, i64, i64, dbl, dbl, dbl, i64, i64, vp, vp, i64, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

@@ -49,3 +49,25 @@ def test_restatement_3d_type2_scale(oracle, w):
     ref = RefPlan3(shape, spacing, 2, w)
     got = ref.type2(modes, pos, oracle) * np.prod(ref.m)
     assert rel_l2(got, exact2(modes, pos, shape, L)) < (1e-6 if w == 6 else 1e-3)
+
+
+def test_cpp_restatement_matches_numpy_restatement(oracle):
+    """The C++ plans (the timed CPU baseline) and the numpy plans agree."""
+    from oracle import nufft as N
+    rng = np.random.default_rng(21)
+    n, dx = 48, 0.125
+    L = n * dx
+    pos = rng.uniform(-0.5 * L, 1.5 * L, 80)
+    val = rng.standard_normal(80) + 1j * rng.standard_normal(80)
+    coeffs = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    ref = RefPlan(n, dx, 2, 6)
+    assert rel_l2(N.c_type1_1d(n, dx, 2, 6, pos, val), ref.type1(pos, val, oracle)) < 1e-13
+    assert rel_l2(N.c_type2_1d(n, dx, 2, 6, coeffs, pos), ref.type2(coeffs, pos, oracle)) < 1e-13
+    shape, spacing = (6, 5, 4), (0.5, 0.4, 0.25)
+    Ls = [a * b for a, b in zip(shape, spacing)]
+    pos3 = np.stack([rng.uniform(-0.5 * l, 1.5 * l, 40) for l in Ls], -1)
+    val3 = rng.standard_normal(40) + 1j * rng.standard_normal(40)
+    modes = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    ref3 = RefPlan3(shape, spacing, 2, 6)
+    assert rel_l2(N.c_type1_3d(shape, spacing, 2, 6, pos3, val3), ref3.type1(pos3, val3, oracle)) < 1e-13
+    assert rel_l2(N.c_type2_3d(shape, spacing, 2, 6, modes, pos3), ref3.type2(modes, pos3, oracle)) < 1e-13
