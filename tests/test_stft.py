@@ -119,3 +119,14 @@ def test_stft_inverse_vs_reference_and_roundtrip(afc, oracle, cuda, frame_len, h
     from apollofft_b200.stft import StftError
     with pytest.raises(StftError):
         plan.inverse(spec[:-1].contiguous(), n_sig)
+
+
+def test_restatement_roundtrip_reference_case(oracle):  # stft/dimension_1d/tests.rs:19-30
+    """The analysis / synthesis restatements reproduce the reference's COLA
+    round trip (frame 8, hop 4, its 12-sample signal) to its 1e-8 bound."""
+    from apollofft_b200.stft import hann_window
+    signal = np.array([1.0, -1.0, 0.5, 2.0, -0.75, 0.25, 1.5, -0.5, 0.125, 0.875, -1.25, 0.75])
+    w = hann_window(8)
+    spec = oracle.fft1d(frames_ref(signal, w, 8, 4))
+    rec, _ = istft_ref(spec, w, 8, 4, len(signal), oracle)
+    assert np.abs(rec - signal).max() < 1e-8
