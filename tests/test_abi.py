@@ -123,3 +123,20 @@ def test_czt_entry_points_validate_without_device(afc):
     v = ctypes.c_int64()
     assert lib.afc_czt_conv_len(None, ctypes.byref(v)) == L.AFC_ERR_VALIDATION
     assert lib.afc_czt_plan_destroy(None) == L.AFC_OK
+
+
+@pytest.mark.parametrize("compiler,std,lang", [("gcc", "-std=c99", "c"), ("g++", "-std=c++17", "c++")])
+def test_header_is_plain_c_and_cpp(tmp_path, compiler, std, lang):
+    """include/apollofft_cuda.h is the C ABI: it compiles as strict C99 (no torch
+    or CUDA types in the signatures) and as C++."""
+    import shutil
+    import subprocess
+    if shutil.which(compiler) is None:
+        pytest.skip(f"{compiler} not found")
+    src = tmp_path / "use_header.c"
+    src.write_text('#include "apollofft_cuda.h"\nint main(void) { afc_plan p = 0; (void)p; return 0; }\n')
+    cmd = [compiler, std, "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-x", lang,
+           "-I", os.path.join(ROOT, "include"), str(src)]
+    if lang == "c":
+        cmd.insert(3, "-pedantic")
+    subprocess.run(cmd, check=True)
