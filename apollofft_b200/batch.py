@@ -13,12 +13,14 @@ from typing import Sequence
 import numpy as np
 
 from . import _lib as L
+from .plan import require_device
 
 
 class BatchPlan:
     def __init__(self, lengths: Sequence[int], precision: str = "f32", device: int = 0):
         self.lengths = np.ascontiguousarray(np.asarray(lengths, dtype=np.int64))
         self.precision = precision
+        self.device = int(device)
         self.offsets = np.concatenate([[0], np.cumsum(self.lengths)[:-1]]).astype(np.int64)
         self.total = int(self.lengths.sum())
         self._h = ctypes.c_void_p()
@@ -32,10 +34,12 @@ class BatchPlan:
         want = torch.complex128 if self.precision == "f64" else torch.complex64
         if x.dtype != want or not x.is_contiguous() or x.numel() != self.total or not x.is_cuda:
             raise ValueError(f"expected a contiguous {want} tensor of {self.total} elements")
+        require_device(x, self.device, "input")
         if out is None:
             out = torch.empty_like(x)
         if out.dtype != want or not out.is_contiguous() or out.numel() != self.total or not out.is_cuda:
             raise ValueError("output buffer does not match the plan")
+        require_device(out, self.device, "output")
         st = stream if stream is not None else torch.cuda.current_stream(x.device).cuda_stream
         L.check(L.lib().afc_batch_execute(self._h, x.data_ptr(), out.data_ptr(), int(inverse), int(mode), st),
                 "batch execute")

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <complex>
+#include <condition_variable>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -961,6 +962,82 @@ struct PlanKey {
   }
 };
 
+// ─────────────────── ordering of plan-owned device buffers ───────────────────
+// Plan-owned scratch (execution workspaces, NUFFT grids, batch workspaces) is
+// reused by every call on the plan.  The reference's plans are shared across
+// threads (Arc, Send + Sync; apollo-stft runs Rayon over one FftPlan1D,
+// stft/dimension_1d.rs:225-239), so a call on one stream must not touch such a
+// buffer while a call on another stream still does.  A Fence is an event
+// recorded on the stream of the buffer's last use; the next user's stream waits
+// for it on the GPU, so no host thread blocks.  Inside a stream capture the
+// fence is skipped (an event recorded outside a capture cannot be waited on in
+// it): replays of a captured graph are ordered with other calls on the plan by
+// the caller.
+
+static bool stream_capturing(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return cs != cudaStreamCaptureStatusNone;
+}
+
+struct Fence {
+  cudaEvent_t ev = nullptr;
+  bool used = false;
+  cudaError_t before(cudaStream_t st, bool cap) const {
+    if (cap || !used) return cudaSuccess;
+    return cudaStreamWaitEvent(st, ev, 0);
+  }
+  cudaError_t after(cudaStream_t st, bool cap) {
+    if (cap) return cudaSuccess;
+    if (!ev) {
+      cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      if (e != cudaSuccess) return e;
+    }
+    used = true;
+    return cudaEventRecord(ev, st);
+  }
+  Fence() = default;
+  Fence(const Fence&) = delete;
+  Fence& operator=(const Fence&) = delete;
+  ~Fence() {
+    if (ev) cudaEventDestroy(ev);
+  }
+};
+
+// One execution workspace, bound to the stream that last used it.
+struct WsSlot {
+  cudaStream_t st = nullptr;
+  void* ptr = nullptr;
+  Fence fence;
+  uint64_t last = 0;
+  ~WsSlot() {
+    if (ptr) cudaFree(ptr);
+  }
+};
+
+// Device staging of one afc_execute_host call in flight: its own stream (and
+// through it its own workspace) and input / output buffers.
+struct HostStage {
+  cudaStream_t st = nullptr;
+  void* in = nullptr;
+  void* out = nullptr;
+  bool busy = false;
+  ~HostStage() {
+    if (in) cudaFree(in);
+    if (out) cudaFree(out);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
+// Workspaces per plan: concurrent streams get their own up to this count, then
+// take turns on the least recently used one (ordered by its fence).
+static const size_t kWsSlots = 4;
+// afc_execute_host calls of one plan in flight at once; more callers wait.
+static const size_t kHostStages = 4;
+
 }  // namespace afc
 
 struct afc_plan_s {
@@ -976,19 +1053,16 @@ struct afc_plan_s {
   std::atomic<int> refs{1};
   bool cached = false;
   afc::PlanKey key{};
+  // execution workspaces, one per stream in use (at most afc::kWsSlots)
   std::mutex ws_mu;
-  void* ws = nullptr;
+  std::vector<std::unique_ptr<afc::WsSlot>> ws_slots;
+  uint64_t ws_tick = 0;
   size_t ws_bytes = 0;
-  void* host_in = nullptr;   // staging for afc_execute_host
-  void* host_out = nullptr;
-  cudaStream_t host_stream = nullptr;
+  // staging of afc_execute_host calls in flight (at most afc::kHostStages)
+  std::mutex host_mu;
+  std::condition_variable host_cv;
+  std::vector<std::unique_ptr<afc::HostStage>> stages;
   int64_t N() const { return dims[0] * dims[1] * dims[2]; }
-  ~afc_plan_s() {
-    if (ws) cudaFree(ws);
-    if (host_in) cudaFree(host_in);
-    if (host_out) cudaFree(host_out);
-    if (host_stream) cudaStreamDestroy(host_stream);
-  }
 };
 
 // 1D NUFFT plan (apollo-nufft NufftPlan1D, transform/dimension_1d.rs:101-154):
@@ -1002,6 +1076,8 @@ struct afc_nufft_plan_s {
   afc_plan fft = nullptr;          // C2C f64 plan of length m
   double* deconv = nullptr;        // 1 / kb_ft(k_signed / m), k < n
   void* grid = nullptr;            // plan-owned oversampled grid (m complex128)
+  std::mutex mu;                   // one caller enqueues on the grid at a time
+  afc::Fence fence;                // the grid's last use on the GPU
   ~afc_nufft_plan_s();
 };
 
@@ -1019,6 +1095,8 @@ struct afc_nufft3d_plan_s {
   void* grid = nullptr;      // mx my mz complex128, C order
   afc::NuTileLaunch tiles;   // B = 0: per-point kernels
   int64_t pts_cap = 0;       // points the tile / rank / index buffers hold
+  std::mutex mu;             // one caller enqueues on the grid at a time
+  afc::Fence fence;          // the grid's (and tile buffers') last use on the GPU
   ~afc_nufft3d_plan_s();
 };
 
@@ -1306,6 +1384,39 @@ static afc_status create_plan(afc_plan* out, int rank, const int64_t* dims, afc_
   return AFC_OK;
 }
 
+// The workspace a call on stream st uses (caller holds p.ws_mu): the one st
+// used last; else a new one while the plan has fewer than kWsSlots; else the
+// least recently used one, whose fence orders st after its last use.  Inside a
+// capture nothing is allocated when a workspace exists: the capture takes the
+// most recently used one.
+static afc_status take_ws_slot(afc_plan_s& p, cudaStream_t st, bool cap, WsSlot** out) {
+  for (auto& w : p.ws_slots)
+    if (w->st == st) {
+      *out = w.get();
+      return AFC_OK;
+    }
+  WsSlot* lru = nullptr;
+  WsSlot* mru = nullptr;
+  for (auto& w : p.ws_slots) {
+    if (!lru || w->last < lru->last) lru = w.get();
+    if (!mru || w->last > mru->last) mru = w.get();
+  }
+  if (cap && mru) {
+    *out = mru;
+    return AFC_OK;
+  }
+  if (p.ws_slots.size() < kWsSlots) {
+    std::unique_ptr<WsSlot> w(new WsSlot());
+    AFC_CUDA(dev_alloc(&w->ptr, p.ws_bytes), "workspace");
+    w->st = st;
+    p.ws_slots.push_back(std::move(w));
+    *out = p.ws_slots.back().get();
+    return AFC_OK;
+  }
+  *out = lru;
+  return AFC_OK;
+}
+
 static afc_status execute(afc_plan p, const void* in, void* out, afc_direction dir, double scale, bool use_scale,
                           double pair_w, void* ws, size_t ws_bytes, bool own_ws, void* stream) {
   if (!p) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
@@ -1335,10 +1446,22 @@ static afc_status execute(afc_plan p, const void* in, void* out, afc_direction d
     return AFC_OK;
   }
   if (own_ws) {
+    if (!p->ws_bytes) {  // single-pass plans touch no plan-owned buffer
+      cudaError_t e = run_plan(*p, in, out, inv, sc, pair_w, nullptr, st);
+      if (e != cudaSuccess) return cuda_fail(e, "execute");
+      return AFC_OK;
+    }
     std::lock_guard<std::mutex> lk(p->ws_mu);
-    if (p->ws_bytes && !p->ws) AFC_CUDA(dev_alloc(&p->ws, p->ws_bytes), "workspace");
-    cudaError_t e = run_plan(*p, in, out, inv, sc, pair_w, p->ws, st);
+    const bool cap = stream_capturing(st);
+    WsSlot* w = nullptr;
+    afc_status s = take_ws_slot(*p, st, cap, &w);
+    if (s != AFC_OK) return s;
+    AFC_CUDA(w->fence.before(st, cap), "workspace ordering");
+    cudaError_t e = run_plan(*p, in, out, inv, sc, pair_w, w->ptr, st);
     if (e != cudaSuccess) return cuda_fail(e, "execute");
+    AFC_CUDA(w->fence.after(st, cap), "workspace ordering");
+    w->st = st;
+    w->last = ++p->ws_tick;
     return AFC_OK;
   }
   if (ws_bytes < p->ws_bytes)
@@ -1383,6 +1506,7 @@ struct afc_batch_plan_s {
   };
   std::vector<Phase> phases[2];
   int* counters = nullptr;  // one per phase and direction
+  afc::Fence fence;         // last use of ws / counters on the GPU
   // CUDA graph of the persistent phases, keyed by (in, out, direction)
   cudaGraphExec_t gexec = nullptr;
   const void* g_in = nullptr;
@@ -2127,11 +2251,15 @@ afc_status afc_nufft1d_type1(afc_nufft_plan plan, const double* positions, const
     return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
   DeviceGuard g(plan->device);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::lock_guard<std::mutex> lk(plan->mu);
+  const bool cap = stream_capturing(st);
+  AFC_CUDA(plan->fence.before(st, cap), "NUFFT ordering");
   AFC_CUDA(cudaMemsetAsync(plan->grid, 0, (size_t)plan->m * 16, st), "NUFFT grid");
   AFC_CUDA(nufft_spread_dev(nu_launch(*plan), positions, values, npts, plan->grid, st), "NUFFT spread");
   afc_status s = afc_execute(plan->fft, plan->grid, plan->grid, AFC_FORWARD, stream);
   if (s != AFC_OK) return s;
   AFC_CUDA(nufft_deconv_out_dev(plan->grid, plan->deconv, plan->n, plan->m, out, st), "NUFFT deconvolution");
+  AFC_CUDA(plan->fence.after(st, cap), "NUFFT ordering");
   return AFC_OK;
 }
 
@@ -2143,12 +2271,16 @@ afc_status afc_nufft1d_type2(afc_nufft_plan plan, const void* coeffs, const doub
     return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
   DeviceGuard g(plan->device);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::lock_guard<std::mutex> lk(plan->mu);
+  const bool cap = stream_capturing(st);
+  AFC_CUDA(plan->fence.before(st, cap), "NUFFT ordering");
   AFC_CUDA(cudaMemsetAsync(plan->grid, 0, (size_t)plan->m * 16, st), "NUFFT grid");
   AFC_CUDA(nufft_place_coeffs_dev(coeffs, plan->deconv, plan->n, plan->m, plan->grid, st), "NUFFT coefficients");
   // the reference's normalized inverse times m = the unnormalized inverse
   afc_status s = afc_execute_scaled(plan->fft, plan->grid, plan->grid, AFC_INVERSE, 1.0, stream);
   if (s != AFC_OK) return s;
   AFC_CUDA(nufft_interp_dev(nu_launch(*plan), plan->grid, positions, npts, out, st), "NUFFT interpolation");
+  AFC_CUDA(plan->fence.after(st, cap), "NUFFT ordering");
   return AFC_OK;
 }
 
@@ -2266,6 +2398,9 @@ afc_status afc_nufft3d_type1(afc_nufft3d_plan plan, const double* positions, con
     return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
   DeviceGuard g(plan->device);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::lock_guard<std::mutex> lk(plan->mu);
+  const bool cap = stream_capturing(st);
+  AFC_CUDA(plan->fence.before(st, cap), "NUFFT ordering");
   const NuLaunch3 L = nu_launch3(*plan);
   AFC_CUDA(cudaMemsetAsync(plan->grid, 0, (size_t)(L.mx * L.my * L.mz) * 16, st), "NUFFT grid");
   bool tiled = false;
@@ -2279,6 +2414,7 @@ afc_status afc_nufft3d_type1(afc_nufft3d_plan plan, const double* positions, con
   if (s != AFC_OK) return s;
   const double* dc = plan->deconv;
   AFC_CUDA(nufft3_modes_dev(L, dc, dc + L.nx, dc + L.nx + L.ny, plan->grid, out, false, st), "NUFFT deconvolution");
+  AFC_CUDA(plan->fence.after(st, cap), "NUFFT ordering");
   return AFC_OK;
 }
 
@@ -2290,6 +2426,9 @@ afc_status afc_nufft3d_type2(afc_nufft3d_plan plan, const void* modes, const dou
     return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
   DeviceGuard g(plan->device);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::lock_guard<std::mutex> lk(plan->mu);
+  const bool cap = stream_capturing(st);
+  AFC_CUDA(plan->fence.before(st, cap), "NUFFT ordering");
   const NuLaunch3 L = nu_launch3(*plan);
   AFC_CUDA(cudaMemsetAsync(plan->grid, 0, (size_t)(L.mx * L.my * L.mz) * 16, st), "NUFFT grid");
   const double* dc = plan->deconv;
@@ -2304,6 +2443,7 @@ afc_status afc_nufft3d_type2(afc_nufft3d_plan plan, const void* modes, const dou
     AFC_CUDA(nufft3_tiled_dev(L, plan->tiles, false, positions, plan->grid, npts, out, st), "NUFFT interpolation");
   else
     AFC_CUDA(nufft3_interp_dev(L, plan->grid, positions, npts, out, st), "NUFFT interpolation");
+  AFC_CUDA(plan->fence.after(st, cap), "NUFFT ordering");
   return AFC_OK;
 }
 
@@ -2343,17 +2483,48 @@ afc_status afc_execute_host(afc_plan plan, const void* host_in, void* host_out, 
   const size_t ib = (size_t)ie * (real_in ? rsz : csz), ob = (size_t)oe * (real_out ? rsz : csz);
   const size_t maxb = (size_t)std::max(ie, oe) * csz;
   DeviceGuard g(plan->device);
+  // Take a free staging set (own stream, own buffers), creating one while the
+  // plan has fewer than kHostStages; otherwise wait until a call returns one.
+  // Concurrent host threads on one shared plan thus never share a buffer.
+  HostStage* hs = nullptr;
   {
-    std::lock_guard<std::mutex> lk(plan->ws_mu);
-    if (!plan->host_stream) AFC_CUDA(cudaStreamCreateWithFlags(&plan->host_stream, cudaStreamNonBlocking), "stream");
-    if (!plan->host_in) AFC_CUDA(dev_alloc(&plan->host_in, maxb), "staging");
-    if (!plan->host_out) AFC_CUDA(dev_alloc(&plan->host_out, maxb), "staging");
+    std::unique_lock<std::mutex> lk(plan->host_mu);
+    for (;;) {
+      for (auto& s : plan->stages)
+        if (!s->busy) {
+          hs = s.get();
+          break;
+        }
+      if (hs || plan->stages.size() < kHostStages) break;
+      plan->host_cv.wait(lk);
+    }
+    if (!hs) {
+      std::unique_ptr<HostStage> ns(new HostStage());
+      AFC_CUDA(cudaStreamCreateWithFlags(&ns->st, cudaStreamNonBlocking), "stream");
+      AFC_CUDA(dev_alloc(&ns->in, maxb), "staging");
+      AFC_CUDA(dev_alloc(&ns->out, maxb), "staging");
+      plan->stages.push_back(std::move(ns));
+      hs = plan->stages.back().get();
+    }
+    hs->busy = true;
   }
-  cudaStream_t st = plan->host_stream;
-  AFC_CUDA(cudaMemcpyAsync(plan->host_in, host_in, ib, cudaMemcpyHostToDevice, st), "host to device");
-  afc_status s = afc_execute(plan, plan->host_in, plan->host_out, direction, st);
-  if (s != AFC_OK) return s;
-  AFC_CUDA(cudaMemcpyAsync(host_out, plan->host_out, ob, cudaMemcpyDeviceToHost, st), "device to host");
+  struct Release {
+    afc_plan p;
+    HostStage* s;
+    ~Release() {
+      std::lock_guard<std::mutex> lk(p->host_mu);
+      s->busy = false;
+      p->host_cv.notify_one();
+    }
+  } release{plan, hs};
+  cudaStream_t st = hs->st;
+  AFC_CUDA(cudaMemcpyAsync(hs->in, host_in, ib, cudaMemcpyHostToDevice, st), "host to device");
+  afc_status s = afc_execute(plan, hs->in, hs->out, direction, st);
+  if (s != AFC_OK) {
+    cudaStreamSynchronize(st);  // the staging set goes back idle
+    return s;
+  }
+  AFC_CUDA(cudaMemcpyAsync(host_out, hs->out, ob, cudaMemcpyDeviceToHost, st), "device to host");
   AFC_CUDA(cudaStreamSynchronize(st), "synchronize");
   return AFC_OK;
 }
@@ -2582,14 +2753,19 @@ afc_status afc_batch_execute(afc_batch_plan plan, const void* in, void* out, afc
   DeviceGuard g(plan->device);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   std::lock_guard<std::mutex> lk(plan->mu);
+  // the plan-owned workspace and tile counters: ordered after their last use
+  const bool cap = stream_capturing(st);
+  AFC_CUDA(plan->fence.before(st, cap), "batch ordering");
   if (mode == 1) {
     cudaError_t e = run_batch(*plan, in, out, inv, st);
     if (e != cudaSuccess) return cuda_fail(e, "batch execute");
+    AFC_CUDA(plan->fence.after(st, cap), "batch ordering");
     return AFC_OK;
   }
   if (mode == 2) {  // persistent phases without the graph
     cudaError_t e = run_batch_persistent(*plan, in, out, inv, st);
     if (e != cudaSuccess) return cuda_fail(e, "batch execute");
+    AFC_CUDA(plan->fence.after(st, cap), "batch ordering");
     return AFC_OK;
   }
   // mode 0: the persistent phases as one CUDA graph, captured once per (in, out, direction)
@@ -2613,6 +2789,7 @@ afc_status afc_batch_execute(afc_batch_plan plan, const void* in, void* out, afc
     plan->g_dir = (int)direction;
   }
   AFC_CUDA(cudaGraphLaunch(plan->gexec, st), "batch graph launch");
+  AFC_CUDA(plan->fence.after(st, cap), "batch ordering");
   return AFC_OK;
 }
 

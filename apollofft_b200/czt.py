@@ -11,6 +11,7 @@ from __future__ import annotations
 import ctypes
 
 from . import _lib as L
+from .plan import require_device
 
 
 class CztError(ValueError):
@@ -55,11 +56,13 @@ class CztPlan:
         cdt = torch.complex128 if self.precision == "f64" else torch.complex64
         if x.dtype != cdt or not x.is_contiguous() or x.shape[-1] != self.n or not x.is_cuda:
             raise ValueError(f"expected a contiguous {cdt} tensor with last dimension {self.n}")
+        require_device(x, self.device, "input")
         batch = x.numel() // self.n
         if out is None:
             out = torch.empty(tuple(x.shape[:-1]) + (self.m,), dtype=cdt, device=x.device)
         if out.dtype != cdt or not out.is_contiguous() or out.numel() != batch * self.m or not out.is_cuda:
             raise ValueError("output buffer does not match the plan")
+        require_device(out, self.device, "output")
         st = stream if stream is not None else torch.cuda.current_stream(x.device).cuda_stream
         L.check(L.lib().afc_czt_execute(self._h, x.data_ptr(), out.data_ptr(), batch, st), "czt execute")
         return out

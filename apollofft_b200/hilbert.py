@@ -14,6 +14,7 @@ from __future__ import annotations
 import ctypes
 
 from . import _lib as L
+from .plan import require_device
 
 _PREC = {"f32": L.PREC_F32, "f64": L.PREC_F64}
 
@@ -36,11 +37,13 @@ class HilbertPlan:
         ct = torch.complex128 if self.precision == "f64" else torch.complex64
         if x.dtype != rt or not x.is_contiguous() or x.dim() < 1 or x.shape[-1] != self.n or not x.is_cuda:
             raise ValueError(f"signal: expected a contiguous {rt} tensor whose last dimension is {self.n}")
+        require_device(x, self.device, "signal")
         lanes = x.numel() // self.n
         if out is None:
             out = torch.empty(x.shape, dtype=ct, device=x.device)
         if out.dtype != ct or not out.is_contiguous() or out.numel() != x.numel() or not out.is_cuda:
             raise ValueError("output buffer does not match the signal")
+        require_device(out, self.device, "output")
         if lanes == 0:
             return out
         st = stream if stream is not None else torch.cuda.current_stream(x.device).cuda_stream

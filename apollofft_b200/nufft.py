@@ -22,6 +22,7 @@ from __future__ import annotations
 import ctypes
 
 from . import _lib as L
+from .plan import require_device
 
 DEFAULT_NUFFT_KERNEL_WIDTH = 6
 DEFAULT_NUFFT_OVERSAMPLING = 2
@@ -37,10 +38,10 @@ class NufftPlan1D:
         L.check(L.lib().afc_nufft1d_plan_create(ctypes.byref(self._h), self.n, self.dx, self.sigma,
                                                 self.kernel_width, self.device), "nufft plan")
 
-    @staticmethod
-    def _check(t, dtype, what):
+    def _check(self, t, dtype, what):
         if t.dtype != dtype or not t.is_contiguous() or t.dim() != 1 or not t.is_cuda:
             raise ValueError(f"{what}: expected a contiguous 1D {dtype} tensor")
+        require_device(t, self.device, what)
 
     def type1(self, positions, values, out=None, stream=None):
         import torch
@@ -101,10 +102,10 @@ class NufftPlan3D:
         L.check(L.lib().afc_nufft3d_grid_dims(self._h, m), "nufft3d grid dims")
         self.oversampled = tuple(int(v) for v in m)
 
-    @staticmethod
-    def _check(t, dtype, what, shape=None):
+    def _check(self, t, dtype, what, shape=None):
         if t.dtype != dtype or not t.is_contiguous() or not t.is_cuda:
             raise ValueError(f"{what}: expected a contiguous {dtype} tensor")
+        require_device(t, self.device, what)
         if shape is not None and tuple(t.shape) != tuple(shape):
             raise ValueError(f"{what}: expected shape {tuple(shape)}, got {tuple(t.shape)}")
 

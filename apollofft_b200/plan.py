@@ -115,12 +115,16 @@ class CudaPlan:
             raise ValueError(f"shape mismatch: expected {ie} elements, got {x.numel()}")
         if not x.is_cuda:
             raise ValueError("input must be a CUDA tensor (use execute_host for host arrays)")
+        if x.get_device() != self.device:
+            require_device(x, self.device, "input")
         if out is None:
             import torch
             out = torch.empty(self.out_shape(inverse) if oe == int(np.prod(self.out_shape(inverse))) else (oe,),
                               dtype=t_out, device=x.device)
         if out.numel() != oe or out.dtype != t_out or not out.is_contiguous() or not out.is_cuda:
             raise ValueError("output buffer does not match the plan")
+        if out.get_device() != self.device:
+            require_device(out, self.device, "output")
         st = stream if stream is not None else _stream_of(x)
         if scale is None:
             status = self._exec(self._h, x.data_ptr(), out.data_ptr(), 1 if inverse else 0, st)
@@ -139,6 +143,7 @@ class CudaPlan:
         t_out = _TORCH_DTYPES[np.dtype(self.in_dtype(inverse))]
         ie, oe = self.io_elems(inverse)
         g = g.to(t_in).contiguous()
+        require_device(g, self.device, "gradient")
         if g.numel() != oe:
             raise ValueError(f"shape mismatch: expected {oe} elements, got {g.numel()}")
         out = torch.empty((ie,), dtype=t_out, device=g.device)
@@ -170,6 +175,16 @@ class CudaPlan:
             self.close()
         except Exception:
             pass
+
+
+def require_device(t, device: int, what: str) -> None:
+    """Raises ValueError unless torch tensor `t` lives on CUDA device `device`
+    (the plan's): the kernels run on the plan's device, so a pointer into host
+    memory or into another GPU's memory must never reach them."""
+    d = t.get_device()
+    if d != device:
+        where = "host memory" if d < 0 else f"cuda:{d}"
+        raise ValueError(f"{what} is in {where}; the plan is on cuda:{device}")
 
 
 _RAW_STREAM = None

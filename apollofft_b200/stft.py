@@ -17,7 +17,7 @@ import math
 import numpy as np
 
 from . import _lib as L
-from .plan import CudaPlan
+from .plan import CudaPlan, require_device
 
 
 class StftError(ValueError):
@@ -73,6 +73,7 @@ class StftPlan:
         rdt = self._real_dtype()
         if signal.dtype != rdt or signal.dim() != 1 or not signal.is_contiguous() or not signal.is_cuda:
             raise ValueError(f"expected a contiguous 1D {rdt} signal")
+        require_device(signal, self.device, "signal")
         if signal.numel() < self.frame_len:
             raise StftError("input signal shorter than frame length")
         if window is None:
@@ -89,6 +90,7 @@ class StftPlan:
             out = torch.empty((frames, self.frame_len), dtype=cdt, device=signal.device)
         if out.dtype != cdt or not out.is_contiguous() or not out.is_cuda:
             raise ValueError("output buffer does not match the plan")
+        require_device(out, self.device, "output")
         st = stream if stream is not None else torch.cuda.current_stream(signal.device).cuda_stream
         L.check(L.lib().afc_stft_forward(self.plan._h, signal.data_ptr(), signal.numel(), win.data_ptr(),
                                          self.hop_len, out.data_ptr(), out.numel(), st), "stft forward")
@@ -102,6 +104,7 @@ class StftPlan:
         cdt = torch.complex128 if rdt == torch.float64 else torch.complex64
         if spectrum.dtype != cdt or not spectrum.is_contiguous() or not spectrum.is_cuda:
             raise ValueError(f"expected a contiguous {cdt} spectrum")
+        require_device(spectrum, self.device, "spectrum")
         if signal_len < self.frame_len:
             raise StftError("input signal shorter than frame length")
         frames = self.frame_count(signal_len)
@@ -123,6 +126,7 @@ class StftPlan:
             out = torch.empty(int(signal_len), dtype=rdt, device=spectrum.device)
         if out.dtype != rdt or not out.is_contiguous() or out.numel() != int(signal_len) or not out.is_cuda:
             raise ValueError("output buffer does not match the signal length")
+        require_device(out, self.device, "output")
         st = stream if stream is not None else torch.cuda.current_stream(spectrum.device).cuda_stream
         L.check(L.lib().afc_stft_inverse(self.plan._h, spectrum.data_ptr(), spectrum.numel(), win.data_ptr(),
                                          self.hop_len, out.data_ptr(), int(signal_len), ws.data_ptr(),

@@ -2,23 +2,30 @@
 
 Workload (the headline): 256 x 256 x 256 complex128 (f64 high_accuracy plan),
 entries i.i.d. standard normal re/im from a seed, forward then normalized
-inverse per step.  The other shapes/dtypes of the same configuration
-(243x250x343, complex64) are measured in the same run and reported under
-"also".  Inputs (268 MB) exceed the 126 MB L2, so no flush is needed between
-steps.
+inverse per step.  Inputs (268 MB) exceed the 126 MB L2, so no flush is needed
+between steps.  Every other measured configuration is timed in the same run and
+reported under "also", each with its error against the oracle: the other C2
+shapes and dtypes (243x250x343, complex64), C1 (64 x 4096 f64), C3 (4096
+uneven complex64 lengths), C4 (16384 x 4096 complex64: FP32 and the
+split-precision tensor-core forms) and C5 (8 x 2048^2 real f32 with gradient).
 
 value        : whole-job GFLOP/s, 5 N log2 N per transform, two transforms per step,
                data already in HBM, CUDA events on the launching stream.
+roofline     : algorithmic bytes (2 N sizeof(complex) per transform; intermediate
+               passes not counted) over the measured time, against the measured
+               copy bandwidth in MEASURED_PEAKS.json.  Per launch this is the
+               transform's bytes split over its launches; `per_pass_frac` is the
+               separate figure of one pass's own read + write of the volume.
 e2e          : the same metric through afc_execute_host (the reference-facing slice
-               API) from pinned host buffers, copies inside the timed region.
-roofline     : the dominant kernel (tma_kernel, every launch of the step): bytes a
-               launch moves algorithmically (read + write of the volume it
-               transforms) / its average duration, against MEASURED_PEAKS.json.
+               API) from pinned host buffers, copies inside the timed region; the
+               measured pinned copy bandwidth of the host link is reported beside it.
 cpu_baseline : the oracle's restatement of the reference CPU plan (FftPlan3D<f64>),
                all host threads, one forward+inverse of the same volume.
 
---impl reference times that CPU path alone on the same config.
-Multi-GPU: replicas only (one transform per rank, no collective on the data path).
+--impl reference times that CPU path alone on the same config, with a live
+calibration of the restatement against the reference's published single-thread
+latencies.  Multi-GPU: replicas only (one transform per rank, no collective on
+the data path).
 """
 from __future__ import annotations
 
@@ -38,6 +45,12 @@ sys.path.insert(0, ROOT)
 
 SHAPE = (256, 256, 256)
 ALSO = [((243, 250, 343), "f64"), ((256, 256, 256), "f32"), ((243, 250, 343), "f32")]
+# the reference's published single-thread forward latencies (ns) of its 1D plans:
+# benchmark_results.md:74,138,211,212 (criterion, clone-inclusive) and the
+# checklist.md:1689-1699 / 1622-1624 dev-log N=4096 figures
+PUBLISHED_NS = {("f64", 64): 147.20, ("f64", 128): 322.56, ("f64", 4096): 15844.0, ("f64", 10007): 494364.58,
+                ("f64", 32768): 185739.87, ("f32", 64): 97.97, ("f32", 128): 177.00, ("f32", 4096): 5429.8,
+                ("f32", 10007): 365107.41, ("f32", 32768): 134409.78}
 METRIC = "FFT GFLOP/s (5N log2N) and % HBM roofline vs plain FP32, at stated FP64-oracle error"
 
 
@@ -202,11 +215,28 @@ class ClockSampler:
                 "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
 
 
-def cpu_transform_gflops(shape, reps, threads=0, want_output=False):
-    """Oracle FftPlan3D<f64> forward + inverse on host cores; returns GFLOP/s."""
+def c2_input(shape, seed=2):
+    """re/im i.i.d. N(0,1) from a seed (the C2 configuration's input)."""
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+def c2_config(shape, prec, world):
+    """The config dict both arms print (same keys and values)."""
+    nbytes = int(np.prod(shape)) * (16 if prec == "f64" else 8)
+    return {"workload": f"3D C2C {'x'.join(map(str, shape))} {'complex128' if prec == 'f64' else 'complex64'}"
+                        " forward+inverse (1/N)", "shape": list(shape),
+            "precision": "f64 high_accuracy" if prec == "f64" else "f32 low_precision",
+            "parallelism": f"replicas x{world}",
+            "l2": f"inputs ({nbytes / 1e6:.0f} MB) larger than L2; no flush"}
+
+
+def cpu_transform_gflops(shape, reps, threads=0, x=None):
+    """Oracle FftPlan3D<f64> forward + inverse on host cores.  Returns
+    (GFLOP/s, seconds, forward output of the last rep)."""
     from oracle import oracle as O
-    rng = np.random.default_rng(2)
-    x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    if x is None:
+        x = c2_input(shape)
     O.fft3d(np.zeros((4, 4, 4), dtype=np.complex128))  # load + warm caches
     t0 = time.perf_counter()
     y = None
@@ -214,21 +244,48 @@ def cpu_transform_gflops(shape, reps, threads=0, want_output=False):
         y = O.fft3d(x, threads=threads)
         O.fft3d(y, inverse=True, threads=threads)
     dt = time.perf_counter() - t0
-    g = reps * 2 * flops_per_transform(shape) / dt / 1e9
-    return (g, dt, x, y) if want_output else (g, dt)
+    return reps * 2 * flops_per_transform(shape) / dt / 1e9, dt, y
+
+
+def port_calibration():
+    """The oracle port on ONE host thread against the reference's published
+    single-thread forward latencies (same lengths and precisions).  factor =
+    port time / published time; > 1 means the port is slower than the
+    reference, so CPU ratios against the port overstate the GPU's lead by
+    about that factor.  Bounded: well under a second of CPU work."""
+    from oracle import oracle as O
+    rows = []
+    for (prec, n), pub_ns in sorted(PUBLISHED_NS.items()):
+        dt = np.complex128 if prec == "f64" else np.complex64
+        lanes = max(1, min(2048, (1 << 18) // n))
+        rng = np.random.default_rng(n)
+        x = (rng.uniform(-1, 1, (lanes, n)) + 1j * rng.uniform(-1, 1, (lanes, n))).astype(dt)
+        O.fft1d(x[:1], threads=1)
+        best = float("inf")
+        for _ in range(3):
+            t0 = time.perf_counter()
+            O.fft1d(x, threads=1)
+            best = min(best, (time.perf_counter() - t0) / lanes)
+        rows.append({"precision": prec, "n": n, "port_ns": round(best * 1e9, 1), "published_ns": pub_ns,
+                     "factor": round(best * 1e9 / pub_ns, 3)})
+    gm = float(np.exp(np.mean([np.log(r["factor"]) for r in rows])))
+    return {"factor_geomean": round(gm, 3), "rows": rows,
+            "note": "oracle port, one thread, per-transform time over a batch of lanes; published = reference "
+                    "benchmark_results.md (criterion, clone-inclusive) and checklist.md dev-log N=4096"}
 
 
 def run_reference(args):
-    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    world, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     from oracle import oracle as O
     threads = O.max_threads()
+    x = c2_input(SHAPE)
     vals = []
     for _ in range(args.warmup):
-        cpu_transform_gflops(SHAPE, 1)
+        cpu_transform_gflops(SHAPE, 1, x=x)
     for _ in range(args.steps):
-        g, _ = cpu_transform_gflops(SHAPE, 1)
+        g, _, _ = cpu_transform_gflops(SHAPE, 1, x=x)
         vals.append(g)
     v = float(np.mean(vals))
     step_s = 2 * flops_per_transform(SHAPE) / (v * 1e9)
@@ -236,11 +293,11 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "GFLOP/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_s * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1) re/im)",
-        "config": {"workload": "3D C2C 256x256x256 complex128 forward+inverse (1/N)", "shape": list(SHAPE),
-                   "precision": "f64 high_accuracy", "l2": "inputs larger than L2"},
+        "config": c2_config(SHAPE, "f64", args.gpus),
         "cpu_baseline": {"value": round(v, 3), "unit": "GFLOP/s", "cores": threads, "kind": "port",
                          "sample": "one forward+inverse of the 256^3 complex128 volume per step (oracle FftPlan3D<f64>)"},
         "e2e": {"value": round(v, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "port_calibration": port_calibration(),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -263,6 +320,21 @@ def time_device(plan, x, y, steps, warmup, torch):
     return e0.elapsed_time(e1) / 1e3 / steps
 
 
+def link_bandwidth(torch, nbytes, dev):
+    """Pinned host <-> device copy bandwidth (GB/s) of one nbytes copy each way."""
+    h = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    out = {}
+    for name, fn in (("h2d_gbs", lambda: d.copy_(h, non_blocking=True)),
+                     ("d2h_gbs", lambda: h.copy_(d, non_blocking=True))):
+        fn()
+        torch.cuda.synchronize()
+        t = _events_time(fn, 3, 1, torch)
+        out[name] = round(nbytes / t / 1e9, 1)
+    del h, d
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -272,12 +344,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--shape", default=None, help="override the 3D shape, e.g. 128,256,256 (profiling cases)")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
-    ap.add_argument("--quick", action="store_true", help="headline only: no other shapes, e2e or CPU legs")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "stft", "czt", "nufft", "nufft3d", "hilbert"],
-                    help="c2 (default) is the headline; c1/c3/c4/c5 print their own lines")
+    ap.add_argument("--quick", action="store_true", help="headline only: no other configurations, e2e or CPU legs")
+    ap.add_argument("--workload", default="c2",
+                    choices=["c1", "c2", "c3", "c4", "c5", "calib", "stft", "czt", "nufft", "nufft3d", "hilbert"],
+                    help="c2 (default) is the headline; the others print their own lines")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "calib":
+        print(json.dumps({"workload": "calib", "port_calibration": port_calibration()}), flush=True)
+        return 0
     if args.workload != "c2":
         return run_secondary(args)
 
@@ -294,16 +370,14 @@ def main():
     dev = torch.device("cuda", local)
     hbm_peak, peak_kind = load_peaks()
 
-    g = torch.Generator(device=dev).manual_seed(2 + rank)
-    x = torch.randn(SHAPE, dtype=cdt, device=dev, generator=g)
+    x_host = c2_input(SHAPE, seed=2 + rank)
+    x = torch.from_numpy(x_host).to(dev, cdt)
     x0 = x.clone()
     y = torch.empty_like(x)
     plan = afc.CudaPlan(list(SHAPE), precision=prec, device=local)
-    launches_per_transform = len(SHAPE)
 
     barrier(world)
     torch.cuda.synchronize()
-    n0 = afc.kernel_launch_count()
     with ClockSampler(local) as clk:
         for _ in range(args.warmup):
             plan.execute(x, out=y)
@@ -325,54 +399,64 @@ def main():
         n2 = afc.kernel_launch_count()
     t_step_max = max_over_ranks(t_step, world, dev)
     launches = n2 - n1
+    launches_per_step = launches / args.steps
     roundtrip_err = (torch.linalg.vector_norm(x - x0) / torch.linalg.vector_norm(x0)).item()
+    del x0
 
     flops_step = 2 * flops_per_transform(SHAPE)
     value = world * flops_step / t_step_max / 1e9
-    vol_bytes = bytes_per_transform(SHAPE, prec)  # read + write of the volume
-    launches_per_step = 2 * launches_per_transform
-    t_launch = t_step / launches_per_step
-    achieved = vol_bytes / t_launch / 1e9
-    transform_frac = (2 * vol_bytes / t_step / 1e9) / hbm_peak
+    vol_bytes = bytes_per_transform(SHAPE, prec)  # algorithmic: read + write of the volume, per transform
+    achieved = 2 * vol_bytes / t_step / 1e9     # = per launch: the transform's bytes over its launches
+    per_pass = vol_bytes / (t_step / launches_per_step) / 1e9  # one launch's own read + write of the volume
 
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "tma_kernel_traffic.json")
-    if os.path.exists(tf):
-        try:
-            traffic = (json.load(open(tf)).get("bytes_per_launch_256cube_f64")
-                       if SHAPE == (256, 256, 256) and prec == "f64" else None)
-        except (ValueError, OSError):
-            traffic = None
+    # error of the headline forward against the oracle (rank 0): same host input
+    err_oracle = None
+    cpu = None
+    ref_fwd = None
+    if rank == 0 and world == 1 and not args.no_cpu and not args.quick and prec == "f64":
+        from oracle import oracle as O
+        gcpu, _, ref_fwd = cpu_transform_gflops(SHAPE, 1, x=x_host)
+        cpu = {"value": round(gcpu, 3), "unit": "GFLOP/s", "cores": O.max_threads(), "kind": "port",
+               "sample": "one forward+inverse of the 256^3 complex128 volume (oracle FftPlan3D<f64>, all threads)"}
+        yt = plan.execute(torch.from_numpy(x_host).to(dev)).cpu().numpy()
+        err_oracle = float(np.linalg.norm(yt - ref_fwd) / np.linalg.norm(ref_fwd))
+        del yt
 
-    # other shapes / dtypes of the configuration
+    # other shapes / dtypes of the configuration, each against the oracle
     also = []
     del y
-    for shp, prec in ([] if args.quick else ALSO):
-        dt = torch.complex128 if prec == "f64" else torch.complex64
-        xa = torch.randn(shp, dtype=dt, device=dev, generator=g)
+    with_oracle = rank == 0 and world == 1 and not args.no_cpu
+    for shp, pa_prec in ([] if args.quick else ALSO):
+        dt = torch.complex128 if pa_prec == "f64" else torch.complex64
+        xh = c2_input(shp, seed=2)
+        xa = torch.from_numpy(xh).to(dev, dt)
         ya = torch.empty_like(xa)
-        pa = afc.CudaPlan(list(shp), precision=prec, device=local)
+        pa = afc.CudaPlan(list(shp), precision=pa_prec, device=local)
         ts = time_device(pa, xa, ya, max(3, args.steps // 2), args.warmup, torch)
         err = None
-        if prec == "f32":
-            ref = afc.CudaPlan(list(shp), precision="f64", device=local).execute(xa.to(torch.complex128))
-            out = pa.execute(xa)
-            err = (torch.linalg.vector_norm(out.to(torch.complex128) - ref) / torch.linalg.vector_norm(ref)).item()
-            del ref, out
-        also.append({"shape": list(shp), "precision": prec, "ms_per_step": round(ts * 1e3, 4),
+        if with_oracle:
+            from oracle import oracle as O
+            ref = ref_fwd if (shp == SHAPE and ref_fwd is not None) else O.fft3d(xh)
+            out = pa.execute(torch.from_numpy(xh).to(dev, dt)).cpu().numpy()
+            err = float(np.linalg.norm(out - ref) / np.linalg.norm(ref))
+            del out, ref
+        also.append({"config": "C2", "shape": list(shp), "precision": pa_prec, "ms_per_step": round(ts * 1e3, 4),
                      "gflops": round(2 * flops_per_transform(shp) / ts / 1e9, 2),
-                     "transform_hbm_frac": round((2 * bytes_per_transform(shp, prec) / ts / 1e9) / hbm_peak, 4),
-                     "rel_l2_vs_f64_path": err})
+                     "hbm_frac": round((2 * bytes_per_transform(shp, pa_prec) / ts / 1e9) / hbm_peak, 4),
+                     "rel_l2_vs_oracle": err})
         del xa, ya, pa
         torch.cuda.empty_cache()
+    if not args.quick:
+        steps2 = max(3, args.steps // 2)
+        for fn in (c1_entry, c3_entry, c4_entry, c5_entry):
+            also.append(fn(afc, torch, dev, steps2, args.warmup, hbm_peak, with_oracle))
+            torch.cuda.empty_cache()
 
-    prec = args.precision
     # end to end through the host-pointer C-ABI call, pinned buffers
-    hx = torch.randn(SHAPE, dtype=cdt, generator=torch.Generator().manual_seed(2)).pin_memory()
+    hx = torch.from_numpy(x_host.astype(np.complex128 if prec == "f64" else np.complex64)).pin_memory()
     hy = torch.empty_like(hx).pin_memory()
     hz = torch.empty_like(hx).pin_memory()
     xn, yn, zn = hx.numpy(), hy.numpy(), hz.numpy()
-    import ctypes
     L = afc._lib.lib()
     for _ in range(2):
         afc._lib.check(L.afc_execute_host(plan._h, xn.ctypes.data, yn.ctypes.data, 0))
@@ -386,41 +470,35 @@ def main():
     t_e2e = (time.perf_counter() - t0) / max(e2e_steps, 1)
     t_e2e = max_over_ranks(t_e2e, world, dev)
     e2e_val = world * flops_step / t_e2e / 1e9
-
-    # CPU baseline (rank 0, N = 1 only) and the error against the f64 oracle
-    cpu = None
-    err_oracle = None
-    if rank == 0 and world == 1 and not args.no_cpu and not args.quick and prec == "f64":
-        from oracle import oracle as O
-        gcpu, dt, xin, yref = cpu_transform_gflops(SHAPE, 1, want_output=True)
-        cpu = {"value": round(gcpu, 3), "unit": "GFLOP/s", "cores": O.max_threads(), "kind": "port",
-               "sample": "one forward+inverse of the 256^3 complex128 volume (oracle FftPlan3D<f64>, all threads)"}
-        xt = torch.from_numpy(xin).to(dev)
-        yt = plan.execute(xt).cpu().numpy()
-        err_oracle = float(np.linalg.norm(yt - yref) / np.linalg.norm(yref))
+    link = None if args.quick else link_bandwidth(torch, int(vol_bytes // 2), dev)
+    del hx, hy, hz
 
     if rank == 0:
+        io_bytes = int(2 * (16 if prec == "f64" else 8) * np.prod(SHAPE))
+        e2e = None
+        if not args.quick:
+            # each afc_execute_host call copies the volume in and out, serialized
+            bound_s = (io_bytes / 2) / (link["h2d_gbs"] * 1e9) + (io_bytes / 2) / (link["d2h_gbs"] * 1e9)
+            e2e = {"value": round(e2e_val, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": io_bytes,
+                   "d2h_bytes_per_step": io_bytes, "link": link,
+                   "copy_bound_gflops": round(flops_step / (2 * bound_s) / 1e9, 1)}
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t_step_max * 1e3, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": prec, "data": "synthetic (seeded N(0,1) re/im)",
-            "config": {"workload": f"3D C2C {'x'.join(map(str, SHAPE))} {'complex128' if prec == 'f64' else 'complex64'}"
-                                   " forward+inverse (1/N)", "shape": list(SHAPE),
-                       "precision": "f64 high_accuracy" if prec == "f64" else "f32 low_precision",
-                       "parallelism": f"replicas x{world}",
-                       "l2": "inputs (268 MB) larger than L2; no flush"},
+            "config": c2_config(SHAPE, prec, world),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                         "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
-                         "kernel": f"tma_kernel<{'double' if prec == 'f64' else 'float'}> (all launches of the step)",
+                         "frac": round(achieved / hbm_peak, 4), "traffic": None,
+                         "traffic_source": "DRAM bytes per launch: ncu capture summarized in profiles/ "
+                                           "(not measured inside this run)",
+                         "kernel": f"all launches of the step ({launches_per_step:.0f} per step)",
+                         "bytes_definition": "2 N sizeof(complex) per transform, intermediate passes not counted",
+                         "per_pass_frac": round(per_pass / hbm_peak, 4),
                          "peak_source": peak_kind},
-            "transform_hbm_frac": round(transform_frac, 4),
             "error_vs_oracle_rel_l2": err_oracle,
             "roundtrip_rel_l2": roundtrip_err,
             "cpu_baseline": cpu,
-            "e2e": None if args.quick else {
-                "value": round(e2e_val, 3), "unit": "GFLOP/s",
-                "h2d_bytes_per_step": int(2 * (16 if prec == "f64" else 8) * np.prod(SHAPE)),
-                "d2h_bytes_per_step": int(2 * (16 if prec == "f64" else 8) * np.prod(SHAPE))},
+            "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "also": also,
@@ -447,6 +525,155 @@ def _events_time(fn, steps, warmup, torch):
     return e0.elapsed_time(e1) / 1e3 / steps
 
 
+def c1_entry(afc, torch, dev, steps, warmup, hbm_peak, with_oracle):
+    """C1: 64 x 4096 complex128, forward + inverse per step (U[-1, 1), seed 1)."""
+    from apollofft_b200 import workloads as W
+    xin = W.c1_input()
+    x = torch.from_numpy(xin).to(dev)
+    y = torch.empty_like(x)
+    p = afc.CudaPlan([4096], precision="f64", batch=64)
+    t = _events_time(lambda: (p.execute(x, out=y), p.execute(y, out=x, inverse=True)), steps, warmup, torch)
+    fl = 2 * 64 * 5 * 4096 * 12
+    out = {"config": "C1", "workload": "1D C2C f64 N=4096 x64 fwd+inv", "us_per_step": round(t * 1e6, 2),
+           "gflops": round(fl / t / 1e9, 2), "hbm_frac": round(2 * 2 * 64 * 4096 * 16 / t / 1e9 / hbm_peak, 4)}
+    # the same two calls replayed from a CUDA graph: device time without per-call host work
+    try:
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            for _ in range(3):
+                p.execute(x, out=y)
+                p.execute(y, out=x, inverse=True)
+        torch.cuda.current_stream().wait_stream(side)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            p.execute(x, out=y)
+            p.execute(y, out=x, inverse=True)
+        tg = _events_time(g.replay, steps, warmup, torch)
+        out["graph_us_per_step"] = round(tg * 1e6, 2)
+        out["graph_hbm_frac"] = round(2 * 2 * 64 * 4096 * 16 / tg / 1e9 / hbm_peak, 4)
+        del g
+    except Exception as exc:  # capture refused: report the host-driven figure only
+        out["graph_us_per_step"] = None
+        out["graph_error"] = str(exc)[:200]
+    if with_oracle:
+        from oracle import oracle as O
+        ref = O.fft1d(xin)
+        got = p.execute(torch.from_numpy(xin).to(dev)).cpu().numpy()
+        out["rel_l2_vs_oracle"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    return out
+
+
+def c3_entry(afc, torch, dev, steps, warmup, hbm_peak, with_oracle):
+    """C3: 4096 uneven complex64 lengths in one persistent launch per phase (CUDA graph)."""
+    from apollofft_b200 import workloads as W
+    lens = W.c3_lengths()
+    xv = W.c3_values(lens)
+    x = torch.from_numpy(xv).to(dev)
+    t0 = time.perf_counter()
+    bp = afc.BatchPlan(lens, precision="f32")
+    plan_s = time.perf_counter() - t0
+    y = torch.empty_like(x)
+    fl = float(np.sum(5.0 * lens * np.log2(lens)))
+    by = float(np.sum(2.0 * lens * 8))
+    t = _events_time(lambda: bp.execute(x, out=y, mode=0), steps, warmup, torch)
+    tp = _events_time(lambda: bp.execute(x, out=y, mode=1), 2, 1, torch)
+    out = {"config": "C3", "workload": "4096 uneven 1D complex64 lengths log-uniform [64, 65536], thirds "
+                                       "pow2/7-smooth/prime, forward", "us": round(t * 1e6, 1),
+           "gflops": round(fl / t / 1e9, 1), "hbm_frac": round(by / t / 1e9 / hbm_peak, 4),
+           "per_size_launches_us": round(tp * 1e6, 1), "plan_seconds": round(plan_s, 2)}
+    if with_oracle:
+        from oracle import oracle as O
+        yy = bp.execute(x, mode=0).cpu().numpy()
+        offs = np.concatenate([[0], np.cumsum(lens)[:-1]])
+        sel = np.arange(0, len(lens), 16)
+        sx = np.concatenate([xv[offs[i]:offs[i] + lens[i]] for i in sel]).astype(np.complex128)
+        so = np.concatenate([[0], np.cumsum(lens[sel])[:-1]])
+        ref = O.fft_uneven(sx, so, lens[sel])
+        errs = [np.linalg.norm(yy[offs[i]:offs[i] + lens[i]] - ref[o:o + lens[i]]) /
+                np.linalg.norm(ref[o:o + lens[i]]) for i, o in zip(sel, so)]
+        out["rel_l2_vs_oracle_max_sampled_lanes"] = float(max(errs))
+        out["oracle_sample"] = f"every 16th lane ({len(sel)} lanes), f64 oracle per-length dispatch"
+    return out
+
+
+def c4_entry(afc, torch, dev, steps, warmup, hbm_peak, with_oracle):
+    """C4: 16384 x 4096 complex64 forward; FP32 SIMT vs the split-precision tensor-core forms."""
+    from apollofft_b200 import workloads as W
+    xs, k = W.c4_rows()
+    x = torch.from_numpy(xs).to(dev)
+    fl = 16384 * 5 * 4096 * 12
+    ref = None
+    if with_oracle:
+        from oracle import oracle as O
+        ref = O.fft1d(xs.astype(np.complex128))
+        den = np.linalg.norm(ref, axis=1)
+    variants = {}
+    t32 = None
+    for name, prec in (("fp32_simt", "f32"), ("tc_bf16_split", "tc_bf16"), ("tc_fp16_split", "tc_fp16")):
+        p = afc.CudaPlan([4096], precision=prec, batch=16384)
+        y = torch.empty_like(x)
+        t = _events_time(lambda: p.execute(x, out=y), steps, warmup, torch)
+        v = {"us": round(t * 1e6, 1), "gflops": round(fl / t / 1e9, 1),
+             "hbm_frac": round(2 * 16384 * 4096 * 8 / t / 1e9 / hbm_peak, 4)}
+        if t32 is None:
+            t32 = t
+        else:
+            v["speedup_vs_fp32_simt"] = round(t32 / t, 3)
+        if ref is not None:
+            yc = y.cpu().numpy()
+            r = np.linalg.norm(yc - ref, axis=1) / den
+            v["rel_l2_per_row_max_vs_oracle"] = float(r.max())
+            v["rel_l2_per_row_median_vs_oracle"] = float(np.median(r))
+            v["rel_l2_per_row_max_hdr_rows"] = float(r[k != 0].max())
+        variants[name] = v
+        del p, y
+    return {"config": "C4", "workload": "16384 x 4096 complex64 forward, 25% rows x 10^k (k in [-6, 6])",
+            "variants": variants}
+
+
+def c5_entry(afc, torch, dev, steps, warmup, hbm_peak, with_oracle):
+    """C5: 8 x 2048^2 real f32, full-spectrum R2C, loss sum |w X|^2, gradient by the adjoint."""
+    from apollofft_b200 import autograd as AG
+    from apollofft_b200 import workloads as W
+    rng = np.random.default_rng(5)
+    img_h = rng.standard_normal((8, 2048, 2048)).astype(np.float32)
+    img = torch.from_numpy(img_h).to(dev)
+    w = torch.from_numpy(W.radial_weight(2048)).to(dev).to(torch.float32)
+
+    def fwd():
+        with torch.no_grad():
+            return torch.sum(torch.abs(w * AG.rfft2(img)) ** 2)
+
+    xg = img.clone().requires_grad_(True)
+
+    def fwdbwd():
+        xg.grad = None
+        loss = torch.sum(torch.abs(w * AG.rfft2(xg)) ** 2)
+        loss.backward()
+
+    p = afc.CudaPlan([2048, 2048], precision="f32", kind="r2c_full", batch=8)
+    yb = torch.empty((8, 2048, 2048), dtype=torch.complex64, device=dev)
+    tr = _events_time(lambda: p.execute(img, out=yb), steps, warmup, torch)
+    tf = _events_time(fwd, steps, warmup, torch)
+    tb = _events_time(fwdbwd, steps, warmup, torch)
+    N = 2048 * 2048
+    fl = 8 * 2.5 * N * math.log2(N)
+    r2c_bytes = 8 * N * (4 + 8)  # real input + full complex spectrum
+    out = {"config": "C5", "workload": "8 x 2048^2 f32 real, full-spectrum R2C (reference contract), loss sum |w X|^2",
+           "r2c_forward_ms": round(tr * 1e3, 3), "r2c_gflops": round(fl / tr / 1e9, 1),
+           "r2c_hbm_frac": round(r2c_bytes / tr / 1e9 / hbm_peak, 4),
+           "loss_forward_ms": round(tf * 1e3, 3), "loss_forward_backward_ms": round(tb * 1e3, 3),
+           "backward_over_forward": round(tb / tf, 3)}
+    if with_oracle:
+        from oracle import oracle as O
+        ref = O.fft2d(img_h.astype(np.complex128))
+        got = yb.cpu().numpy()
+        out["rel_l2_vs_oracle"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    del xg, img, yb
+    return out
+
+
 def run_secondary(args):
     """Lines for the other configurations (not the headline)."""
     import torch
@@ -456,141 +683,34 @@ def run_secondary(args):
     dev = torch.device("cuda", 0)
     hbm_peak, peak_kind = load_peaks()
     line = {"workload": args.workload, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "peak_gbs": hbm_peak}
-    if args.workload == "c1":
-        x = torch.from_numpy(W.c1_input()).to(dev)
-        y = torch.empty_like(x)
-        p = afc.CudaPlan([4096], precision="f64", batch=64)
-        t = _events_time(lambda: (p.execute(x, out=y), p.execute(y, out=x, inverse=True)), args.steps, args.warmup, torch)
-        fl = 2 * 64 * 5 * 4096 * 12
-        line.update({"metric": "GFLOP/s", "value": round(fl / t / 1e9, 2), "us_per_step": round(t * 1e6, 2),
-                     "config": "1D C2C f64 N=4096 x64 fwd+inv",
-                     "hbm_frac": round(2 * 2 * 64 * 4096 * 16 / t / 1e9 / hbm_peak, 4)})
+    if args.workload in ("c1", "c3", "c4", "c5"):
+        fn = {"c1": c1_entry, "c3": c3_entry, "c4": c4_entry, "c5": c5_entry}[args.workload]
+        line.update(fn(afc, torch, dev, args.steps, args.warmup, hbm_peak, True))
         from oracle import oracle as O
-        xin = W.c1_input()
-        t0 = time.perf_counter()
-        reps = 20
-        for _ in range(reps):
-            yy = O.fft1d(xin)
-            O.fft1d(yy, inverse=True)
-        tc = (time.perf_counter() - t0) / reps
-        line["cpu_baseline"] = {"value": round(fl / tc / 1e9, 2), "unit": "GFLOP/s", "cores": O.max_threads(),
-                                "kind": "port", "sample": f"{reps} x (64 x 4096 fwd+inv)"}
-        line["error_vs_oracle_rel_l2"] = float(np.linalg.norm(p.execute(torch.from_numpy(xin).to(dev)).cpu().numpy()
-                                                              - yy) / np.linalg.norm(yy))
-        # the same two calls captured once in a CUDA graph and replayed: the device
-        # time without the per-call host work (Python checks, C ABI, launch)
-        try:
-            side = torch.cuda.Stream()
-            side.wait_stream(torch.cuda.current_stream())
-            with torch.cuda.stream(side):
-                for _ in range(3):
-                    p.execute(x, out=y)
-                    p.execute(y, out=x, inverse=True)
-            torch.cuda.current_stream().wait_stream(side)
-            g = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(g):
-                p.execute(x, out=y)
-                p.execute(y, out=x, inverse=True)
-            tg = _events_time(g.replay, args.steps, args.warmup, torch)
-            line["graph_us_per_step"] = round(tg * 1e6, 2)
-            line["graph_hbm_frac"] = round(2 * 2 * 64 * 4096 * 16 / tg / 1e9 / hbm_peak, 4)
-        except Exception as exc:  # capture refused: report the host-driven figure only
-            line["graph_us_per_step"] = None
-            line["graph_error"] = str(exc)[:200]
-    elif args.workload == "c3":
-        lens = W.c3_lengths()
-        xv = W.c3_values(lens)
-        x = torch.from_numpy(xv).to(dev)
-        t0 = time.perf_counter()
-        bp = afc.BatchPlan(lens, precision="f32")
-        plan_s = time.perf_counter() - t0
-        y = torch.empty_like(x)
-        fl = float(np.sum(5.0 * lens * np.log2(lens)))
-        by = float(np.sum(2.0 * lens * 8))
-        res = {}
-        for mode, name in ((0, "persistent_graph"), (2, "persistent_nograph"), (1, "per_size_launches")):
-            t = _events_time(lambda: bp.execute(x, out=y, mode=mode), args.steps, args.warmup, torch)
-            res[name] = {"us": round(t * 1e6, 1), "gflops": round(fl / t / 1e9, 1),
-                         "hbm_frac": round(by / t / 1e9 / hbm_peak, 4)}
-        line.update({"metric": "GFLOP/s", "value": res["persistent_graph"]["gflops"], "modes": res,
-                     "config": "4096 uneven 1D complex64 lengths log-uniform [64, 65536], thirds pow2/7-smooth/prime",
-                     "distinct_lengths": int(len(np.unique(lens))), "points": int(lens.sum()),
-                     "plan_seconds": round(plan_s, 2)})
-        yy = bp.execute(x, mode=0).cpu().numpy()
-        offs = np.concatenate([[0], np.cumsum(lens)[:-1]])
-        errs = [np.linalg.norm(yy[o:o + n] - np.fft.fft(xv[o:o + n].astype(np.complex128)))
-                / np.linalg.norm(np.fft.fft(xv[o:o + n].astype(np.complex128))) for o, n in zip(offs[::64], lens[::64])]
-        line["max_rel_l2_sampled_lanes_vs_f64"] = float(max(errs))
-        from oracle import oracle as O
-        sample = slice(0, len(lens), 16)
-        sl = lens[sample]
-        so = np.concatenate([[0], np.cumsum(sl)[:-1]])
-        sx = np.concatenate([xv[o:o + n] for o, n in zip(offs[sample], sl)])
-        t0 = time.perf_counter()
-        O.fft_uneven(sx, so, sl)
-        tc = time.perf_counter() - t0
-        line["cpu_baseline"] = {"value": round(float(np.sum(5.0 * sl * np.log2(sl))) / tc / 1e9, 3), "unit": "GFLOP/s",
-                                "cores": O.max_threads(), "kind": "port",
-                                "sample": f"every 16th lane ({len(sl)} lanes), oracle per-length dispatch f32"}
-    elif args.workload == "c4":
-        xs, k = W.c4_rows()
-        x = torch.from_numpy(xs).to(dev)
-        y = torch.empty_like(x)
-        p32 = afc.CudaPlan([4096], precision="f32", batch=16384)
-        t = _events_time(lambda: p32.execute(x, out=y), args.steps, args.warmup, torch)
-        fl = 16384 * 5 * 4096 * 12
-        ref = afc.CudaPlan([4096], precision="f64", batch=16384).execute(x.to(torch.complex128))
-        y = p32.execute(x).to(torch.complex128)
-        num = torch.linalg.vector_norm(y - ref, dim=-1)
-        den = torch.linalg.vector_norm(ref, dim=-1)
-        rel = (num / den).cpu().numpy()
-        variants = {"fp32_simt": {"gflops": round(fl / t / 1e9, 1), "us": round(t * 1e6, 1),
-                                  "hbm_frac": round(2 * 16384 * 4096 * 8 / t / 1e9 / hbm_peak, 4),
-                                  "rel_l2_per_row_max": float(rel.max()), "rel_l2_per_row_median": float(np.median(rel)),
-                                  "max_abs": float(torch.max(torch.abs(y - ref)).item())}}
-        hdr = torch.from_numpy(k != 0).to(dev)
-        for name, prec in (("tc_bf16_split", "tc_bf16"), ("tc_fp16_split", "tc_fp16")):
-            ptc = afc.CudaPlan([4096], precision=prec, batch=16384)
-            yt = torch.empty_like(x)
-            ttc = _events_time(lambda: ptc.execute(x, out=yt), args.steps, args.warmup, torch)
-            yc = ptc.execute(x).to(torch.complex128)
-            r2 = (torch.linalg.vector_norm(yc - ref, dim=-1) / den)
-            variants[name] = {"gflops": round(fl / ttc / 1e9, 1), "us": round(ttc * 1e6, 1),
-                              "hbm_frac": round(2 * 16384 * 4096 * 8 / ttc / 1e9 / hbm_peak, 4),
-                              "speedup_vs_fp32_simt": round(t / ttc, 3),
-                              "rel_l2_per_row_max": float(r2.max().item()),
-                              "rel_l2_per_row_median": float(r2.median().item()),
-                              "rel_l2_per_row_max_hdr_rows": float(r2[hdr].max().item()),
-                              "max_abs": float(torch.max(torch.abs(yc - ref)).item())}
-            del ptc, yt, yc
-        line.update({"metric": "GFLOP/s", "value": variants["fp32_simt"]["gflops"], "variants": variants,
-                     "config": "16384 x 4096 complex64 forward; FP32 SIMT Stockham vs split-precision tensor-core radix-16",
-                     "reference": "GPU f64 path (matches the f64 oracle to 1e-15 in tests)",
-                     "hdr_rows": int((k != 0).sum())})
-    elif args.workload == "c5":
-        from apollofft_b200 import autograd as AG
-        g = torch.Generator(device=dev).manual_seed(5)
-        img = torch.randn(8, 2048, 2048, dtype=torch.float32, device=dev, generator=g)
-        w = torch.from_numpy(W.radial_weight(2048)).to(dev).to(torch.float32)
-
-        def fwd():
-            with torch.no_grad():
-                return torch.sum(torch.abs(w * AG.rfft2(img)) ** 2)
-
-        xg = img.clone().requires_grad_(True)
-
-        def fwdbwd():
-            xg.grad = None
-            loss = torch.sum(torch.abs(w * AG.rfft2(xg)) ** 2)
-            loss.backward()
-
-        tf = _events_time(fwd, args.steps, args.warmup, torch)
-        tb = _events_time(fwdbwd, args.steps, args.warmup, torch)
-        N = 2048 * 2048
-        fl = 8 * 2.5 * N * math.log2(N)
-        line.update({"metric": "ms", "forward_ms": round(tf * 1e3, 3), "forward_backward_ms": round(tb * 1e3, 3),
-                     "ratio": round(tb / tf, 3), "forward_gflops_r2c_convention": round(fl / tf / 1e9, 1),
-                     "config": "8 x 2048^2 f32 real, full-spectrum R2C (reference contract), loss sum |w X|^2"})
+        if args.workload == "c1":
+            xin = W.c1_input()
+            fl = 2 * 64 * 5 * 4096 * 12
+            t0 = time.perf_counter()
+            reps = 20
+            for _ in range(reps):
+                O.fft1d(O.fft1d(xin), inverse=True)
+            tc = (time.perf_counter() - t0) / reps
+            line["cpu_baseline"] = {"value": round(fl / tc / 1e9, 2), "unit": "GFLOP/s", "cores": O.max_threads(),
+                                    "kind": "port", "sample": f"{reps} x (64 x 4096 fwd+inv)"}
+        elif args.workload == "c3":
+            lens = W.c3_lengths()
+            xv = W.c3_values(lens)
+            offs = np.concatenate([[0], np.cumsum(lens)[:-1]])
+            sample = slice(0, len(lens), 16)
+            sl = lens[sample]
+            so = np.concatenate([[0], np.cumsum(sl)[:-1]])
+            sx = np.concatenate([xv[o:o + n] for o, n in zip(offs[sample], sl)])
+            t0 = time.perf_counter()
+            O.fft_uneven(sx, so, sl)
+            tc = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": round(float(np.sum(5.0 * sl * np.log2(sl))) / tc / 1e9, 3),
+                                    "unit": "GFLOP/s", "cores": O.max_threads(), "kind": "port",
+                                    "sample": f"every 16th lane ({len(sl)} lanes), oracle per-length dispatch f32"}
     elif args.workload == "stft":
         # apollo-stft's analysis loop (frame copy + window + one FFT per frame) fused
         # into the FFT load: 2^22 f64 samples, frame 1024, hop 256 (seeded N(0,1))

@@ -144,12 +144,20 @@ AFC_API afc_status afc_execute_adjoint(afc_plan plan, const void* in, void* out,
 
 /* Host-pointer convenience form (mirrors the slice API callers such as
  * apollo-nufft/stft/czt use): copies host -> device, executes, copies back,
- * synchronizes.  Uses plan-owned staging buffers. */
+ * synchronizes.  Safe from many host threads on one shared (cached) plan, as
+ * the reference's Send + Sync plans are: each call in flight takes its own
+ * staging set (device stream, input and output buffers, workspace); up to 4
+ * calls of one plan run at once and further callers wait for a free set. */
 AFC_API afc_status afc_execute_host(afc_plan plan, const void* host_in, void* host_out, afc_direction direction);
 
 /* Workspace the plan needs for one execution on one stream, in bytes (0 if
- * none).  afc_execute uses a plan-owned workspace guarded by a mutex;
- * afc_execute_ws takes a caller-owned one so concurrent streams can share a plan. */
+ * none).  afc_execute keeps plan-owned workspaces, one per stream that uses the
+ * plan (up to 4; further streams take turns on the least recently used one):
+ * each is ordered after its last use by an event the next user's stream waits
+ * on, so calls on one shared plan from several streams and threads are safe
+ * without host synchronization.  Calls captured into a CUDA graph skip that
+ * ordering: replay such a graph ordered with other calls on the plan.
+ * afc_execute_ws takes a caller-owned workspace and does no ordering at all. */
 AFC_API afc_status afc_workspace_size(afc_plan plan, size_t* bytes);
 AFC_API afc_status afc_execute_ws(afc_plan plan, const void* in, void* out, afc_direction direction, double scale,
                           int use_scale, void* workspace, size_t workspace_bytes, void* stream);
@@ -167,7 +175,10 @@ AFC_API afc_status afc_batch_plan_create(afc_batch_plan* out, const int64_t* len
                                  afc_precision precision, int device);
 AFC_API afc_status afc_batch_plan_destroy(afc_batch_plan plan);
 /* mode 0: one persistent launch per phase (captured into a CUDA graph on the
- * first call per stream), mode 1: one plain launch per distinct length. */
+ * first call per buffer pair and direction), mode 1: one plain launch per
+ * distinct length, mode 2: the persistent phases without the graph.  Calls on
+ * one batch plan from several streams are ordered on the GPU (its workspace is
+ * shared), so they are safe but do not overlap. */
 AFC_API afc_status afc_batch_execute(afc_batch_plan plan, const void* in, void* out, afc_direction direction,
                              int mode, void* stream);
 AFC_API afc_status afc_batch_total_elems(afc_batch_plan plan, int64_t* elems);

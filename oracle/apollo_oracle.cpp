@@ -400,22 +400,33 @@ static void stockham_pow2(Cx<F>* data, Cx<F>* scratch, usize n, const Cx<F>* tw,
 // Generic size-r DFT in F precision with roots from f64 trig narrowed to F.
 // Stands in for the Winograd codelets (mixed_radix/traits.rs:39-244), which
 // compute the same exact DFT with hand-derived constants.
+// Roots of the size-r DFT, w[e] = exp(sign 2 pi i e / r) narrowed to F (w[0] = 1),
+// built once per (r, direction) and thread (the reference caches its codelet
+// constants statically; caching changes no value, only the host time).
+template <class F> static const std::vector<Cx<F>>& dft_roots(usize r, bool inv) {
+  static thread_local std::map<std::pair<usize, int>, std::vector<Cx<F>>> cache;
+  auto key = std::make_pair(r, (int)inv);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  std::vector<Cx<F>> w(r);
+  double sign = inv ? 1.0 : -1.0;
+  for (usize e = 0; e < r; ++e) {
+    double a = sign * 2.0 * M_PI * (double)e / (double)r;
+    w[e] = e == 0 ? Cx<F>(1, 0) : Cx<F>((F)std::cos(a), (F)std::sin(a));
+  }
+  return cache.emplace(key, std::move(w)).first->second;
+}
+
 template <class F> static void small_dft(Cx<F>* x, usize r, bool inv, usize stride = 1) {
   if (r == 1) return;
   Cx<F> tmp[128];
   std::vector<Cx<F>> big;
   Cx<F>* out = tmp;
   if (r > 128) { big.resize(r); out = big.data(); }
-  double sign = inv ? 1.0 : -1.0;
+  const Cx<F>* w = dft_roots<F>(r, inv).data();
   for (usize k = 0; k < r; ++k) {
     Cx<F> s(0, 0);
-    for (usize m = 0; m < r; ++m) {
-      usize e = (m * k) % r;
-      double a = sign * 2.0 * M_PI * (double)e / (double)r;
-      Cx<F> w((F)std::cos(a), (F)std::sin(a));
-      if (e == 0) w = Cx<F>(1, 0);
-      s += cmul(x[m * stride], w);
-    }
+    for (usize m = 0; m < r; ++m) s += cmul(x[m * stride], w[(m * k) % r]);
     out[k] = s;
   }
   for (usize k = 0; k < r; ++k) x[k * stride] = out[k];
@@ -582,10 +593,70 @@ template <class F> static void pfa(Cx<F>* data, usize n1, usize n2, bool inv) {
 // Forward/inverse used by the Rader convolutions: the reference routes these
 // through short Winograd / composite / PFA / full dispatch (convolution.rs:98-144),
 // all of which are exact DFTs; here the full dispatch is used.
-template <class F> static void rader(Cx<F>* data, usize n, bool inv) {
+// Tables of one Rader prime and direction: the generator order and the kernel
+// spectra (cyclic, or the half-cyclic pair and its twist).  The reference
+// caches the spectra per (p, direction, g^-1) (scalar/rader.rs, caches); here
+// once per thread.  Built exactly as the uncached form did, so every value is
+// unchanged.
+template <class F> struct RaderTables {
+  std::vector<usize> order;
+  std::vector<Cx<F>> ker, kc, kn, tw;
+};
+
+template <class F> static const RaderTables<F>& rader_tables(usize n, bool inv) {
+  static thread_local std::map<std::pair<usize, int>, RaderTables<F>> cache;
+  auto key = std::make_pair(n, (int)inv);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  RaderTables<F> t;
   usize g = primitive_root(n);
   usize g_inv = inverse_mod(g, n);
-  std::vector<usize> order = generator_order(n, g);
+  t.order = generator_order(n, g);
+  usize L = n - 1;
+  double sign = inv ? 1.0 : -1.0;
+  if (L >= 1024) {
+    // Half-cyclic CRT split (convolution.rs:155-280; spectra scalar/rader.rs:37-91).
+    usize m = L / 2;
+    t.kc.resize(m);
+    t.kn.resize(m);
+    t.tw.resize(m);
+    double pi_m = M_PI / (double)m;
+    usize cur = 1;
+    for (usize j = 0; j < m; ++j) {
+      double a = sign * 2.0 * M_PI * (double)cur / (double)n;
+      t.kc[j] = Cx<F>((F)std::cos(a), (F)std::sin(a));
+      cur = (usize)(((unsigned __int128)cur * g_inv) % n);
+    }
+    for (usize j = 0; j < m; ++j) {
+      double a = sign * 2.0 * M_PI * (double)cur / (double)n;
+      Cx<F> upper((F)std::cos(a), (F)std::sin(a));
+      Cx<F> lower = t.kc[j];
+      t.kc[j] = lower + upper;
+      double ta = pi_m * (double)j;
+      Cx<F> twist((F)std::cos(ta), (F)std::sin(ta));
+      t.kn[j] = cmul(lower - upper, twist);
+      t.tw[j] = twist;
+      cur = (usize)(((unsigned __int128)cur * g_inv) % n);
+    }
+    dispatch_inplace<F>(t.kc.data(), m, false, false);
+    dispatch_inplace<F>(t.kn.data(), m, false, false);
+  } else {
+    // Full cyclic convolution (convolution.rs:98-144; spectrum scalar/rader.rs:3-19).
+    t.ker.resize(L);
+    usize cur = 1;
+    for (usize q = 0; q < L; ++q) {
+      double a = sign * 2.0 * M_PI * (double)cur / (double)n;
+      t.ker[q] = Cx<F>((F)std::cos(a), (F)std::sin(a));
+      cur = (usize)(((unsigned __int128)cur * g_inv) % n);
+    }
+    dispatch_inplace<F>(t.ker.data(), L, false, false);
+  }
+  return cache.emplace(key, std::move(t)).first->second;
+}
+
+template <class F> static void rader(Cx<F>* data, usize n, bool inv) {
+  const RaderTables<F>& T = rader_tables<F>(n, inv);
+  const std::vector<usize>& order = T.order;
   usize L = n - 1;
   Cx<F> x0 = data[0];
   std::vector<Cx<F>> pad(L);
@@ -593,31 +664,12 @@ template <class F> static void rader(Cx<F>* data, usize n, bool inv) {
   Cx<F> sum(0, 0);
   for (usize i = 0; i < L; ++i) sum += data[1 + i];
   for (usize q = 0; q < L; ++q) pad[q] = data[order[q]];
-  double sign = inv ? 1.0 : -1.0;
   if (L >= 1024) {
-    // Half-cyclic CRT split (convolution.rs:155-280; spectra scalar/rader.rs:37-91).
+    // Half-cyclic CRT split (convolution.rs:155-280).
     usize m = L / 2;
-    std::vector<Cx<F>> kc(m), kn(m), tw(m);
-    double pi_m = M_PI / (double)m;
-    usize cur = 1;
-    for (usize j = 0; j < m; ++j) {
-      double a = sign * 2.0 * M_PI * (double)cur / (double)n;
-      kc[j] = Cx<F>((F)std::cos(a), (F)std::sin(a));
-      cur = (usize)(((unsigned __int128)cur * g_inv) % n);
-    }
-    for (usize j = 0; j < m; ++j) {
-      double a = sign * 2.0 * M_PI * (double)cur / (double)n;
-      Cx<F> upper((F)std::cos(a), (F)std::sin(a));
-      Cx<F> lower = kc[j];
-      kc[j] = lower + upper;
-      double ta = pi_m * (double)j;
-      Cx<F> twist((F)std::cos(ta), (F)std::sin(ta));
-      kn[j] = cmul(lower - upper, twist);
-      tw[j] = twist;
-      cur = (usize)(((unsigned __int128)cur * g_inv) % n);
-    }
-    dispatch_inplace<F>(kc.data(), m, false, false);
-    dispatch_inplace<F>(kn.data(), m, false, false);
+    const std::vector<Cx<F>>& kc = T.kc;
+    const std::vector<Cx<F>>& kn = T.kn;
+    const std::vector<Cx<F>>& tw = T.tw;
     Cx<F>* first = pad.data();
     Cx<F>* second = pad.data() + m;
     for (usize j = 0; j < m; ++j) {
@@ -640,15 +692,8 @@ template <class F> static void rader(Cx<F>* data, usize n, bool inv) {
       second[j] = (c - nn) * half;
     }
   } else {
-    // Full cyclic convolution (convolution.rs:98-144; spectrum scalar/rader.rs:3-19).
-    std::vector<Cx<F>> ker(L);
-    usize cur = 1;
-    for (usize q = 0; q < L; ++q) {
-      double a = sign * 2.0 * M_PI * (double)cur / (double)n;
-      ker[q] = Cx<F>((F)std::cos(a), (F)std::sin(a));
-      cur = (usize)(((unsigned __int128)cur * g_inv) % n);
-    }
-    dispatch_inplace<F>(ker.data(), L, false, false);
+    // Full cyclic convolution (convolution.rs:98-144).
+    const std::vector<Cx<F>>& ker = T.ker;
     dispatch_inplace<F>(pad.data(), L, false, false);
     for (usize q = 0; q < L; ++q) pad[q] = cmul(pad[q], ker[q]);
     dispatch_inplace<F>(pad.data(), L, true, true);

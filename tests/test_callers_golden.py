@@ -31,8 +31,32 @@ def test_fixtures_reproduce_and_meet_reference_bounds(oracle):
                            cmath.rect(abs(w) ** (j * k), cmath.phase(w) * j * k) for j in range(50))
                        for k in range(30)])
     assert np.abs(G["czt_out"] - direct).max() < 1e-9
-    # analytic signal: real part is the input, the quadrature of the mask path
+    # analytic signal: real part is the input; the quadrature recomputed from the
+    # oracle FFT and the analytic mask (hilbert infrastructure/kernel/direct.rs:85-143)
     assert np.array_equal(G["hilb_z"].real, G["hilb_x"])
+    hx = G["hilb_x"]
+    n = hx.shape[-1]
+    k = np.arange(n)
+    mask = np.where(k < (n + 1) // 2, 2.0, 0.0)
+    mask[0] = 1.0
+    if n % 2 == 0:
+        mask[n // 2] = 1.0
+    z = oracle.fft1d(oracle.fft1d(hx.astype(np.complex128)) * mask, inverse=True)
+    assert rel_l2(z.imag, G["hilb_z"].imag) < 1e-14
+    # STFT spectrum recomputed from the frame loop of apollo-stft (frames centred
+    # at m hop - frame_len / 2, zero outside the signal, symmetric Hann window;
+    # stft/dimension_1d.rs:96-108, 225-239) and the oracle's 1D plan
+    sig = G["stft_signal"]
+    frame, hop = G["stft_spec"].shape[1], 16
+    win = 0.5 - 0.5 * np.cos(2 * np.pi * np.arange(frame) / (frame - 1))
+    frames = 1 + -(-sig.size // hop)
+    assert frames == G["stft_spec"].shape[0]
+    fr = np.zeros((frames, frame), dtype=np.complex128)
+    for mm in range(frames):
+        st = mm * hop - frame // 2
+        lo, hi = max(st, 0), min(st + frame, sig.size)
+        fr[mm, lo - st:hi - st] = sig[lo:hi] * win[lo - st:hi - st]
+    assert rel_l2(oracle.fft1d(fr), G["stft_spec"]) < 1e-14
 
 
 @pytest.mark.gpu

@@ -6,8 +6,10 @@ frame loop), are forbidden inside CUDA stream capture, and are unwelcome where
 a caching allocator owns the memory.  This entry point runs the two-pass
 (four-step) kernels with their intermediate in a static device array.  The
 test calls it through the C ABI twice in a row and compares each result with
-afc_execute on the same input (f64, relative L2 <= 1e-12), and checks the
-size limit.  It lives in a file of its own that pytest collects last.
+afc_execute on the same input (f64 relative L2 <= 1e-12, f32 <= 1e-5), with
+every library device allocation made to fail during the call (so the call
+provably allocates nothing), and checks the size limit.  It lives in a file of
+its own that pytest collects last.
 """
 import ctypes
 
@@ -22,20 +24,29 @@ def rel(a, b):
     return (torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)).item()
 
 
-def test_no_alloc_matches_execute_twice(afc, cuda):
+@pytest.mark.parametrize("prec,n,tol", [("f64", 1 << 16, 1e-12), ("f32", 1 << 17, 1e-5)])
+def test_no_alloc_matches_execute_twice(afc, cuda, prec, n, tol):
     L = afc._lib
-    n, batch = 1 << 16, 4  # 65536 runs on the two-pass kernels in f64; 4 MiB of scratch
-    plan = afc.CudaPlan([n], precision="f64", batch=batch, cached=False)
+    batch = 4  # 4 MiB of scratch in both precisions
+    cdt = torch.complex128 if prec == "f64" else torch.complex64
+    plan = afc.CudaPlan([n], precision=prec, batch=batch, cached=False)
     assert plan.describe(0)["gpu_algo"] == "four_step"
     st = torch.cuda.current_stream().cuda_stream
     g = torch.Generator(device="cuda").manual_seed(11)
     for direction in (0, 1, 0):
-        x = torch.randn(batch * n, dtype=torch.complex128, device=cuda, generator=g)
+        x = torch.randn(batch * n, dtype=cdt, device=cuda, generator=g)
         ref = plan.execute(x, inverse=bool(direction)).reshape(-1)
         out = torch.empty_like(x)
-        L.check(L.lib().afc_execute_1d_no_alloc(plan._h, x.data_ptr(), out.data_ptr(), direction, st), "no_alloc")
         torch.cuda.synchronize()
-        assert rel(out, ref) <= 1e-12
+        # every device allocation the library attempts now fails: the call must not need one
+        L.lib().afc_test_fail_next_allocs(1 << 20)
+        try:
+            status = L.lib().afc_execute_1d_no_alloc(plan._h, x.data_ptr(), out.data_ptr(), direction, st)
+        finally:
+            L.lib().afc_test_fail_next_allocs(0)
+        L.check(status, "no_alloc")
+        torch.cuda.synchronize()
+        assert rel(out, ref) <= tol
     plan.close()
 
 
