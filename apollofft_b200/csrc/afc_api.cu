@@ -1180,7 +1180,21 @@ static LaneMap axis_map(const afc_plan_s& p, int a, int64_t last, long long& lan
   return LaneMap{1, es, shp[a] * es, 0, 1, es, nullptr};
 }
 
-static size_t plan_ws_bytes(const afc_plan_s& p) {
+// x-planes of the plane-by-plane pass pair (the last two axes of a C2C plan of
+// rank >= 2, each in one CTA per lane), 0 when the plan has no such pair.
+// Planes are the batch times the leading axis (rank 3) or the batch (rank 2).
+static long long pair_planes(const afc_plan_s& p) {
+  if (p.kind != AFC_KIND_C2C || p.rank < 2 || p.tc) return 0;
+  const AxisPlan& a = *p.axes[p.rank - 1];
+  const AxisPlan& b = *p.axes[p.rank - 2];
+  if (a.algo != ALGO_SMEM || b.algo != ALGO_SMEM) return 0;
+  const size_t csz = p.dbl ? 16 : 8;
+  const long long plane_bytes = (long long)(a.n * b.n) * (long long)csz;
+  if (plane_bytes > (4ll << 20)) return 0;  // a few planes in flight must stay well inside L2
+  return p.batch * (p.rank == 3 ? p.dims[0] : 1);
+}
+
+static size_t axes_ws_bytes(const afc_plan_s& p) {
   const size_t csz = p.dbl ? 16 : 8;
   size_t need = 0;
   for (int a = 0; a < p.rank; ++a) {
@@ -1189,12 +1203,46 @@ static size_t plan_ws_bytes(const afc_plan_s& p) {
     axis_map(p, a, last, lanes);
     need = std::max(need, axis_ws_bytes(*p.axes[a], lanes, csz));
   }
+  return (need + 255) / 256 * 256;
+}
+
+// Workspace layout: [complex intermediate of the C2R forms][axis passes][pair counters].
+static size_t plan_ws_bytes(const afc_plan_s& p) {
+  const size_t csz = p.dbl ? 16 : 8;
   // C2R forms keep their complex intermediate in the workspace.
   size_t inter = 0;
   if (p.rank > 1 && p.kind == AFC_KIND_R2C_FULL) inter = (size_t)p.N() * p.batch * csz;
   if (p.rank > 1 && p.kind == AFC_KIND_R2C_HALF) inter = (size_t)(p.N() / last_len(p) * half_len(p)) * p.batch * csz;
   inter = (inter + 255) / 256 * 256;
-  return inter + need;
+  const long long planes = pair_planes(p);
+  return inter + axes_ws_bytes(p) + (planes ? tma_pair_sync_bytes(planes) : 0);
+}
+
+// The two plane-local passes of a C2C plan (axes a0 then a1) as one pair
+// launch; false when the TMA kernels cannot take them (the caller then runs
+// the passes one by one).
+static bool try_pair(const afc_plan_s& p, int a0, int a1, const void* in, void* out, double scale, bool inv,
+                     int* sync, cudaStream_t st, cudaError_t& e) {
+  const long long planes = pair_planes(p);
+  if (!planes || !sync || tl_rec) return false;
+  LaunchDesc d[2];
+  const int ax[2] = {a0, a1};
+  for (int k = 0; k < 2; ++k) {
+    const AxisPlan& ap = *p.axes[ax[k]];
+    fill_common(d[k], ap.lp);
+    long long lanes = 0;
+    d[k].im = d[k].om = axis_map(p, ax[k], last_len(p), lanes);
+    d[k].lanes = lanes;
+    d[k].in = k == 0 ? in : out;
+    d[k].out = out;
+    d[k].scale = k == 1 ? scale : 1.0;
+  }
+  TmaPairPlan pp;
+  if (!tma_pair_plan(d[0], d[1], planes, p.dbl, pp)) return false;
+  unsigned* err = device_err_word();
+  if (!err) return false;
+  e = launch_tma_pair(d[0], d[1], pp, sync, err, p.dbl, inv, st);
+  return true;
 }
 
 // Runs one transform of the plan.  scale is applied on the last pass;
@@ -1210,6 +1258,8 @@ static cudaError_t run_plan(const afc_plan_s& p, const void* in, void* out, bool
   inter_b = (inter_b + 255) / 256 * 256;
   void* inter = ws;
   void* axis_ws = static_cast<char*>(ws) + inter_b;
+  int* pair_sync = (ws && pair_planes(p)) ? reinterpret_cast<int*>(static_cast<char*>(ws) + inter_b + axes_ws_bytes(p))
+                                          : nullptr;
 
   // Pass order: forward last axis first (plan/fft/dimension_3d.rs:148-157,
   // dimension_2d.rs forward rows then columns); inverse first axis first.
@@ -1224,6 +1274,18 @@ static cudaError_t run_plan(const afc_plan_s& p, const void* in, void* out, bool
     const int a = order[k];
     const bool lastpass = k + 1 == order.size();
     const AxisPlan& ap = *p.axes[a];
+    // the last two axes run plane by plane in one launch (z then y forward,
+    // y then z inverse) when both fit the TMA kernels
+    if (pair_sync && k + 1 < order.size() && a >= p.rank - 2 && order[k + 1] >= p.rank - 2) {
+      cudaError_t pe = cudaSuccess;
+      const bool pair_last = k + 2 == order.size();
+      if (try_pair(p, a, order[k + 1], first ? src : dst, dst, pair_last ? scale : 1.0, inv, pair_sync, st, pe)) {
+        if (pe != cudaSuccess) return pe;
+        first = false;
+        ++k;
+        continue;
+      }
+    }
     AxisIO io;
     io.scale = lastpass ? scale : 1.0;
     io.pair_w = 1.0;

@@ -260,6 +260,119 @@ __device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long t
   bulk_commit();
 }
 
+// Every stage of the tile in slot `cur` (`work` is the ping-pong buffer when
+// the stages do not run in place).  Returns the buffer that holds the result in
+// the linear layout, the TMA store's source.  Every thread of the CTA calls it
+// (the stages hold CTA barriers); (l, t) is the thread's lane and position in
+// the lane, with t >= P for a thread that has no butterflies in this tile.
+template <class T, bool INV, int V, bool IP>
+__device__ __forceinline__ typename CT<T>::type* tma_stages(const TmaArgs<T>& a, typename CT<T>::type* cur,
+                                                            typename CT<T>::type* work,
+                                                            const typename CT<T>::type* twb, int l, int t) {
+  constexpr bool P2 = V == 1 || V == 2 || V == 4;
+  constexpr bool S7 = V == 3;
+  using C = typename CT<T>::type;
+  const int L = a.L, P = a.P, n = a.sl.n, ld = a.ld;
+  const bool lm = a.mode == 1;
+  const TView<C> wv{work, ld, 1, 1};
+  const int nst = a.sl.nst;
+  const TView<C> lin = lm ? TView<C>{cur, 1, L, 0} : TView<C>{cur, n, 1, 0};
+  const TView<C> cpad{cur, ld, 1, 1};
+  // output buffer (linear layout): the one the last stage does not read
+  C* obuf = (IP || !(nst & 1)) ? cur : work;
+  const TView<C> olin = lm ? TView<C>{obuf, 1, L, 0} : TView<C>{obuf, n, 1, 0};
+  for (int s = 0; IP && s < nst; ++s) {
+    const StageDesc sd = a.sl.st[s];
+    const bool last = s == nst - 1;
+    const TView<C> src = s == 0 ? lin : cpad;
+    const TView<C> dst = last ? olin : cpad;
+    const C* twi = twb + sd.twoff;
+    const T* rsrc = (s == 0 && a.real_in) ? reinterpret_cast<const T*>(cur) : nullptr;
+    T* rdst = (last && a.real_out) ? reinterpret_cast<T*>(cur) : nullptr;
+#define AFC_TI(R) tma_stage_inplace<R, INV, (V == 4 ? 1 : 0)>(src, dst, l, n, sd.Ns, twi, t, P, last, a.scale, rsrc, rdst)
+    if constexpr (P2) {
+      switch (sd.R) {
+        case 2: AFC_TI(2); break;
+        case 4: AFC_TI(4); break;
+        case 8: AFC_TI(8); break;
+        case 16: AFC_TI(16); break;
+        default: break;
+      }
+    } else {
+      switch (sd.R) {
+        case 2: AFC_TI(2); break;
+        case 3: AFC_TI(3); break;
+        case 4: AFC_TI(4); break;
+        case 5: AFC_TI(5); break;
+        case 7: AFC_TI(7); break;
+        case 8: AFC_TI(8); break;
+        case 11: AFC_TI(11); break;
+        case 13: AFC_TI(13); break;
+        case 16: AFC_TI(16); break;
+        default: break;
+      }
+    }
+#undef AFC_TI
+    __syncthreads();
+  }
+  for (int s = 0; !IP && s < nst; ++s) {
+    const StageDesc sd = a.sl.st[s];
+    const bool last = s == nst - 1;
+    const TView<C> src = s == 0 ? lin : ((s & 1) ? wv : cpad);
+    const TView<C> dst = last ? olin : ((s & 1) ? cpad : wv);
+    const C* twi = twb + sd.twoff;
+#define AFC_TM(R) tma_stage<R, INV>(src, dst, l, n, sd.Ns, twi, t, P, last, a.scale)
+    if constexpr (P2) {
+      switch (sd.R) {
+        case 2: AFC_TM(2); break;
+        case 4: AFC_TM(4); break;
+        case 8: AFC_TM(8); break;
+        case 16: AFC_TM(16); break;
+        default: break;
+      }
+    } else if constexpr (S7) {
+      switch (sd.R) {
+        case 2: AFC_TM(2); break;
+        case 3: AFC_TM(3); break;
+        case 4: AFC_TM(4); break;
+        case 5: AFC_TM(5); break;
+        case 6: AFC_TM(6); break;
+        case 7: AFC_TM(7); break;
+        case 8: AFC_TM(8); break;
+        case 9: AFC_TM(9); break;
+        case 10: AFC_TM(10); break;
+        case 12: AFC_TM(12); break;
+        case 14: AFC_TM(14); break;
+        case 15: AFC_TM(15); break;
+        case 16: AFC_TM(16); break;
+        default: break;
+      }
+    } else {
+      switch (sd.R) {
+        case 2: AFC_TM(2); break;
+        case 3: AFC_TM(3); break;
+        case 4: AFC_TM(4); break;
+        case 5: AFC_TM(5); break;
+        case 6: AFC_TM(6); break;
+        case 7: AFC_TM(7); break;
+        case 8: AFC_TM(8); break;
+        case 9: AFC_TM(9); break;
+        case 10: AFC_TM(10); break;
+        case 12: AFC_TM(12); break;
+        case 14: AFC_TM(14); break;
+        case 15: AFC_TM(15); break;
+        case 11: AFC_TM(11); break;
+        case 13: AFC_TM(13); break;
+        case 16: AFC_TM(16); break;
+        default: break;
+      }
+    }
+#undef AFC_TM
+    __syncthreads();
+  }
+  return obuf;
+}
+
 // V (variant): 0 any radix, 256 threads; 1 every stage radix 2/4/8/16 (no
 // odd-radix butterflies, fewer registers; complex64 built for two CTAs per
 // SM); 2 the same for complex128 tiles of at most 128 threads, built for three
@@ -273,11 +386,9 @@ template <class T, bool INV, int V, bool IP>
 __global__ void __launch_bounds__(V == 2 ? 128 : 256,
                                   V == 2 ? 3 : (V == 3 || ((V == 1 || V == 4) && sizeof(T) == 4)) ? 2 : 1)
     tma_kernel(const __grid_constant__ TmaArgs<T> a) {
-  constexpr bool P2 = V == 1 || V == 2 || V == 4;
-  constexpr bool S7 = V == 3;
   using C = typename CT<T>::type;
   extern __shared__ __align__(128) unsigned char smraw[];
-  const int L = a.L, P = a.P, n = a.sl.n, ld = a.ld;
+  const int L = a.L, P = a.P, ld = a.ld;
   C* slots[2];
   slots[0] = reinterpret_cast<C*>(smraw);
   slots[1] = slots[0] + a.slot_elems;
@@ -302,8 +413,6 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
   // shared memory instead of L1 misses to L2)
   if (tid == 0) tma_issue_load(a, tile, slots[0], &bars[0], a.tw_bytes ? slots[1] : nullptr);
   const C* twb = a.tw_bytes ? slots[1] : a.tw;
-  const TView<C> wv{work, ld, 1, 1};
-  const int nst = a.sl.nst;
   for (int it = 0;; ++it) {
     const int cb = it & 1;
     const long long nxt = tile + gridDim.x;
@@ -322,100 +431,7 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
       return;
     }
     C* cur = slots[cb];
-    const TView<C> lin = lm ? TView<C>{cur, 1, L, 0} : TView<C>{cur, n, 1, 0};
-    const TView<C> cpad{cur, ld, 1, 1};
-    // output buffer (linear layout): the one the last stage does not read
-    C* obuf = (IP || !(nst & 1)) ? cur : work;
-    const TView<C> olin = lm ? TView<C>{obuf, 1, L, 0} : TView<C>{obuf, n, 1, 0};
-    for (int s = 0; IP && s < nst; ++s) {
-      const StageDesc sd = a.sl.st[s];
-      const bool last = s == nst - 1;
-      const TView<C> src = s == 0 ? lin : cpad;
-      const TView<C> dst = last ? olin : cpad;
-      const C* twi = twb + sd.twoff;
-      const T* rsrc = (s == 0 && a.real_in) ? reinterpret_cast<const T*>(cur) : nullptr;
-      T* rdst = (last && a.real_out) ? reinterpret_cast<T*>(cur) : nullptr;
-#define AFC_TI(R) tma_stage_inplace<R, INV, (V == 4 ? 1 : 0)>(src, dst, l, n, sd.Ns, twi, t, P, last, a.scale, rsrc, rdst)
-      if constexpr (P2) {
-        switch (sd.R) {
-          case 2: AFC_TI(2); break;
-          case 4: AFC_TI(4); break;
-          case 8: AFC_TI(8); break;
-          case 16: AFC_TI(16); break;
-          default: break;
-        }
-      } else {
-        switch (sd.R) {
-          case 2: AFC_TI(2); break;
-          case 3: AFC_TI(3); break;
-          case 4: AFC_TI(4); break;
-          case 5: AFC_TI(5); break;
-          case 7: AFC_TI(7); break;
-          case 8: AFC_TI(8); break;
-          case 11: AFC_TI(11); break;
-          case 13: AFC_TI(13); break;
-          case 16: AFC_TI(16); break;
-          default: break;
-        }
-      }
-#undef AFC_TI
-      __syncthreads();
-    }
-    for (int s = 0; !IP && s < nst; ++s) {
-      const StageDesc sd = a.sl.st[s];
-      const bool last = s == nst - 1;
-      const TView<C> src = s == 0 ? lin : ((s & 1) ? wv : cpad);
-      const TView<C> dst = last ? olin : ((s & 1) ? cpad : wv);
-      const C* twi = twb + sd.twoff;
-#define AFC_TM(R) tma_stage<R, INV>(src, dst, l, n, sd.Ns, twi, t, P, last, a.scale)
-      if constexpr (P2) {
-        switch (sd.R) {
-          case 2: AFC_TM(2); break;
-          case 4: AFC_TM(4); break;
-          case 8: AFC_TM(8); break;
-          case 16: AFC_TM(16); break;
-          default: break;
-        }
-      } else if constexpr (S7) {
-        switch (sd.R) {
-          case 2: AFC_TM(2); break;
-          case 3: AFC_TM(3); break;
-          case 4: AFC_TM(4); break;
-          case 5: AFC_TM(5); break;
-          case 6: AFC_TM(6); break;
-          case 7: AFC_TM(7); break;
-          case 8: AFC_TM(8); break;
-          case 9: AFC_TM(9); break;
-          case 10: AFC_TM(10); break;
-          case 12: AFC_TM(12); break;
-          case 14: AFC_TM(14); break;
-          case 15: AFC_TM(15); break;
-          case 16: AFC_TM(16); break;
-          default: break;
-        }
-      } else {
-        switch (sd.R) {
-          case 2: AFC_TM(2); break;
-          case 3: AFC_TM(3); break;
-          case 4: AFC_TM(4); break;
-          case 5: AFC_TM(5); break;
-          case 6: AFC_TM(6); break;
-          case 7: AFC_TM(7); break;
-          case 8: AFC_TM(8); break;
-          case 9: AFC_TM(9); break;
-          case 10: AFC_TM(10); break;
-          case 12: AFC_TM(12); break;
-          case 14: AFC_TM(14); break;
-          case 15: AFC_TM(15); break;
-          case 11: AFC_TM(11); break;
-          case 13: AFC_TM(13); break;
-          case 16: AFC_TM(16); break;
-          default: break;
-        }
-      }
-#undef AFC_TM
-      __syncthreads();
-    }
+    C* obuf = tma_stages<T, INV, V, IP>(a, cur, work, twb, l, t);
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) tma_issue_store(a, tile, obuf);
@@ -423,6 +439,212 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
     if (tile >= a.ntiles) break;
   }
   if (tid == 0) bulk_wait0();
+}
+
+// ───────────────────── two axis passes, plane by plane ─────────────────────
+//
+// The first two axis passes of a 3D transform (forward: z then y; inverse: y
+// then z) both stay inside one x-plane (the outermost index), so they can run
+// plane by plane: one persistent launch holds both passes' tiles, ordered so
+// that the phase-1 tiles of plane p come `lag` planes after its phase-0 tiles.
+// Phase-1 tiles of a plane wait for that plane's phase-0 tiles through a
+// per-plane counter; by then the plane (1 MiB at 256^2 complex128) is still in
+// L2, so the intermediate between the two passes never makes a DRAM round trip
+// and the 3D transform reads and writes the volume twice instead of three times.
+//
+// Tiles are claimed in ticket order from an atomic counter, so a tile that
+// waits only waits for tiles with earlier tickets, which are held by running
+// CTAs that never wait on later ones: the schedule cannot deadlock, whatever
+// number of CTAs is resident.  Every wait is bounded; on timeout the CTA sets
+// the error word and leaves.
+
+template <class T> struct TmaPairArgs {
+  TmaArgs<T> ph[2];   // phase 0 and phase 1 (same thread count L * P)
+  long long planes;   // x-planes (outermost index, batch included)
+  long long n0, n1;   // tiles per plane of each phase
+  long long lag;      // planes between a plane's phase-0 and phase-1 tiles
+  int slot_elems;     // per slot: the larger of the two phases
+  int* sync;          // [0] ticket counter, [1 + p] finished phase-0 tiles of plane p (zeroed per launch)
+};
+
+// Ticket -> (phase, tile).  Steps s = 0 .. planes + lag - 1: the phase-0 tiles
+// of plane s (s < planes), then the phase-1 tiles of plane s - lag (s >= lag).
+template <class T>
+__device__ __forceinline__ void pair_item(const TmaPairArgs<T>& pa, long long tk, int& ph, long long& tile) {
+  const long long D = pa.lag, X = pa.planes, n0 = pa.n0, n1 = pa.n1;
+  if (tk < D * n0) {
+    ph = 0;
+    tile = tk;
+    return;
+  }
+  tk -= D * n0;
+  const long long M = X - D;
+  if (tk < M * (n0 + n1)) {
+    const long long s = tk / (n0 + n1), r = tk % (n0 + n1);
+    if (r < n0) {
+      ph = 0;
+      tile = (D + s) * n0 + r;
+    } else {
+      ph = 1;
+      tile = s * n1 + (r - n0);
+    }
+    return;
+  }
+  tk -= M * (n0 + n1);
+  ph = 1;
+  tile = M * n1 + tk;
+}
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
+
+// Bounded wait for `need` finished phase-0 tiles of a plane (about a second at
+// most); then orders this thread's later TMA loads after what they published.
+__device__ __forceinline__ bool plane_wait(const int* cnt, long long need, int limit = 1 << 24) {
+  for (int i = 0; i < limit; ++i) {
+    if (ld_acquire_gpu(cnt) >= need) {
+      fence_proxy_async_global();
+      return true;
+    }
+    __nanosleep(64);
+  }
+  return false;
+}
+
+// Publishes a finished phase-0 tile: its bulk stores have completed (caller
+// waited), made visible to later TMA loads of other CTAs, then counted.
+__device__ __forceinline__ void plane_publish(int* cnt) {
+  fence_proxy_async_global();
+  __threadfence();
+  atomicAdd(cnt, 1);
+}
+
+template <class T, bool INV, int V, bool IP>
+__global__ void __launch_bounds__(V == 2 ? 128 : 256,
+                                  V == 2 ? 3 : (V == 3 || ((V == 1 || V == 4) && sizeof(T) == 4)) ? 2 : 1)
+    tma_pair_kernel(const __grid_constant__ TmaPairArgs<T> pa) {
+  using C = typename CT<T>::type;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ long long s_ticket[2];
+  C* slots[2];
+  slots[0] = reinterpret_cast<C*>(smraw);
+  slots[1] = slots[0] + pa.slot_elems;
+  int wl = pa.ph[0].L * pa.ph[0].ld;
+  if (pa.ph[1].L * pa.ph[1].ld > wl) wl = pa.ph[1].L * pa.ph[1].ld;
+  C* work = IP ? nullptr : slots[1] + pa.slot_elems;
+  C* end = IP ? slots[1] + pa.slot_elems : work + wl;
+  unsigned long long* bars =
+      reinterpret_cast<unsigned long long*>(reinterpret_cast<uintptr_t>(end + 1) & ~(uintptr_t)7);
+  const int tid = threadIdx.x;
+  int* const ticket = pa.sync;
+  int* const cnt = pa.sync + 1;
+  const long long total = pa.planes * (pa.n0 + pa.n1);
+  unsigned* const err = pa.ph[0].err;
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_proxy_async();
+  }
+  __syncthreads();
+  // tid 0 only: a phase-0 tile whose stores were issued but not yet published
+  long long pend_plane = -1;
+  bool fail = false;
+  if (tid == 0) {
+    const long long tk = atomicAdd(ticket, 1);
+    s_ticket[0] = tk;
+    if (tk < total) {
+      int ph;
+      long long tile;
+      pair_item(pa, tk, ph, tile);
+      if (ph == 1 && !plane_wait(cnt + tile / pa.n1, pa.n0)) fail = true;
+      if (!fail) tma_issue_load(pa.ph[ph], tile, slots[0], &bars[0]);
+    }
+    if (fail) {
+      atomicExch(err, 1u);
+      s_ticket[0] = total;
+    }
+  }
+  __syncthreads();
+  long long tk = s_ticket[0];
+  for (int it = 0; tk < total; ++it) {
+    const int cb = it & 1;
+    int ph;
+    long long tile;
+    pair_item(pa, tk, ph, tile);
+    const TmaArgs<T>& a = pa.ph[ph];
+    bool deferred = false;
+    long long ntk = total;
+    int nph = 0;
+    long long ntile = 0;
+    if (tid == 0) {
+      bulk_wait_read0();  // the previous tile's store has finished reading its buffer
+      ntk = atomicAdd(ticket, 1);
+      if (ntk < total) {
+        pair_item(pa, ntk, nph, ntile);
+        // prefetch unless the next tile still waits for its plane's phase-0 tiles
+        if (nph == 0 || ld_acquire_gpu(cnt + ntile / pa.n1) >= pa.n0) {
+          if (nph == 1) fence_proxy_async_global();
+          tma_issue_load(pa.ph[nph], ntile, slots[cb ^ 1], &bars[cb ^ 1]);
+        } else {
+          deferred = true;
+        }
+      }
+      s_ticket[1] = ntk;
+    }
+    const bool ok = mbar_wait(&bars[cb], (unsigned)((it >> 1) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(err, 1u);
+        if (ntk < total && !deferred) mbar_wait(&bars[cb ^ 1], (unsigned)(((it + 1) >> 1) & 1));
+        bulk_wait0();
+      }
+      return;
+    }
+    ntk = s_ticket[1];
+    const bool lm = a.mode == 1;
+    const int L = a.L, P = a.P;
+    const int l = lm ? tid % L : tid / P;
+    const int t = lm ? tid / L : tid % P;
+    C* obuf = tma_stages<T, INV, V, IP>(a, slots[cb], work, a.tw, l, t);
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      if (pend_plane >= 0) {  // the previous phase-0 tile's stores are long done: publish it
+        bulk_wait0();
+        plane_publish(cnt + pend_plane);
+        pend_plane = -1;
+      }
+      tma_issue_store(a, tile, obuf);
+      if (ph == 0) pend_plane = tile / pa.n0;
+      if (deferred) {
+        // the next tile waits on a plane: publish ours first (it may be one of
+        // the tiles waited for), then wait and load
+        if (pend_plane >= 0) {
+          bulk_wait0();
+          plane_publish(cnt + pend_plane);
+          pend_plane = -1;
+        }
+        if (plane_wait(cnt + ntile / pa.n1, pa.n0)) {
+          tma_issue_load(pa.ph[nph], ntile, slots[cb ^ 1], &bars[cb ^ 1]);
+        } else {
+          atomicExch(err, 1u);
+          fail = true;
+        }
+      }
+      s_ticket[0] = fail ? -1 : 0;
+    }
+    __syncthreads();
+    if (s_ticket[0] < 0) break;  // a wait timed out: leave (the error word is set)
+    tk = ntk;
+  }
+  if (tid == 0) {
+    bulk_wait0();
+    if (pend_plane >= 0) plane_publish(cnt + pend_plane);
+  }
 }
 
 // ─────────────────────────────── host side ───────────────────────────────
@@ -573,23 +795,15 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
   return true;
 }
 
-template <class T, bool INV>
-static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, cudaStream_t st) {
+// Kernel arguments of one axis pass on the TMA kernels (tensor maps for
+// strided lanes); false when a tensor map cannot be encoded.
+template <class T> static bool fill_tma_args(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, TmaArgs<T>& a) {
   using C = typename CT<T>::type;
-  auto k = tp.variant == 4  ? tma_kernel<T, INV, 4, true>
-           : tp.variant == 2 ? tma_kernel<T, INV, 2, true>
-           : tp.variant == 1 ? (tp.inplace ? tma_kernel<T, INV, 1, true> : tma_kernel<T, INV, 1, false>)
-           : tp.variant == 3 ? tma_kernel<T, INV, 3, false>
-                             : tma_kernel<T, INV, 0, false>;
-  const size_t smem = tma_smem_bytes(tp, sizeof(C));
-  cudaError_t e = kernel_smem_grant(reinterpret_cast<const void*>(k), smem);
-  if (e != cudaSuccess) return e;
-  TmaArgs<T> a;
   memset(&a, 0, sizeof(a));
   const bool dbl = sizeof(T) == 8;
   if (tp.mode == 1) {
-    if (!make_map(&a.tmi, d.in, dbl, d.im.es, d.sl.n, tp.outer, tp.L, tp.bn)) return cudaErrorInvalidValue;
-    if (!make_map(&a.tmo, d.out, dbl, d.om.es, d.sl.n, tp.outer, tp.L, tp.bn)) return cudaErrorInvalidValue;
+    if (!make_map(&a.tmi, d.in, dbl, d.im.es, d.sl.n, tp.outer, tp.L, tp.bn)) return false;
+    if (!make_map(&a.tmo, d.out, dbl, d.om.es, d.sl.n, tp.outer, tp.L, tp.bn)) return false;
   }
   a.sl = d.sl;
   a.tw = static_cast<const C*>(d.tw);
@@ -610,14 +824,34 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
   a.bn = tp.bn;
   a.scale = (T)d.scale;
   a.err = err;
+  return true;
+}
+
+static int sm_count() {
   if (g_tma_sm == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_tma_sm, cudaDevAttrMultiProcessorCount, dev);
     if (g_tma_sm <= 0) g_tma_sm = 148;
   }
+  return g_tma_sm;
+}
+
+template <class T, bool INV>
+static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, cudaStream_t st) {
+  using C = typename CT<T>::type;
+  auto k = tp.variant == 4  ? tma_kernel<T, INV, 4, true>
+           : tp.variant == 2 ? tma_kernel<T, INV, 2, true>
+           : tp.variant == 1 ? (tp.inplace ? tma_kernel<T, INV, 1, true> : tma_kernel<T, INV, 1, false>)
+           : tp.variant == 3 ? tma_kernel<T, INV, 3, false>
+                             : tma_kernel<T, INV, 0, false>;
+  const size_t smem = tma_smem_bytes(tp, sizeof(C));
+  cudaError_t e = kernel_smem_grant(reinterpret_cast<const void*>(k), smem);
+  if (e != cudaSuccess) return e;
+  TmaArgs<T> a;
+  if (!fill_tma_args<T>(d, tp, err, a)) return cudaErrorInvalidValue;
   const int per_sm = kernel_ctas_per_sm(reinterpret_cast<const void*>(k), tp.L * tp.P, smem);
-  long long grid = (long long)g_tma_sm * per_sm;
+  long long grid = (long long)sm_count() * per_sm;
   if (grid >= tp.ntiles) {
     // one tile per CTA: stage the twiddle table (r-major, twoff + (R - 1) Ns
     // entries per stage) in the second slot when it fits and can be bulk-copied
@@ -632,6 +866,91 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
   k<<<(unsigned)grid, tp.L * tp.P, smem, st>>>(a);
   count_launch(1);
   return cudaGetLastError();
+}
+
+// Two axis passes of the same x-planes in one launch (tma_pair_kernel).  Both
+// phases must run on the same kernel build with the same threads per CTA, and
+// each tile must lie inside one plane.
+bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes, bool dbl, TmaPairPlan& pp) {
+  static const int on = [] {
+    const char* e = getenv("AFC_PAIR");
+    return e && *e ? atoi(e) : 1;
+  }();
+  if (!on || planes < 1) return false;
+  for (int ph = 0; ph < 2; ++ph) {
+    const LaunchDesc& d = ph ? d1 : d0;
+    TmaPlan& tp = pp.ph[ph];
+    if (d.in_op != IN_C || d.out_op != OUT_C) return false;
+    if (!tma_plan(d.sl, d.ld, d.lanes, d.im, d.om, d.in, d.out, dbl, 0, tp)) return false;
+    if (d.lanes % planes) return false;
+    if (tp.mode == 0) {
+      const long long lpp = d.lanes / planes;
+      if (lpp % tp.L) return false;
+      pp.n[ph] = lpp / tp.L;
+    } else {
+      if (tp.outer != planes) return false;
+      pp.n[ph] = tp.kb;
+    }
+    if (tp.ntiles != planes * pp.n[ph]) return false;
+  }
+  const TmaPlan &a = pp.ph[0], &b = pp.ph[1];
+  if (a.variant != b.variant || a.inplace != b.inplace || a.L * a.P != b.L * b.P) return false;
+  if (a.variant == 0) return false;  // radix 11 / 13 plans keep the separate passes
+  const size_t csz = dbl ? 16 : 8;
+  pp.slot_elems = std::max(a.slot_elems, b.slot_elems);
+  pp.threads = a.L * a.P;
+  pp.smem = 2 * (size_t)pp.slot_elems * csz +
+            (a.inplace ? 0 : (size_t)std::max(a.L * a.ld, b.L * b.ld) * csz) + 64;
+  if (pp.smem > 220 * 1024) return false;
+  pp.planes = planes;
+  // lag: about twice the planes the resident CTAs work on at once, so a
+  // plane's phase-0 tiles are published well before its phase-1 tiles start
+  const long long resident = (long long)sm_count() * (a.variant == 2 ? 3 : 2);
+  pp.lag = std::min<long long>(planes, std::max<long long>(4, 2 * resident / (pp.n[0] + pp.n[1]) + 2));
+  return true;
+}
+
+size_t tma_pair_sync_bytes(long long planes) { return (size_t)((planes + 1) * sizeof(int) + 255) / 256 * 256; }
+
+template <class T, bool INV>
+static cudaError_t launch_tma_pair_t(const LaunchDesc& d0, const LaunchDesc& d1, const TmaPairPlan& pp, int* sync,
+                                     unsigned* err, cudaStream_t st) {
+  const int v = pp.ph[0].variant;
+  const bool ip = pp.ph[0].inplace;
+  auto k = v == 4   ? tma_pair_kernel<T, INV, 4, true>
+           : v == 2 ? tma_pair_kernel<T, INV, 2, true>
+           : v == 1 ? (ip ? tma_pair_kernel<T, INV, 1, true> : tma_pair_kernel<T, INV, 1, false>)
+                    : tma_pair_kernel<T, INV, 3, false>;
+  cudaError_t e = kernel_smem_grant(reinterpret_cast<const void*>(k), pp.smem);
+  if (e != cudaSuccess) return e;
+  TmaPairArgs<T> a;
+  memset(&a, 0, sizeof(a));
+  if (!fill_tma_args<T>(d0, pp.ph[0], err, a.ph[0]) || !fill_tma_args<T>(d1, pp.ph[1], err, a.ph[1]))
+    return cudaErrorInvalidValue;
+  a.planes = pp.planes;
+  a.n0 = pp.n[0];
+  a.n1 = pp.n[1];
+  a.lag = pp.lag;
+  a.slot_elems = pp.slot_elems;
+  a.sync = sync;
+  e = cudaMemsetAsync(sync, 0, tma_pair_sync_bytes(pp.planes), st);
+  if (e != cudaSuccess) return e;
+  const int per_sm = kernel_ctas_per_sm(reinterpret_cast<const void*>(k), pp.threads, pp.smem);
+  long long grid = (long long)sm_count() * per_sm;
+  const long long total = pp.planes * (pp.n[0] + pp.n[1]);
+  if (grid > total) grid = total;
+  k<<<(unsigned)grid, pp.threads, pp.smem, st>>>(a);
+  count_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tma_pair(const LaunchDesc& d0, const LaunchDesc& d1, const TmaPairPlan& pp, int* sync,
+                            unsigned* err, bool dbl, bool inv, cudaStream_t st) {
+  if (dbl)
+    return inv ? launch_tma_pair_t<double, true>(d0, d1, pp, sync, err, st)
+               : launch_tma_pair_t<double, false>(d0, d1, pp, sync, err, st);
+  return inv ? launch_tma_pair_t<float, true>(d0, d1, pp, sync, err, st)
+             : launch_tma_pair_t<float, false>(d0, d1, pp, sync, err, st);
 }
 
 cudaError_t launch_tma(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, bool dbl, bool inv, cudaStream_t st) {

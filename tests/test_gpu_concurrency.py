@@ -66,7 +66,7 @@ def test_device_calls_on_two_streams(afc, cuda):
     assert plan.workspace_size() > 0  # the four-step intermediate lives in a plan workspace
     g = torch.Generator(device="cuda").manual_seed(21)
     xs = [torch.randn(batch * dims[0], dtype=torch.complex128, device=cuda, generator=g) for _ in range(2)]
-    alone = [plan.execute(x).clone() for x in xs]
+    alone = [plan.execute(x).reshape(-1).clone() for x in xs]
     torch.cuda.synchronize()
     streams = [torch.cuda.Stream(), torch.cuda.Stream()]
     outs = [[torch.empty_like(xs[0]) for _ in range(6)] for _ in range(2)]

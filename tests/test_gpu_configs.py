@@ -82,21 +82,40 @@ def test_c1_as_configured(afc, oracle, cuda):
     assert row_rel(back, oracle.fft1d(ref, inverse=True)).max() < 1e-12
 
 
+# Primes of the C3 batch whose reference result is not a DFT: the reference's
+# Rader half-cyclic convolution of p - 1 reaches a prime power q^k (q = 19 or
+# q > 23, k >= 2; 10830 = 2 3 5 19^2, 16810 = 2 5 41^2) for which
+# dispatch_inplace (crates/apollo-fft/src/application/execution/kernel/
+# mixed_radix/dispatch.rs:26-86) finds no strategy and returns the data
+# unchanged (radix_shape.rs:277-285 pins 361 as unsupported), so its output is
+# off by about 100%.  The oracle reproduces that; on these lanes the device is
+# held to the exact DFT.
+REFERENCE_DEFECT_PRIMES = {10831, 16811}
+
+
 def test_c3_every_lane_vs_oracle(afc, oracle, cuda):
     from apollofft_b200 import workloads as W
     lens = W.c3_lengths()
     assert len(lens) == 4096
     xv = W.c3_values(lens)
     offs = np.concatenate([[0], np.cumsum(lens)[:-1]])
-    ref = oracle.fft_uneven(xv.astype(np.complex128), offs, lens)
+    x64 = xv.astype(np.complex128)
+    ref = oracle.fft_uneven(x64, offs, lens)
+    # lanes where the reference path is not a DFT (see REFERENCE_DEFECT_PRIMES)
+    defect = set()
+    for i, (o, n) in enumerate(zip(offs, lens)):
+        if int(n) in REFERENCE_DEFECT_PRIMES or rel_l2(ref[o:o + n], np.fft.fft(x64[o:o + n])) > 1e-10:
+            defect.add(i)
+    assert {int(lens[i]) for i in defect} == REFERENCE_DEFECT_PRIMES & set(int(v) for v in lens)
+    for i in defect:
+        o, n = offs[i], lens[i]
+        ref[o:o + n] = np.fft.fft(x64[o:o + n])
     bp = afc.BatchPlan(lens, precision="f32")
     xt = torch.from_numpy(xv).to(cuda)
-    worst = {}
     for mode in (0, 1):
         y = bp.execute(xt, mode=mode).cpu().numpy()
         errs = np.array([rel_l2(y[o:o + n], ref[o:o + n]) for o, n in zip(offs, lens)])
-        worst[mode] = (float(errs.max()), int(lens[np.argmax(errs)]))
-        assert errs.max() < 1e-5, (mode, worst[mode])
+        assert errs.max() < 1e-5, (mode, float(errs.max()), int(lens[np.argmax(errs)]))
 
 
 def test_c4_rows_vs_oracle(afc, oracle, cuda):
