@@ -402,6 +402,10 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
   const int t = lm ? tid / L : tid % P;
   long long tile = blockIdx.x;
   if (tile >= a.ntiles) return;
+  if (smem_u32(smraw) & 127) {  // the tile slots must start on 128 bytes: report, never copy
+    if (tid == 0) atomicExch(a.err, 1u);
+    return;
+  }
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
@@ -459,7 +463,7 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
 // the error word and leaves.
 
 template <class T> struct TmaPairArgs {
-  TmaArgs<T> ph[2];   // phase 0 and phase 1 (same thread count L * P)
+  TmaArgs<T> ph[2];   // phase 0 and phase 1 (the CTA has the larger L * P of the two)
   long long planes;   // x-planes (outermost index, batch included)
   long long n0, n1;   // tiles per plane of each phase
   long long lag;      // planes between a plane's phase-0 and phase-1 tiles
@@ -528,8 +532,9 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
                                   V == 2 ? 3 : (V == 3 || ((V == 1 || V == 4) && sizeof(T) == 4)) ? 2 : 1)
     tma_pair_kernel(const __grid_constant__ TmaPairArgs<T> pa) {
   using C = typename CT<T>::type;
+  // no static shared variables: they would move the dynamic block off the
+  // 128-byte boundary the tensor copies' destinations need
   extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ long long s_ticket[2];
   C* slots[2];
   slots[0] = reinterpret_cast<C*>(smraw);
   slots[1] = slots[0] + pa.slot_elems;
@@ -539,11 +544,16 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
   C* end = IP ? slots[1] + pa.slot_elems : work + wl;
   unsigned long long* bars =
       reinterpret_cast<unsigned long long*>(reinterpret_cast<uintptr_t>(end + 1) & ~(uintptr_t)7);
+  long long* s_ticket = reinterpret_cast<long long*>(bars + 2);  // [0] current / flag, [1] next
   const int tid = threadIdx.x;
   int* const ticket = pa.sync;
   int* const cnt = pa.sync + 1;
   const long long total = pa.planes * (pa.n0 + pa.n1);
   unsigned* const err = pa.ph[0].err;
+  if (smem_u32(smraw) & 127) {  // the tile slots must start on 128 bytes: report, never copy
+    if (tid == 0) atomicExch(err, 1u);
+    return;
+  }
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
@@ -607,8 +617,11 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
     ntk = s_ticket[1];
     const bool lm = a.mode == 1;
     const int L = a.L, P = a.P;
-    const int l = lm ? tid % L : tid / P;
-    const int t = lm ? tid / L : tid % P;
+    // a phase with fewer threads than the CTA leaves the rest idle (no
+    // butterflies: t beyond every stage's count), still at every barrier
+    const bool act = tid < L * P;
+    const int l = !act ? 0 : lm ? tid % L : tid / P;
+    const int t = !act ? (1 << 20) : lm ? tid / L : tid % P;
     C* obuf = tma_stages<T, INV, V, IP>(a, slots[cb], work, a.tw, l, t);
     fence_proxy_async();
     __syncthreads();
@@ -869,8 +882,8 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
 }
 
 // Two axis passes of the same x-planes in one launch (tma_pair_kernel).  Both
-// phases must run on the same kernel build with the same threads per CTA, and
-// each tile must lie inside one plane.
+// phases must run on the same kernel build, and each tile must lie inside one
+// plane; the CTA gets the larger of the two phases' thread counts.
 bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes, bool dbl, TmaPairPlan& pp) {
   static const int on = [] {
     const char* e = getenv("AFC_PAIR");
@@ -894,11 +907,12 @@ bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes,
     if (tp.ntiles != planes * pp.n[ph]) return false;
   }
   const TmaPlan &a = pp.ph[0], &b = pp.ph[1];
-  if (a.variant != b.variant || a.inplace != b.inplace || a.L * a.P != b.L * b.P) return false;
+  if (a.variant != b.variant || a.inplace != b.inplace) return false;
   if (a.variant == 0) return false;  // radix 11 / 13 plans keep the separate passes
   const size_t csz = dbl ? 16 : 8;
   pp.slot_elems = std::max(a.slot_elems, b.slot_elems);
-  pp.threads = a.L * a.P;
+  pp.threads = std::max(a.L * a.P, b.L * b.P);
+  if (pp.threads > (a.variant == 2 ? 128 : 256)) return false;
   pp.smem = 2 * (size_t)pp.slot_elems * csz +
             (a.inplace ? 0 : (size_t)std::max(a.L * a.ld, b.L * b.ld) * csz) + 64;
   if (pp.smem > 220 * 1024) return false;
