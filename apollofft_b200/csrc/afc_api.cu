@@ -1180,17 +1180,15 @@ static LaneMap axis_map(const afc_plan_s& p, int a, int64_t last, long long& lan
   return LaneMap{1, es, shp[a] * es, 0, 1, es, nullptr};
 }
 
-// x-planes of the plane-by-plane pass pair (the last two axes of a C2C plan of
-// rank >= 2, each in one CTA per lane), 0 when the plan has no such pair.
-// Planes are the batch times the leading axis (rank 3) or the batch (rank 2).
+// x-planes of the plane-by-plane pass pair (the last two axes of a C2C or
+// full-spectrum real plan of rank >= 2, each in one CTA per lane), 0 when the
+// plan has no such pair.  Planes are the batch times the leading axis (rank 3)
+// or the batch (rank 2).
 static long long pair_planes(const afc_plan_s& p) {
-  if (p.kind != AFC_KIND_C2C || p.rank < 2 || p.tc) return 0;
+  if ((p.kind != AFC_KIND_C2C && p.kind != AFC_KIND_R2C_FULL) || p.rank < 2 || p.tc) return 0;
   const AxisPlan& a = *p.axes[p.rank - 1];
   const AxisPlan& b = *p.axes[p.rank - 2];
   if (a.algo != ALGO_SMEM || b.algo != ALGO_SMEM) return 0;
-  const size_t csz = p.dbl ? 16 : 8;
-  const long long plane_bytes = (long long)(a.n * b.n) * (long long)csz;
-  if (plane_bytes > (4ll << 20)) return 0;  // a few planes in flight must stay well inside L2
   return p.batch * (p.rank == 3 ? p.dims[0] : 1);
 }
 
@@ -1218,27 +1216,32 @@ static size_t plan_ws_bytes(const afc_plan_s& p) {
   return inter + axes_ws_bytes(p) + (planes ? tma_pair_sync_bytes(planes) : 0);
 }
 
-// The two plane-local passes of a C2C plan (axes a0 then a1) as one pair
-// launch; false when the TMA kernels cannot take them (the caller then runs
-// the passes one by one).
-static bool try_pair(const afc_plan_s& p, int a0, int a1, const void* in, void* out, double scale, bool inv,
-                     int* sync, cudaStream_t st, cudaError_t& e) {
+// The two plane-local passes (axes a0 then a1, with the buffers and
+// operators run_plan chose for them) as one pair launch; false when the TMA
+// kernels cannot take them (the caller then runs the passes one by one).
+static bool try_pair(const afc_plan_s& p, int a0, int a1, const AxisIO& io0, const AxisIO& io1, bool inv, int* sync,
+                     cudaStream_t st, cudaError_t& e) {
   const long long planes = pair_planes(p);
   if (!planes || !sync || tl_rec) return false;
   LaunchDesc d[2];
   const int ax[2] = {a0, a1};
+  const AxisIO* io[2] = {&io0, &io1};
   for (int k = 0; k < 2; ++k) {
     const AxisPlan& ap = *p.axes[ax[k]];
     fill_common(d[k], ap.lp);
-    long long lanes = 0;
-    d[k].im = d[k].om = axis_map(p, ax[k], last_len(p), lanes);
-    d[k].lanes = lanes;
-    d[k].in = k == 0 ? in : out;
-    d[k].out = out;
-    d[k].scale = k == 1 ? scale : 1.0;
+    d[k].im = io[k]->im;
+    d[k].om = io[k]->om;
+    d[k].lanes = io[k]->lanes;
+    d[k].in = io[k]->in;
+    d[k].out = io[k]->out;
+    d[k].in_op = io[k]->in_op;
+    d[k].out_op = io[k]->out_op;
+    d[k].scale = io[k]->scale;
   }
+  // one x-plane of the intermediate (complex), for the L2 budget of the lag
+  const long long plane_bytes = (long long)(p.axes[a0]->n * p.axes[a1]->n) * (p.dbl ? 16 : 8);
   TmaPairPlan pp;
-  if (!tma_pair_plan(d[0], d[1], planes, p.dbl, pp)) return false;
+  if (!tma_pair_plan(d[0], d[1], planes, plane_bytes, p.dbl, pp)) return false;
   unsigned* err = device_err_word();
   if (!err) return false;
   e = launch_tma_pair(d[0], d[1], pp, sync, err, p.dbl, inv, st);
@@ -1266,27 +1269,15 @@ static cudaError_t run_plan(const afc_plan_s& p, const void* in, void* out, bool
   std::vector<int> order;
   if (!inv) for (int a = r - 1; a >= 0; --a) order.push_back(a);
   else for (int a = 0; a < r; ++a) order.push_back(a);
-  // Skip length-1 axes (no-op passes) unless they carry a dtype change.
   const void* src = in;
   void* dst = out;
-  bool first = true;
+  // Each pass's buffers, lane maps and load / store operators.
+  std::vector<AxisIO> ios(order.size());
   for (size_t k = 0; k < order.size(); ++k) {
     const int a = order[k];
+    const bool first = k == 0;
     const bool lastpass = k + 1 == order.size();
-    const AxisPlan& ap = *p.axes[a];
-    // the last two axes run plane by plane in one launch (z then y forward,
-    // y then z inverse) when both fit the TMA kernels
-    if (pair_sync && k + 1 < order.size() && a >= p.rank - 2 && order[k + 1] >= p.rank - 2) {
-      cudaError_t pe = cudaSuccess;
-      const bool pair_last = k + 2 == order.size();
-      if (try_pair(p, a, order[k + 1], first ? src : dst, dst, pair_last ? scale : 1.0, inv, pair_sync, st, pe)) {
-        if (pe != cudaSuccess) return pe;
-        first = false;
-        ++k;
-        continue;
-      }
-    }
-    AxisIO io;
+    AxisIO& io = ios[k];
     io.scale = lastpass ? scale : 1.0;
     io.pair_w = 1.0;
     long long lanes = 0;
@@ -1343,12 +1334,26 @@ static cudaError_t run_plan(const afc_plan_s& p, const void* in, void* out, bool
       }
     }
     io.lanes = lanes;
+  }
+  for (size_t k = 0; k < order.size(); ++k) {
+    const int a = order[k];
+    const AxisPlan& ap = *p.axes[a];
+    const AxisIO& io = ios[k];
+    // the last two axes run plane by plane in one launch (z then y forward,
+    // y then z inverse) when both fit the TMA kernels
+    if (pair_sync && k + 1 < order.size() && a >= r - 2 && order[k + 1] >= r - 2) {
+      cudaError_t pe = cudaSuccess;
+      if (try_pair(p, a, order[k + 1], io, ios[k + 1], inv, pair_sync, st, pe)) {
+        if (pe != cudaSuccess) return pe;
+        ++k;
+        continue;
+      }
+    }
     // A length-1 axis is the identity, but it may still have to move or convert data.
     if (ap.algo == ALGO_NOOP) {
       AxisPlan one;
       one.n = 1;
       if (io.in == io.out && io.in_op == IN_C && io.out_op == OUT_C && io.scale == 1.0) {
-        first = false;
         continue;
       }
       // route through a radix-free copy: a length-1 "transform" is a scaled copy
@@ -1372,12 +1377,10 @@ static cudaError_t run_plan(const afc_plan_s& p, const void* in, void* out, bool
       d.L = (int)std::min<long long>(256, std::max(1LL, io.lanes));
       cudaError_t e = launch_lanes(d, p.dbl, inv, st);
       if (e != cudaSuccess) return e;
-      first = false;
       continue;
     }
     cudaError_t e = exec_axis(ap, p.dbl, inv, io, axis_ws, st);
     if (e != cudaSuccess) return e;
-    first = false;
   }
   return cudaSuccess;
 }

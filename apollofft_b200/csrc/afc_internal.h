@@ -101,7 +101,8 @@ struct TmaPairPlan {
   int slot_elems = 0, threads = 0;
   size_t smem = 0;
 };
-bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes, bool dbl, TmaPairPlan& pp);
+bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes, long long plane_bytes, bool dbl,
+                   TmaPairPlan& pp);
 size_t tma_pair_sync_bytes(long long planes);
 cudaError_t launch_tma_pair(const LaunchDesc& d0, const LaunchDesc& d1, const TmaPairPlan& pp, int* sync,
                             unsigned* err, bool dbl, bool inv, cudaStream_t st);

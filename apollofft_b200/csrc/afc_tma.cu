@@ -527,6 +527,49 @@ __device__ __forceinline__ void plane_publish(int* cnt) {
   atomicAdd(cnt, 1);
 }
 
+// Thread 0 keeps the schedule two tiles ahead of the tile being transformed,
+// so no global round trip sits between two tiles: while tile i is transformed,
+// the load of tile i+1 is in flight (issued if its plane was ready when polled
+// one tile earlier), the readiness poll of tile i+2's plane is in flight, and
+// the ticket of tile i+3 is being claimed.  A CTA blocks only when tile i+1's
+// plane was not ready: then it first publishes its own finished tiles (every
+// tile it holds unprocessed has a later ticket than the one it waits for), so
+// a chain of waits always ends at a CTA that can progress.
+// Thread 0's schedule state lives in shared memory (only the two values read
+// a whole transform after they were requested stay in registers), so the
+// transform itself keeps every register.
+struct PairSlot {
+  int tk;  // ticket (>= total: none)
+  int ph;
+  int tile;
+};
+struct PairState {
+  PairSlot cur, nx, nn;
+  int pend;       // plane of a phase-0 tile whose stores are issued, not yet published (-1: none)
+  int nx_loaded;  // the load of nx is in flight
+  int fail;       // a wait timed out
+};
+
+template <class T>
+__device__ __forceinline__ PairSlot pair_slot(const TmaPairArgs<T>& pa, int tk, long long total) {
+  PairSlot s{tk, 0, 0};
+  if (tk < total) {
+    long long tile;
+    pair_item(pa, tk, s.ph, tile);
+    s.tile = (int)tile;
+  }
+  return s;
+}
+
+// Publishes the pending phase-0 tile of thread 0's state (its stores complete first).
+__device__ __forceinline__ void publish_pending(PairState& S, int* cnt) {
+  if (S.pend >= 0) {
+    bulk_wait0();
+    plane_publish(cnt + S.pend);
+    S.pend = -1;
+  }
+}
+
 template <class T, bool INV, int V, bool IP>
 __global__ void __launch_bounds__(V == 2 ? 128 : 256,
                                   V == 2 ? 3 : (V == 3 || ((V == 1 || V == 4) && sizeof(T) == 4)) ? 2 : 1)
@@ -544,7 +587,8 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
   C* end = IP ? slots[1] + pa.slot_elems : work + wl;
   unsigned long long* bars =
       reinterpret_cast<unsigned long long*>(reinterpret_cast<uintptr_t>(end + 1) & ~(uintptr_t)7);
-  long long* s_ticket = reinterpret_cast<long long*>(bars + 2);  // [0] current / flag, [1] next
+  int* s_tk = reinterpret_cast<int*>(bars + 2);            // [0] tile being transformed, [1] leave flag
+  PairState& S = *reinterpret_cast<PairState*>(s_tk + 2);  // thread 0 only
   const int tid = threadIdx.x;
   int* const ticket = pa.sync;
   int* const cnt = pa.sync + 1;
@@ -554,67 +598,60 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
     if (tid == 0) atomicExch(err, 1u);
     return;
   }
+  int nn_poll = 0;  // thread 0: plane counter of nn as polled one transform earlier
+  int nnn_tk = 0;   // thread 0: ticket claimed for the tile after nn
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     fence_proxy_async();
-  }
-  __syncthreads();
-  // tid 0 only: a phase-0 tile whose stores were issued but not yet published
-  long long pend_plane = -1;
-  bool fail = false;
-  if (tid == 0) {
-    const long long tk = atomicAdd(ticket, 1);
-    s_ticket[0] = tk;
-    if (tk < total) {
-      int ph;
-      long long tile;
-      pair_item(pa, tk, ph, tile);
-      if (ph == 1 && !plane_wait(cnt + tile / pa.n1, pa.n0)) fail = true;
-      if (!fail) tma_issue_load(pa.ph[ph], tile, slots[0], &bars[0]);
+    S.cur = pair_slot(pa, atomicAdd(ticket, 1), total);
+    S.nx = pair_slot(pa, atomicAdd(ticket, 1), total);
+    S.nn = pair_slot(pa, atomicAdd(ticket, 1), total);
+    S.pend = -1;
+    S.nx_loaded = 0;
+    S.fail = 0;
+    if (S.cur.tk < total) {
+      if (S.cur.ph == 1 && !plane_wait(cnt + S.cur.tile / pa.n1, pa.n0)) S.fail = 1;
+      if (!S.fail) tma_issue_load(pa.ph[S.cur.ph], S.cur.tile, slots[0], &bars[0]);
     }
-    if (fail) {
+    if (S.nx.tk < total && S.nx.ph == 1) nn_poll = ld_acquire_gpu(cnt + S.nx.tile / pa.n1);
+    if (S.fail) {
       atomicExch(err, 1u);
-      s_ticket[0] = total;
+      S.cur.tk = (int)total;
     }
+    s_tk[0] = S.cur.tk;
   }
   __syncthreads();
-  long long tk = s_ticket[0];
+  int tk = s_tk[0];
   for (int it = 0; tk < total; ++it) {
     const int cb = it & 1;
+    if (tid == 0) {
+      bulk_wait_read0();  // the previous tile's store has finished reading its buffer
+      // tile i+1: prefetch when its plane was ready at the last poll
+      S.nx_loaded = 0;
+      if (S.nx.tk < total && (S.nx.ph == 0 || nn_poll >= pa.n0)) {
+        if (S.nx.ph == 1) fence_proxy_async_global();
+        tma_issue_load(pa.ph[S.nx.ph], S.nx.tile, slots[cb ^ 1], &bars[cb ^ 1]);
+        S.nx_loaded = 1;
+      }
+      // tile i+2: poll its plane now, read the value a whole transform later
+      nn_poll = (S.nn.tk < total && S.nn.ph == 1) ? ld_acquire_gpu(cnt + S.nn.tile / pa.n1) : 0;
+      // tile i+3: claim its ticket now, use it after the transform
+      nnn_tk = atomicAdd(ticket, 1);
+    }
     int ph;
     long long tile;
     pair_item(pa, tk, ph, tile);
     const TmaArgs<T>& a = pa.ph[ph];
-    bool deferred = false;
-    long long ntk = total;
-    int nph = 0;
-    long long ntile = 0;
-    if (tid == 0) {
-      bulk_wait_read0();  // the previous tile's store has finished reading its buffer
-      ntk = atomicAdd(ticket, 1);
-      if (ntk < total) {
-        pair_item(pa, ntk, nph, ntile);
-        // prefetch unless the next tile still waits for its plane's phase-0 tiles
-        if (nph == 0 || ld_acquire_gpu(cnt + ntile / pa.n1) >= pa.n0) {
-          if (nph == 1) fence_proxy_async_global();
-          tma_issue_load(pa.ph[nph], ntile, slots[cb ^ 1], &bars[cb ^ 1]);
-        } else {
-          deferred = true;
-        }
-      }
-      s_ticket[1] = ntk;
-    }
     const bool ok = mbar_wait(&bars[cb], (unsigned)((it >> 1) & 1));
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         atomicExch(err, 1u);
-        if (ntk < total && !deferred) mbar_wait(&bars[cb ^ 1], (unsigned)(((it + 1) >> 1) & 1));
+        if (S.nx_loaded) mbar_wait(&bars[cb ^ 1], (unsigned)(((it + 1) >> 1) & 1));
         bulk_wait0();
       }
       return;
     }
-    ntk = s_ticket[1];
     const bool lm = a.mode == 1;
     const int L = a.L, P = a.P;
     // a phase with fewer threads than the CTA leaves the rest idle (no
@@ -626,37 +663,33 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
-      if (pend_plane >= 0) {  // the previous phase-0 tile's stores are long done: publish it
-        bulk_wait0();
-        plane_publish(cnt + pend_plane);
-        pend_plane = -1;
-      }
+      publish_pending(S, cnt);  // the previous phase-0 tile's stores are long done
       tma_issue_store(a, tile, obuf);
-      if (ph == 0) pend_plane = tile / pa.n0;
-      if (deferred) {
-        // the next tile waits on a plane: publish ours first (it may be one of
-        // the tiles waited for), then wait and load
-        if (pend_plane >= 0) {
-          bulk_wait0();
-          plane_publish(cnt + pend_plane);
-          pend_plane = -1;
-        }
-        if (plane_wait(cnt + ntile / pa.n1, pa.n0)) {
-          tma_issue_load(pa.ph[nph], ntile, slots[cb ^ 1], &bars[cb ^ 1]);
+      if (ph == 0) S.pend = (int)(tile / pa.n0);
+      if (S.nx.tk < total && !S.nx_loaded) {
+        // tile i+1 waits on a plane: publish ours first (it may be one of the
+        // tiles waited for), then wait and load
+        publish_pending(S, cnt);
+        if (plane_wait(cnt + S.nx.tile / pa.n1, pa.n0)) {
+          tma_issue_load(pa.ph[S.nx.ph], S.nx.tile, slots[cb ^ 1], &bars[cb ^ 1]);
         } else {
           atomicExch(err, 1u);
-          fail = true;
+          S.fail = 1;
         }
       }
-      s_ticket[0] = fail ? -1 : 0;
+      S.cur = S.nx;
+      S.nx = S.nn;
+      S.nn = pair_slot(pa, nnn_tk, total);
+      s_tk[0] = S.cur.tk;
+      s_tk[1] = S.fail;
     }
     __syncthreads();
-    if (s_ticket[0] < 0) break;  // a wait timed out: leave (the error word is set)
-    tk = ntk;
+    if (s_tk[1]) break;  // a wait timed out: leave (the error word is set)
+    tk = s_tk[0];
   }
   if (tid == 0) {
     bulk_wait0();
-    if (pend_plane >= 0) plane_publish(cnt + pend_plane);
+    publish_pending(S, cnt);
   }
 }
 
@@ -884,7 +917,8 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
 // Two axis passes of the same x-planes in one launch (tma_pair_kernel).  Both
 // phases must run on the same kernel build, and each tile must lie inside one
 // plane; the CTA gets the larger of the two phases' thread counts.
-bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes, bool dbl, TmaPairPlan& pp) {
+bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes, long long plane_bytes, bool dbl,
+                   TmaPairPlan& pp) {
   static const int on = [] {
     const char* e = getenv("AFC_PAIR");
     return e && *e ? atoi(e) : 1;
@@ -893,8 +927,12 @@ bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes,
   for (int ph = 0; ph < 2; ++ph) {
     const LaunchDesc& d = ph ? d1 : d0;
     TmaPlan& tp = pp.ph[ph];
-    if (d.in_op != IN_C || d.out_op != OUT_C) return false;
-    if (!tma_plan(d.sl, d.ld, d.lanes, d.im, d.om, d.in, d.out, dbl, 0, tp)) return false;
+    // complex lanes, or real rows widened on load (first phase of a forward
+    // real transform) / real parts stored (last phase of its inverse)
+    const bool rin = d.in_op == IN_R && d.out_op == OUT_C && ph == 0;
+    const bool rout = d.in_op == IN_C && d.out_op == OUT_RE && ph == 1;
+    if (!(d.in_op == IN_C && d.out_op == OUT_C) && !rin && !rout) return false;
+    if (!tma_plan(d.sl, d.ld, d.lanes, d.im, d.om, d.in, d.out, dbl, 0, tp, rin, rout)) return false;
     if (d.lanes % planes) return false;
     if (tp.mode == 0) {
       const long long lpp = d.lanes / planes;
@@ -913,14 +951,20 @@ bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes,
   pp.slot_elems = std::max(a.slot_elems, b.slot_elems);
   pp.threads = std::max(a.L * a.P, b.L * b.P);
   if (pp.threads > (a.variant == 2 ? 128 : 256)) return false;
+  // + barriers, the tile ticket and thread 0's schedule state (PairState)
   pp.smem = 2 * (size_t)pp.slot_elems * csz +
-            (a.inplace ? 0 : (size_t)std::max(a.L * a.ld, b.L * b.ld) * csz) + 64;
+            (a.inplace ? 0 : (size_t)std::max(a.L * a.ld, b.L * b.ld) * csz) + 128;
   if (pp.smem > 220 * 1024) return false;
   pp.planes = planes;
   // lag: about twice the planes the resident CTAs work on at once, so a
-  // plane's phase-0 tiles are published well before its phase-1 tiles start
+  // plane's phase-0 tiles are published well before its phase-1 tiles start;
+  // but the planes between a plane's two phases must stay in L2 (126 MB):
+  // at most 48 MiB of them, and at least one plane
   const long long resident = (long long)sm_count() * (a.variant == 2 ? 3 : 2);
-  pp.lag = std::min<long long>(planes, std::max<long long>(4, 2 * resident / (pp.n[0] + pp.n[1]) + 2));
+  const long long want = std::max<long long>(4, 2 * resident / (pp.n[0] + pp.n[1]) + 2);
+  const long long fit = std::max<long long>(1, (48ll << 20) / std::max<long long>(plane_bytes, 1));
+  if (plane_bytes > (64ll << 20)) return false;  // two planes in flight would not fit in L2
+  pp.lag = std::min<long long>(planes, std::min(want, fit));
   return true;
 }
 
