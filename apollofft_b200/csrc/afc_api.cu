@@ -1212,17 +1212,16 @@ static size_t plan_ws_bytes(const afc_plan_s& p) {
   if (p.rank > 1 && p.kind == AFC_KIND_R2C_FULL) inter = (size_t)p.N() * p.batch * csz;
   if (p.rank > 1 && p.kind == AFC_KIND_R2C_HALF) inter = (size_t)(p.N() / last_len(p) * half_len(p)) * p.batch * csz;
   inter = (inter + 255) / 256 * 256;
-  const long long planes = pair_planes(p);
-  return inter + axes_ws_bytes(p) + (planes ? tma_pair_sync_bytes(planes) : 0);
+  return inter + axes_ws_bytes(p);
 }
 
 // The two plane-local passes (axes a0 then a1, with the buffers and
 // operators run_plan chose for them) as one pair launch; false when the TMA
 // kernels cannot take them (the caller then runs the passes one by one).
-static bool try_pair(const afc_plan_s& p, int a0, int a1, const AxisIO& io0, const AxisIO& io1, bool inv, int* sync,
+static bool try_pair(const afc_plan_s& p, int a0, int a1, const AxisIO& io0, const AxisIO& io1, bool inv,
                      cudaStream_t st, cudaError_t& e) {
   const long long planes = pair_planes(p);
-  if (!planes || !sync || tl_rec) return false;
+  if (!planes || tl_rec) return false;
   LaunchDesc d[2];
   const int ax[2] = {a0, a1};
   const AxisIO* io[2] = {&io0, &io1};
@@ -1241,10 +1240,10 @@ static bool try_pair(const afc_plan_s& p, int a0, int a1, const AxisIO& io0, con
   // one x-plane of the intermediate (complex), for the L2 budget of the lag
   const long long plane_bytes = (long long)(p.axes[a0]->n * p.axes[a1]->n) * (p.dbl ? 16 : 8);
   TmaPairPlan pp;
-  if (!tma_pair_plan(d[0], d[1], planes, plane_bytes, p.dbl, pp)) return false;
+  if (!tma_pair_plan(d[0], d[1], planes, plane_bytes, p.dbl, inv, pp)) return false;
   unsigned* err = device_err_word();
   if (!err) return false;
-  e = launch_tma_pair(d[0], d[1], pp, sync, err, p.dbl, inv, st);
+  e = launch_tma_pair(d[0], d[1], pp, err, p.dbl, inv, st);
   return true;
 }
 
@@ -1261,8 +1260,6 @@ static cudaError_t run_plan(const afc_plan_s& p, const void* in, void* out, bool
   inter_b = (inter_b + 255) / 256 * 256;
   void* inter = ws;
   void* axis_ws = static_cast<char*>(ws) + inter_b;
-  int* pair_sync = (ws && pair_planes(p)) ? reinterpret_cast<int*>(static_cast<char*>(ws) + inter_b + axes_ws_bytes(p))
-                                          : nullptr;
 
   // Pass order: forward last axis first (plan/fft/dimension_3d.rs:148-157,
   // dimension_2d.rs forward rows then columns); inverse first axis first.
@@ -1341,9 +1338,9 @@ static cudaError_t run_plan(const afc_plan_s& p, const void* in, void* out, bool
     const AxisIO& io = ios[k];
     // the last two axes run plane by plane in one launch (z then y forward,
     // y then z inverse) when both fit the TMA kernels
-    if (pair_sync && k + 1 < order.size() && a >= r - 2 && order[k + 1] >= r - 2) {
+    if (k + 1 < order.size() && a >= r - 2 && order[k + 1] >= r - 2) {
       cudaError_t pe = cudaSuccess;
-      if (try_pair(p, a, order[k + 1], io, ios[k + 1], inv, pair_sync, st, pe)) {
+      if (try_pair(p, a, order[k + 1], io, ios[k + 1], inv, st, pe)) {
         if (pe != cudaSuccess) return pe;
         ++k;
         continue;

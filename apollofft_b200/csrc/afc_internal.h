@@ -90,22 +90,23 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
 size_t tma_smem_bytes(const TmaPlan& tp, size_t csz);
 cudaError_t launch_tma(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, bool dbl, bool inv, cudaStream_t st);
 
-// Two axis passes over the same x-planes in one persistent launch (afc_tma.cu,
-// tma_pair_kernel): phase-1 tiles of a plane wait for its phase-0 tiles, so the
-// intermediate stays in L2.  `sync` holds a ticket counter and one counter per
-// plane (tma_pair_sync_bytes), zeroed by the launch.
+// Two axis passes over the same x-planes in one launch (afc_tma.cu,
+// tma_pair_kernel): a thread-block cluster per plane transforms the plane's
+// first-axis tiles, meets at the cluster barrier, then transforms its
+// second-axis tiles, so the intermediate stays in L2.
 struct TmaPairPlan {
   TmaPlan ph[2];
-  long long n[2] = {0, 0};  // tiles per plane of each phase
-  long long planes = 0, lag = 0;
+  int n[2] = {0, 0};            // tiles per plane of each phase
+  long long lpp[2] = {0, 0};    // contiguous phases: lanes per plane
+  long long planes = 0;
   int slot_elems = 0, threads = 0;
+  int cs = 0, nclusters = 0;    // CTAs per cluster, clusters launched
   size_t smem = 0;
 };
 bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes, long long plane_bytes, bool dbl,
-                   TmaPairPlan& pp);
-size_t tma_pair_sync_bytes(long long planes);
-cudaError_t launch_tma_pair(const LaunchDesc& d0, const LaunchDesc& d1, const TmaPairPlan& pp, int* sync,
-                            unsigned* err, bool dbl, bool inv, cudaStream_t st);
+                   bool inv, TmaPairPlan& pp);
+cudaError_t launch_tma_pair(const LaunchDesc& d0, const LaunchDesc& d1, const TmaPairPlan& pp, unsigned* err,
+                            bool dbl, bool inv, cudaStream_t st);
 
 // tensor-core radix-16 FFT (afc_tc.cu)
 struct TcLaunch {

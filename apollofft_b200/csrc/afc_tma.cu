@@ -43,9 +43,26 @@ template <class T> struct TmaArgs {
   int real_out;     // contiguous in-place mode: output lanes are the real parts
   int nbx, bn;      // boxes along the transformed axis, rows per box
   unsigned tw_bytes;  // > 0: one tile per CTA, the twiddle table is copied into the idle second slot
+  long long tpp, lpp; // contiguous mode, tpp > 0: tiles never straddle planes of lpp lanes (tpp tiles per
+                      // plane, the last one of a plane shorter); tpp = 0: tile q covers lanes [q L, q L + L)
   T scale;
   unsigned* err;
 };
+
+// First lane and lane count of contiguous-mode tile `tile`.
+template <class T>
+__device__ __forceinline__ void tile_lanes(const TmaArgs<T>& a, long long tile, long long& q0, int& nl) {
+  long long rem;
+  if (a.tpp > 0) {
+    const long long pl = tile / a.tpp, k = tile % a.tpp;
+    q0 = pl * a.lpp + k * a.L;
+    rem = a.lpp - k * a.L;
+  } else {
+    q0 = tile * a.L;
+    rem = a.lanes - q0;
+  }
+  nl = (int)(rem < a.L ? rem : a.L);
+}
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -224,9 +241,9 @@ __device__ __forceinline__ void tma_issue_load(const TmaArgs<T>& a, long long ti
   using C = typename CT<T>::type;
   const unsigned extra = tw_dst ? a.tw_bytes : 0u;
   if (a.mode == 0) {
-    const long long q0 = tile * a.L;
-    const long long rem = a.lanes - q0;
-    const int lanes_here = (int)(rem < a.L ? rem : a.L);
+    long long q0;
+    int lanes_here;
+    tile_lanes(a, tile, q0, lanes_here);
     const size_t es = a.real_in ? sizeof(T) : sizeof(C);
     const unsigned bytes = (unsigned)((long long)lanes_here * a.sl.n * es);
     mbar_expect_tx(bar, bytes + extra);
@@ -245,9 +262,9 @@ template <class T>
 __device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long tile, const typename CT<T>::type* buf) {
   using C = typename CT<T>::type;
   if (a.mode == 0) {
-    const long long q0 = tile * a.L;
-    const long long rem = a.lanes - q0;
-    const int lanes_here = (int)(rem < a.L ? rem : a.L);
+    long long q0;
+    int lanes_here;
+    tile_lanes(a, tile, q0, lanes_here);
     const size_t es = a.real_out ? sizeof(T) : sizeof(C);
     bulk_store(reinterpret_cast<char*>(a.out) + q0 * a.sl.n * es, buf, (unsigned)((long long)lanes_here * a.sl.n * es));
   } else {
@@ -449,126 +466,60 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
 //
 // The first two axis passes of a 3D transform (forward: z then y; inverse: y
 // then z) both stay inside one x-plane (the outermost index), so they can run
-// plane by plane: one persistent launch holds both passes' tiles, ordered so
-// that the phase-1 tiles of plane p come `lag` planes after its phase-0 tiles.
-// Phase-1 tiles of a plane wait for that plane's phase-0 tiles through a
-// per-plane counter; by then the plane (1 MiB at 256^2 complex128) is still in
-// L2, so the intermediate between the two passes never makes a DRAM round trip
-// and the 3D transform reads and writes the volume twice instead of three times.
+// plane by plane: a thread-block cluster owns a plane, its CTAs transform the
+// plane's phase-0 tiles, meet at the cluster barrier, then transform its
+// phase-1 tiles.  The plane between the two phases (1 MiB at 256^2
+// complex128) is written and read back through L2 while few enough planes are
+// in flight (the clusters in flight x the plane size stays far below the 126
+// MB L2), so a 3D transform reads and writes the volume in DRAM twice instead
+// of three times.  The only synchronization is one cluster barrier per plane.
 //
-// Tiles are claimed in ticket order from an atomic counter, so a tile that
-// waits only waits for tiles with earlier tickets, which are held by running
-// CTAs that never wait on later ones: the schedule cannot deadlock, whatever
-// number of CTAs is resident.  Every wait is bounded; on timeout the CTA sets
-// the error word and leaves.
+// The cluster barrier has no timeout, so every CTA of a cluster reaches every
+// barrier: a CTA whose bounded wait timed out sets the error word and skips
+// the rest of its copies and transforms, but keeps arriving.
 
 template <class T> struct TmaPairArgs {
   TmaArgs<T> ph[2];   // phase 0 and phase 1 (the CTA has the larger L * P of the two)
   long long planes;   // x-planes (outermost index, batch included)
-  long long n0, n1;   // tiles per plane of each phase
-  long long lag;      // planes between a plane's phase-0 and phase-1 tiles
+  int n0, n1;         // tiles per plane of each phase
   int slot_elems;     // per slot: the larger of the two phases
-  int* sync;          // [0] ticket counter, [1 + p] finished phase-0 tiles of plane p (zeroed per launch)
 };
 
-// Ticket -> (phase, tile).  Steps s = 0 .. planes + lag - 1: the phase-0 tiles
-// of plane s (s < planes), then the phase-1 tiles of plane s - lag (s >= lag).
-template <class T>
-__device__ __forceinline__ void pair_item(const TmaPairArgs<T>& pa, long long tk, int& ph, long long& tile) {
-  const long long D = pa.lag, X = pa.planes, n0 = pa.n0, n1 = pa.n1;
-  if (tk < D * n0) {
-    ph = 0;
-    tile = tk;
-    return;
-  }
-  tk -= D * n0;
-  const long long M = X - D;
-  if (tk < M * (n0 + n1)) {
-    const long long s = tk / (n0 + n1), r = tk % (n0 + n1);
-    if (r < n0) {
-      ph = 0;
-      tile = (D + s) * n0 + r;
-    } else {
-      ph = 1;
-      tile = s * n1 + (r - n0);
-    }
-    return;
-  }
-  tk -= M * (n0 + n1);
-  ph = 1;
-  tile = M * n1 + tk;
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
 }
-
-__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
-  return v;
+__device__ __forceinline__ unsigned cluster_nrank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cluster_id() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%clusterid.x;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cluster_count() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%nclusterid.x;\n" : "=r"(r));
+  return r;
+}
+// Every thread of every CTA of the cluster: writes before are visible to
+// reads after in the other CTAs (release / acquire at cluster scope).
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
 
-// Bounded wait for `need` finished phase-0 tiles of a plane (about a second at
-// most); then orders this thread's later TMA loads after what they published.
-__device__ __forceinline__ bool plane_wait(const int* cnt, long long need, int limit = 1 << 24) {
-  for (int i = 0; i < limit; ++i) {
-    if (ld_acquire_gpu(cnt) >= need) {
-      fence_proxy_async_global();
-      return true;
-    }
-    __nanosleep(64);
-  }
-  return false;
-}
-
-// Publishes a finished phase-0 tile: its bulk stores have completed (caller
-// waited), made visible to later TMA loads of other CTAs, then counted.
-__device__ __forceinline__ void plane_publish(int* cnt) {
-  fence_proxy_async_global();
-  __threadfence();
-  atomicAdd(cnt, 1);
-}
-
-// Thread 0 keeps the schedule two tiles ahead of the tile being transformed,
-// so no global round trip sits between two tiles: while tile i is transformed,
-// the load of tile i+1 is in flight (issued if its plane was ready when polled
-// one tile earlier), the readiness poll of tile i+2's plane is in flight, and
-// the ticket of tile i+3 is being claimed.  A CTA blocks only when tile i+1's
-// plane was not ready: then it first publishes its own finished tiles (every
-// tile it holds unprocessed has a later ticket than the one it waits for), so
-// a chain of waits always ends at a CTA that can progress.
-// Thread 0's schedule state lives in shared memory (only the two values read
-// a whole transform after they were requested stay in registers), so the
-// transform itself keeps every register.
-struct PairSlot {
-  int tk;  // ticket (>= total: none)
-  int ph;
-  int tile;
+// This CTA's work items: per plane q of the cluster (p = cluster + q * clusters),
+// its phase-0 tiles r, r + CS, ... < n0, one barrier, its phase-1 tiles
+// r, r + CS, ... < n1.  Position `pos` within a plane: < a0 phase 0, == a0 the
+// barrier, > a0 phase 1.
+struct PlaneCursor {
+  long long q;
+  int pos;
 };
-struct PairState {
-  PairSlot cur, nx, nn;
-  int pend;       // plane of a phase-0 tile whose stores are issued, not yet published (-1: none)
-  int nx_loaded;  // the load of nx is in flight
-  int fail;       // a wait timed out
-};
-
-template <class T>
-__device__ __forceinline__ PairSlot pair_slot(const TmaPairArgs<T>& pa, int tk, long long total) {
-  PairSlot s{tk, 0, 0};
-  if (tk < total) {
-    long long tile;
-    pair_item(pa, tk, s.ph, tile);
-    s.tile = (int)tile;
-  }
-  return s;
-}
-
-// Publishes the pending phase-0 tile of thread 0's state (its stores complete first).
-__device__ __forceinline__ void publish_pending(PairState& S, int* cnt) {
-  if (S.pend >= 0) {
-    bulk_wait0();
-    plane_publish(cnt + S.pend);
-    S.pend = -1;
-  }
-}
 
 template <class T, bool INV, int V, bool IP>
 __global__ void __launch_bounds__(V == 2 ? 128 : 256,
@@ -587,110 +538,114 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
   C* end = IP ? slots[1] + pa.slot_elems : work + wl;
   unsigned long long* bars =
       reinterpret_cast<unsigned long long*>(reinterpret_cast<uintptr_t>(end + 1) & ~(uintptr_t)7);
-  int* s_tk = reinterpret_cast<int*>(bars + 2);            // [0] tile being transformed, [1] leave flag
-  PairState& S = *reinterpret_cast<PairState*>(s_tk + 2);  // thread 0 only
   const int tid = threadIdx.x;
-  int* const ticket = pa.sync;
-  int* const cnt = pa.sync + 1;
-  const long long total = pa.planes * (pa.n0 + pa.n1);
   unsigned* const err = pa.ph[0].err;
-  if (smem_u32(smraw) & 127) {  // the tile slots must start on 128 bytes: report, never copy
+  // a misaligned block is a plan error every CTA of the launch sees alike: no
+  // CTA copies, and none reaches a cluster barrier
+  if (smem_u32(smraw) & 127) {
     if (tid == 0) atomicExch(err, 1u);
     return;
   }
-  int nn_poll = 0;  // thread 0: plane counter of nn as polled one transform earlier
-  int nnn_tk = 0;   // thread 0: ticket claimed for the tile after nn
+  const int r = (int)cluster_rank(), CS = (int)cluster_nrank();
+  const long long cid = cluster_id(), ncl = cluster_count();
+  const long long nq = cid < pa.planes ? (pa.planes - 1 - cid) / ncl + 1 : 0;  // planes of this cluster
+  const int a0 = r < pa.n0 ? (pa.n0 - 1 - r) / CS + 1 : 0;                    // this CTA's tiles per phase
+  const int a1 = r < pa.n1 ? (pa.n1 - 1 - r) / CS + 1 : 0;
+  const int A = a0 + 1 + a1;  // items per plane, the barrier included
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     fence_proxy_async();
-    S.cur = pair_slot(pa, atomicAdd(ticket, 1), total);
-    S.nx = pair_slot(pa, atomicAdd(ticket, 1), total);
-    S.nn = pair_slot(pa, atomicAdd(ticket, 1), total);
-    S.pend = -1;
-    S.nx_loaded = 0;
-    S.fail = 0;
-    if (S.cur.tk < total) {
-      if (S.cur.ph == 1 && !plane_wait(cnt + S.cur.tile / pa.n1, pa.n0)) S.fail = 1;
-      if (!S.fail) tma_issue_load(pa.ph[S.cur.ph], S.cur.tile, slots[0], &bars[0]);
-    }
-    if (S.nx.tk < total && S.nx.ph == 1) nn_poll = ld_acquire_gpu(cnt + S.nx.tile / pa.n1);
-    if (S.fail) {
-      atomicExch(err, 1u);
-      S.cur.tk = (int)total;
-    }
-    s_tk[0] = S.cur.tk;
   }
   __syncthreads();
-  int tk = s_tk[0];
-  for (int it = 0; tk < total; ++it) {
-    const int cb = it & 1;
-    if (tid == 0) {
-      bulk_wait_read0();  // the previous tile's store has finished reading its buffer
-      // tile i+1: prefetch when its plane was ready at the last poll
-      S.nx_loaded = 0;
-      if (S.nx.tk < total && (S.nx.ph == 0 || nn_poll >= pa.n0)) {
-        if (S.nx.ph == 1) fence_proxy_async_global();
-        tma_issue_load(pa.ph[S.nx.ph], S.nx.tile, slots[cb ^ 1], &bars[cb ^ 1]);
-        S.nx_loaded = 1;
+  // item -> (phase, global tile index) for positions != a0
+  auto tile_of = [&](const PlaneCursor& c, int& ph) -> long long {
+    const long long p = cid + c.q * ncl;
+    if (c.pos < a0) {
+      ph = 0;
+      return p * pa.n0 + r + (long long)c.pos * CS;
+    }
+    ph = 1;
+    return p * pa.n1 + r + (long long)(c.pos - a0 - 1) * CS;
+  };
+  auto advance = [&](PlaneCursor c) {
+    if (++c.pos == A) {
+      c.pos = 0;
+      ++c.q;
+    }
+    return c;
+  };
+  unsigned par[2] = {0u, 0u};  // mbarrier phase of each slot
+  int cs = 0;                  // slot of the tile being transformed
+  bool bad = false;            // a bounded wait timed out: no more copies or transforms (barriers go on)
+  PlaneCursor cur{0, 0};
+  if (nq > 0 && tid == 0 && cur.pos != a0) {
+    int ph;
+    const long long tile = tile_of(cur, ph);
+    tma_issue_load(pa.ph[ph], tile, slots[0], &bars[0]);
+  }
+  while (cur.q < nq) {
+    if (cur.pos == a0) {
+      // the plane's phase-0 tiles of every CTA are complete and visible
+      if (tid == 0 && !bad) {
+        bulk_wait0();
+        fence_proxy_async_global();
       }
-      // tile i+2: poll its plane now, read the value a whole transform later
-      nn_poll = (S.nn.tk < total && S.nn.ph == 1) ? ld_acquire_gpu(cnt + S.nn.tile / pa.n1) : 0;
-      // tile i+3: claim its ticket now, use it after the transform
-      nnn_tk = atomicAdd(ticket, 1);
+      __syncthreads();
+      cluster_sync_all();
+      cur = advance(cur);
+      if (cur.q < nq && cur.pos != a0 && tid == 0 && !bad) {
+        fence_proxy_async_global();  // later tensor loads read what the barrier published
+        int ph;
+        const long long tile = tile_of(cur, ph);
+        cs ^= 1;
+        tma_issue_load(pa.ph[ph], tile, slots[cs], &bars[cs]);
+      } else if (cur.q < nq && cur.pos != a0) {
+        cs ^= 1;
+      }
+      continue;
     }
     int ph;
-    long long tile;
-    pair_item(pa, tk, ph, tile);
-    const TmaArgs<T>& a = pa.ph[ph];
-    const bool ok = mbar_wait(&bars[cb], (unsigned)((it >> 1) & 1));
-    if (__syncthreads_or(!ok)) {
+    const long long tile = tile_of(cur, ph);
+    const PlaneCursor nxt = advance(cur);
+    const bool prefetch = nxt.q < nq && nxt.pos != a0;  // no barrier between: load the next tile now
+    if (tid == 0 && !bad) {
+      bulk_wait_read0();  // the previous tile's store has finished reading its buffer
+      if (prefetch) {
+        int nph;
+        const long long ntile = tile_of(nxt, nph);
+        tma_issue_load(pa.ph[nph], ntile, slots[cs ^ 1], &bars[cs ^ 1]);
+      }
+    }
+    bool ok = true;
+    if (!bad) ok = mbar_wait(&bars[cs], par[cs]);
+    par[cs] ^= 1u;
+    if (__syncthreads_or(!ok) && !bad) {
+      bad = true;
       if (tid == 0) {
         atomicExch(err, 1u);
-        if (S.nx_loaded) mbar_wait(&bars[cb ^ 1], (unsigned)(((it + 1) >> 1) & 1));
+        if (prefetch) mbar_wait(&bars[cs ^ 1], par[cs ^ 1]);  // let the prefetch land (bounded)
         bulk_wait0();
       }
-      return;
     }
-    const bool lm = a.mode == 1;
-    const int L = a.L, P = a.P;
-    // a phase with fewer threads than the CTA leaves the rest idle (no
-    // butterflies: t beyond every stage's count), still at every barrier
-    const bool act = tid < L * P;
-    const int l = !act ? 0 : lm ? tid % L : tid / P;
-    const int t = !act ? (1 << 20) : lm ? tid / L : tid % P;
-    C* obuf = tma_stages<T, INV, V, IP>(a, slots[cb], work, a.tw, l, t);
-    fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      publish_pending(S, cnt);  // the previous phase-0 tile's stores are long done
-      tma_issue_store(a, tile, obuf);
-      if (ph == 0) S.pend = (int)(tile / pa.n0);
-      if (S.nx.tk < total && !S.nx_loaded) {
-        // tile i+1 waits on a plane: publish ours first (it may be one of the
-        // tiles waited for), then wait and load
-        publish_pending(S, cnt);
-        if (plane_wait(cnt + S.nx.tile / pa.n1, pa.n0)) {
-          tma_issue_load(pa.ph[S.nx.ph], S.nx.tile, slots[cb ^ 1], &bars[cb ^ 1]);
-        } else {
-          atomicExch(err, 1u);
-          S.fail = 1;
-        }
-      }
-      S.cur = S.nx;
-      S.nx = S.nn;
-      S.nn = pair_slot(pa, nnn_tk, total);
-      s_tk[0] = S.cur.tk;
-      s_tk[1] = S.fail;
+    if (!bad) {
+      const TmaArgs<T>& a = pa.ph[ph];
+      const bool lm = a.mode == 1;
+      const int L = a.L, P = a.P;
+      // a phase with fewer threads than the CTA leaves the rest idle (no
+      // butterflies: t beyond every stage's count), still at every barrier
+      const bool act = tid < L * P;
+      const int l = !act ? 0 : lm ? tid % L : tid / P;
+      const int t = !act ? (1 << 20) : lm ? tid / L : tid % P;
+      C* obuf = tma_stages<T, INV, V, IP>(a, slots[cs], work, a.tw, l, t);
+      fence_proxy_async();
+      __syncthreads();
+      if (tid == 0) tma_issue_store(a, tile, obuf);
     }
-    __syncthreads();
-    if (s_tk[1]) break;  // a wait timed out: leave (the error word is set)
-    tk = s_tk[0];
+    if (prefetch) cs ^= 1;
+    cur = nxt;
   }
-  if (tid == 0) {
-    bulk_wait0();
-    publish_pending(S, cnt);
-  }
+  if (tid == 0 && !bad) bulk_wait0();
 }
 
 // ─────────────────────────────── host side ───────────────────────────────
@@ -914,11 +869,26 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
   return cudaGetLastError();
 }
 
+template <class T, bool INV> static const void* pair_kernel_ptr(int variant, bool ip) {
+  auto k = variant == 4   ? tma_pair_kernel<T, INV, 4, true>
+           : variant == 2 ? tma_pair_kernel<T, INV, 2, true>
+           : variant == 1 ? (ip ? tma_pair_kernel<T, INV, 1, true> : tma_pair_kernel<T, INV, 1, false>)
+                          : tma_pair_kernel<T, INV, 3, false>;
+  return reinterpret_cast<const void*>(k);
+}
+static const void* pair_kernel_ptr(bool dbl, bool inv, int variant, bool ip) {
+  if (dbl) return inv ? pair_kernel_ptr<double, true>(variant, ip) : pair_kernel_ptr<double, false>(variant, ip);
+  return inv ? pair_kernel_ptr<float, true>(variant, ip) : pair_kernel_ptr<float, false>(variant, ip);
+}
+
 // Two axis passes of the same x-planes in one launch (tma_pair_kernel).  Both
-// phases must run on the same kernel build, and each tile must lie inside one
-// plane; the CTA gets the larger of the two phases' thread counts.
+// phases must run on the same kernel build; the CTA gets the larger of the
+// two phases' thread counts.  The cluster size is chosen by a small cost
+// model: rounds of planes (planes / clusters in flight) times the tiles a CTA
+// transforms per plane plus about half a tile for the barrier, with the
+// planes in flight held to 56 MiB of L2.
 bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes, long long plane_bytes, bool dbl,
-                   TmaPairPlan& pp) {
+                   bool inv, TmaPairPlan& pp) {
   static const int on = [] {
     const char* e = getenv("AFC_PAIR");
     return e && *e ? atoi(e) : 1;
@@ -935,14 +905,13 @@ bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes,
     if (!tma_plan(d.sl, d.ld, d.lanes, d.im, d.om, d.in, d.out, dbl, 0, tp, rin, rout)) return false;
     if (d.lanes % planes) return false;
     if (tp.mode == 0) {
-      const long long lpp = d.lanes / planes;
-      if (lpp % tp.L) return false;
-      pp.n[ph] = lpp / tp.L;
+      pp.lpp[ph] = d.lanes / planes;
+      pp.n[ph] = (int)((pp.lpp[ph] + tp.L - 1) / tp.L);
     } else {
       if (tp.outer != planes) return false;
-      pp.n[ph] = tp.kb;
+      pp.lpp[ph] = 0;
+      pp.n[ph] = (int)tp.kb;
     }
-    if (tp.ntiles != planes * pp.n[ph]) return false;
   }
   const TmaPlan &a = pp.ph[0], &b = pp.ph[1];
   if (a.variant != b.variant || a.inplace != b.inplace) return false;
@@ -951,64 +920,97 @@ bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes,
   pp.slot_elems = std::max(a.slot_elems, b.slot_elems);
   pp.threads = std::max(a.L * a.P, b.L * b.P);
   if (pp.threads > (a.variant == 2 ? 128 : 256)) return false;
-  // + barriers, the tile ticket and thread 0's schedule state (PairState)
   pp.smem = 2 * (size_t)pp.slot_elems * csz +
-            (a.inplace ? 0 : (size_t)std::max(a.L * a.ld, b.L * b.ld) * csz) + 128;
+            (a.inplace ? 0 : (size_t)std::max(a.L * a.ld, b.L * b.ld) * csz) + 64;
   if (pp.smem > 220 * 1024) return false;
   pp.planes = planes;
-  // lag: about twice the planes the resident CTAs work on at once, so a
-  // plane's phase-0 tiles are published well before its phase-1 tiles start;
-  // but the planes between a plane's two phases must stay in L2 (126 MB):
-  // at most 48 MiB of them, and at least one plane
-  const long long resident = (long long)sm_count() * (a.variant == 2 ? 3 : 2);
-  const long long want = std::max<long long>(4, 2 * resident / (pp.n[0] + pp.n[1]) + 2);
-  const long long fit = std::max<long long>(1, (48ll << 20) / std::max<long long>(plane_bytes, 1));
-  if (plane_bytes > (64ll << 20)) return false;  // two planes in flight would not fit in L2
-  pp.lag = std::min<long long>(planes, std::min(want, fit));
-  return true;
+  const void* k = pair_kernel_ptr(dbl, inv, a.variant, a.inplace);
+  if (kernel_smem_grant(k, pp.smem) != cudaSuccess) return false;
+  const long long budget = 56ll << 20;
+  double best = 0;
+  pp.cs = 0;
+  for (int cs : {4, 8, 16}) {
+    if (cs == 16 && cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(cs, 1, 1);
+    cfg.blockDim = dim3(pp.threads, 1, 1);
+    cfg.dynamicSmemBytes = pp.smem;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int ncl = 0;
+    if (cudaOccupancyMaxActiveClusters(&ncl, k, &cfg) != cudaSuccess || ncl < 1) {
+      cudaGetLastError();
+      continue;
+    }
+    const long long want = std::min<long long>(ncl, planes);
+    const long long use = std::min<long long>(want, std::max<long long>(1, budget / std::max<long long>(plane_bytes, 1)));
+    // planes too large for the L2 budget would leave most SMs idle: the
+    // separate passes are faster then
+    if (2 * use < want) continue;
+    const long long rounds = (planes + use - 1) / use;
+    const double per = (double)((pp.n[0] + cs - 1) / cs + (pp.n[1] + cs - 1) / cs) + 0.6;
+    const double cost = (double)rounds * per;
+    if (!pp.cs || cost < best) {
+      best = cost;
+      pp.cs = cs;
+      pp.nclusters = (int)use;
+    }
+  }
+  return pp.cs > 0;
 }
 
-size_t tma_pair_sync_bytes(long long planes) { return (size_t)((planes + 1) * sizeof(int) + 255) / 256 * 256; }
-
 template <class T, bool INV>
-static cudaError_t launch_tma_pair_t(const LaunchDesc& d0, const LaunchDesc& d1, const TmaPairPlan& pp, int* sync,
-                                     unsigned* err, cudaStream_t st) {
-  const int v = pp.ph[0].variant;
-  const bool ip = pp.ph[0].inplace;
-  auto k = v == 4   ? tma_pair_kernel<T, INV, 4, true>
-           : v == 2 ? tma_pair_kernel<T, INV, 2, true>
-           : v == 1 ? (ip ? tma_pair_kernel<T, INV, 1, true> : tma_pair_kernel<T, INV, 1, false>)
-                    : tma_pair_kernel<T, INV, 3, false>;
-  cudaError_t e = kernel_smem_grant(reinterpret_cast<const void*>(k), pp.smem);
+static cudaError_t launch_tma_pair_t(const LaunchDesc& d0, const LaunchDesc& d1, const TmaPairPlan& pp, unsigned* err,
+                                     cudaStream_t st) {
+  const void* k = pair_kernel_ptr<T, INV>(pp.ph[0].variant, pp.ph[0].inplace);
+  cudaError_t e = kernel_smem_grant(k, pp.smem);
   if (e != cudaSuccess) return e;
   TmaPairArgs<T> a;
   memset(&a, 0, sizeof(a));
   if (!fill_tma_args<T>(d0, pp.ph[0], err, a.ph[0]) || !fill_tma_args<T>(d1, pp.ph[1], err, a.ph[1]))
     return cudaErrorInvalidValue;
+  for (int ph = 0; ph < 2; ++ph)
+    if (pp.ph[ph].mode == 0) {  // tiles never straddle a plane
+      a.ph[ph].tpp = pp.n[ph];
+      a.ph[ph].lpp = pp.lpp[ph];
+    }
   a.planes = pp.planes;
   a.n0 = pp.n[0];
   a.n1 = pp.n[1];
-  a.lag = pp.lag;
   a.slot_elems = pp.slot_elems;
-  a.sync = sync;
-  e = cudaMemsetAsync(sync, 0, tma_pair_sync_bytes(pp.planes), st);
-  if (e != cudaSuccess) return e;
-  const int per_sm = kernel_ctas_per_sm(reinterpret_cast<const void*>(k), pp.threads, pp.smem);
-  long long grid = (long long)sm_count() * per_sm;
-  const long long total = pp.planes * (pp.n[0] + pp.n[1]);
-  if (grid > total) grid = total;
-  k<<<(unsigned)grid, pp.threads, pp.smem, st>>>(a);
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = pp.cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3((unsigned)(pp.nclusters * pp.cs), 1, 1);
+  cfg.blockDim = dim3(pp.threads, 1, 1);
+  cfg.dynamicSmemBytes = pp.smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  void* args[] = {&a};
+  e = cudaLaunchKernelExC(&cfg, k, args);
   count_launch(1);
-  return cudaGetLastError();
+  return e;
 }
 
-cudaError_t launch_tma_pair(const LaunchDesc& d0, const LaunchDesc& d1, const TmaPairPlan& pp, int* sync,
-                            unsigned* err, bool dbl, bool inv, cudaStream_t st) {
+cudaError_t launch_tma_pair(const LaunchDesc& d0, const LaunchDesc& d1, const TmaPairPlan& pp, unsigned* err,
+                            bool dbl, bool inv, cudaStream_t st) {
   if (dbl)
-    return inv ? launch_tma_pair_t<double, true>(d0, d1, pp, sync, err, st)
-               : launch_tma_pair_t<double, false>(d0, d1, pp, sync, err, st);
-  return inv ? launch_tma_pair_t<float, true>(d0, d1, pp, sync, err, st)
-             : launch_tma_pair_t<float, false>(d0, d1, pp, sync, err, st);
+    return inv ? launch_tma_pair_t<double, true>(d0, d1, pp, err, st)
+               : launch_tma_pair_t<double, false>(d0, d1, pp, err, st);
+  return inv ? launch_tma_pair_t<float, true>(d0, d1, pp, err, st)
+             : launch_tma_pair_t<float, false>(d0, d1, pp, err, st);
 }
 
 cudaError_t launch_tma(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, bool dbl, bool inv, cudaStream_t st) {
