@@ -515,11 +515,67 @@ __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence
 // This CTA's work items: per plane q of the cluster (p = cluster + q * clusters),
 // its phase-0 tiles r, r + CS, ... < n0, one barrier, its phase-1 tiles
 // r, r + CS, ... < n1.  Position `pos` within a plane: < a0 phase 0, == a0 the
-// barrier, > a0 phase 1.
-struct PlaneCursor {
-  long long q;
-  int pos;
+// barrier, > a0 phase 1.  The schedule lives in shared memory, written by
+// thread 0 and read by every thread after a CTA barrier: nothing of it is live
+// in registers while a tile is transformed (the stages of the complex128
+// build use all 168 registers the three-CTA occupancy allows).
+struct PairCtl {
+  int q, pos;     // the item being processed
+  int cs;         // slot of the tile being transformed
+  int par[2];     // mbarrier phase of each slot
+  int bad;        // a bounded wait timed out: no more copies or transforms (barriers go on)
+  int prefetch;   // the next item is a tile whose load was issued with this one's transform
 };
+
+struct PairGeo {
+  int r, CS, a0, a1, A;
+  long long cid, ncl, nq;
+};
+
+template <class T> __device__ __forceinline__ PairGeo pair_geo(const TmaPairArgs<T>& pa) {
+  PairGeo g;
+  g.r = (int)cluster_rank();
+  g.CS = (int)cluster_nrank();
+  g.cid = cluster_id();
+  g.ncl = cluster_count();
+  g.nq = g.cid < pa.planes ? (pa.planes - 1 - g.cid) / g.ncl + 1 : 0;  // planes of this cluster
+  g.a0 = g.r < pa.n0 ? (pa.n0 - 1 - g.r) / g.CS + 1 : 0;               // this CTA's tiles per phase
+  g.a1 = g.r < pa.n1 ? (pa.n1 - 1 - g.r) / g.CS + 1 : 0;
+  g.A = g.a0 + 1 + g.a1;  // items per plane, the barrier included
+  return g;
+}
+
+// (phase, global tile) of the item at (q, pos), pos != a0
+template <class T>
+__device__ __forceinline__ long long pair_tile(const TmaPairArgs<T>& pa, const PairGeo& g, int q, int pos, int& ph) {
+  const long long p = g.cid + (long long)q * g.ncl;
+  if (pos < g.a0) {
+    ph = 0;
+    return p * pa.n0 + g.r + (long long)pos * g.CS;
+  }
+  ph = 1;
+  return p * pa.n1 + g.r + (long long)(pos - g.a0 - 1) * g.CS;
+}
+
+__device__ __forceinline__ void pair_advance(const PairGeo& g, int& q, int& pos) {
+  if (++pos == g.A) {
+    pos = 0;
+    ++q;
+  }
+}
+
+template <class T, bool INV, int V, bool IP>
+__device__ __forceinline__ typename CT<T>::type* pair_transform(const TmaArgs<T>& a, typename CT<T>::type* slot,
+                                                                typename CT<T>::type* work, int tid) {
+  const bool lm = a.mode == 1;
+  const int L = a.L, P = a.P;
+  // a phase with fewer threads than the CTA leaves the rest idle (no
+  // butterflies: t beyond every stage's count), still at every barrier
+  const bool act = tid < L * P;
+  const int l = !act ? 0 : lm ? tid % L : tid / P;
+  const int t = !act ? (1 << 20) : lm ? tid / L : tid % P;
+  return tma_stages<T, INV, V, IP>(a, slot, work, a.tw, l, t);
+}
 
 template <class T, bool INV, int V, bool IP>
 __global__ void __launch_bounds__(V == 2 ? 128 : 256,
@@ -529,123 +585,132 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
   // no static shared variables: they would move the dynamic block off the
   // 128-byte boundary the tensor copies' destinations need
   extern __shared__ __align__(128) unsigned char smraw[];
-  C* slots[2];
-  slots[0] = reinterpret_cast<C*>(smraw);
-  slots[1] = slots[0] + pa.slot_elems;
+  C* const slot0 = reinterpret_cast<C*>(smraw);
+  C* const slot1 = slot0 + pa.slot_elems;
   int wl = pa.ph[0].L * pa.ph[0].ld;
   if (pa.ph[1].L * pa.ph[1].ld > wl) wl = pa.ph[1].L * pa.ph[1].ld;
-  C* work = IP ? nullptr : slots[1] + pa.slot_elems;
-  C* end = IP ? slots[1] + pa.slot_elems : work + wl;
-  unsigned long long* bars =
+  C* const work = IP ? nullptr : slot1 + pa.slot_elems;
+  C* end = IP ? slot1 + pa.slot_elems : work + wl;
+  unsigned long long* const bars =
       reinterpret_cast<unsigned long long*>(reinterpret_cast<uintptr_t>(end + 1) & ~(uintptr_t)7);
+  volatile PairCtl* const ctl = reinterpret_cast<volatile PairCtl*>(bars + 2);
   const int tid = threadIdx.x;
-  unsigned* const err = pa.ph[0].err;
   // a misaligned block is a plan error every CTA of the launch sees alike: no
   // CTA copies, and none reaches a cluster barrier
   if (smem_u32(smraw) & 127) {
-    if (tid == 0) atomicExch(err, 1u);
+    if (tid == 0) atomicExch(pa.ph[0].err, 1u);
     return;
   }
-  const int r = (int)cluster_rank(), CS = (int)cluster_nrank();
-  const long long cid = cluster_id(), ncl = cluster_count();
-  const long long nq = cid < pa.planes ? (pa.planes - 1 - cid) / ncl + 1 : 0;  // planes of this cluster
-  const int a0 = r < pa.n0 ? (pa.n0 - 1 - r) / CS + 1 : 0;                    // this CTA's tiles per phase
-  const int a1 = r < pa.n1 ? (pa.n1 - 1 - r) / CS + 1 : 0;
-  const int A = a0 + 1 + a1;  // items per plane, the barrier included
   if (tid == 0) {
+    const PairGeo g = pair_geo(pa);
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     fence_proxy_async();
+    ctl->q = g.nq > 0 ? 0 : 1 << 30;
+    ctl->pos = 0;
+    ctl->cs = 0;
+    ctl->par[0] = ctl->par[1] = 0;
+    ctl->bad = 0;
+    ctl->prefetch = 0;
+    if (g.nq > 0 && g.a0 > 0) {
+      int ph;
+      const long long tile = pair_tile(pa, g, 0, 0, ph);
+      tma_issue_load(pa.ph[ph], tile, slot0, &bars[0]);
+    }
   }
   __syncthreads();
-  // item -> (phase, global tile index) for positions != a0
-  auto tile_of = [&](const PlaneCursor& c, int& ph) -> long long {
-    const long long p = cid + c.q * ncl;
-    if (c.pos < a0) {
-      ph = 0;
-      return p * pa.n0 + r + (long long)c.pos * CS;
-    }
-    ph = 1;
-    return p * pa.n1 + r + (long long)(c.pos - a0 - 1) * CS;
-  };
-  auto advance = [&](PlaneCursor c) {
-    if (++c.pos == A) {
-      c.pos = 0;
-      ++c.q;
-    }
-    return c;
-  };
-  unsigned par[2] = {0u, 0u};  // mbarrier phase of each slot
-  int cs = 0;                  // slot of the tile being transformed
-  bool bad = false;            // a bounded wait timed out: no more copies or transforms (barriers go on)
-  PlaneCursor cur{0, 0};
-  if (nq > 0 && tid == 0 && cur.pos != a0) {
-    int ph;
-    const long long tile = tile_of(cur, ph);
-    tma_issue_load(pa.ph[ph], tile, slots[0], &bars[0]);
-  }
-  while (cur.q < nq) {
-    if (cur.pos == a0) {
-      // the plane's phase-0 tiles of every CTA are complete and visible
-      if (tid == 0 && !bad) {
-        bulk_wait0();
-        fence_proxy_async_global();
+  for (;;) {
+    // every thread reads the item; thread 0 wrote it before the last barrier
+    const int q = ctl->q;
+    if (q >= (1 << 30)) break;
+    const int bad = ctl->bad;
+    if (ctl->pos < 0) {
+      // the barrier between a plane's phases: this CTA's phase-0 stores are
+      // complete and visible before any CTA of the cluster loads phase-1 tiles
+      cluster_sync_all();
+      if (tid == 0) {
+        const PairGeo g = pair_geo(pa);
+        int nq_ = q, pos = g.a0;
+        pair_advance(g, nq_, pos);
+        if (nq_ < g.nq && pos != g.a0 && !bad) {
+          fence_proxy_async_global();  // the tensor loads below read what the barrier published
+          int ph;
+          const long long tile = pair_tile(pa, g, nq_, pos, ph);
+          const int cs = ctl->cs ^ 1;
+          tma_issue_load(pa.ph[ph], tile, cs ? slot1 : slot0, &bars[cs]);
+          ctl->cs = cs;
+        } else if (nq_ < g.nq && pos != g.a0) {
+          ctl->cs ^= 1;
+        }
+        ctl->q = nq_ < g.nq ? nq_ : 1 << 30;
+        ctl->pos = pos == g.a0 ? -1 : pos;
       }
       __syncthreads();
-      cluster_sync_all();
-      cur = advance(cur);
-      if (cur.q < nq && cur.pos != a0 && tid == 0 && !bad) {
-        fence_proxy_async_global();  // later tensor loads read what the barrier published
-        int ph;
-        const long long tile = tile_of(cur, ph);
-        cs ^= 1;
-        tma_issue_load(pa.ph[ph], tile, slots[cs], &bars[cs]);
-      } else if (cur.q < nq && cur.pos != a0) {
-        cs ^= 1;
-      }
       continue;
     }
-    int ph;
-    const long long tile = tile_of(cur, ph);
-    const PlaneCursor nxt = advance(cur);
-    const bool prefetch = nxt.q < nq && nxt.pos != a0;  // no barrier between: load the next tile now
-    if (tid == 0 && !bad) {
-      bulk_wait_read0();  // the previous tile's store has finished reading its buffer
-      if (prefetch) {
-        int nph;
-        const long long ntile = tile_of(nxt, nph);
-        tma_issue_load(pa.ph[nph], ntile, slots[cs ^ 1], &bars[cs ^ 1]);
+    const int cs = ctl->cs;
+    const unsigned par = (unsigned)ctl->par[cs];
+    C* const cur = cs ? slot1 : slot0;
+    int ph = 0;
+    if (tid == 0) {
+      const PairGeo g = pair_geo(pa);
+      const int pos = ctl->pos;
+      int nq_ = q, npos = pos;
+      pair_advance(g, nq_, npos);
+      const bool prefetch = nq_ < g.nq && npos != g.a0;  // no barrier between: load the next tile now
+      ctl->prefetch = prefetch;
+      if (!bad) {
+        bulk_wait_read0();  // the previous tile's store has finished reading its buffer
+        if (prefetch) {
+          int nph;
+          const long long ntile = pair_tile(pa, g, nq_, npos, nph);
+          tma_issue_load(pa.ph[nph], ntile, cs ? slot0 : slot1, &bars[cs ^ 1]);
+        }
       }
     }
     bool ok = true;
-    if (!bad) ok = mbar_wait(&bars[cs], par[cs]);
-    par[cs] ^= 1u;
-    if (__syncthreads_or(!ok) && !bad) {
-      bad = true;
-      if (tid == 0) {
-        atomicExch(err, 1u);
-        if (prefetch) mbar_wait(&bars[cs ^ 1], par[cs ^ 1]);  // let the prefetch land (bounded)
+    if (!bad) ok = mbar_wait(&bars[cs], par);
+    const bool timed_out = __syncthreads_or(!ok);
+    if (tid == 0) {
+      ctl->par[cs] = (int)(par ^ 1u);
+      if (timed_out && !bad) {
+        atomicExch(pa.ph[0].err, 1u);
+        if (ctl->prefetch) mbar_wait(&bars[cs ^ 1], (unsigned)ctl->par[cs ^ 1]);  // let it land (bounded)
         bulk_wait0();
+        ctl->bad = 1;
       }
     }
-    if (!bad) {
-      const TmaArgs<T>& a = pa.ph[ph];
-      const bool lm = a.mode == 1;
-      const int L = a.L, P = a.P;
-      // a phase with fewer threads than the CTA leaves the rest idle (no
-      // butterflies: t beyond every stage's count), still at every barrier
-      const bool act = tid < L * P;
-      const int l = !act ? 0 : lm ? tid % L : tid / P;
-      const int t = !act ? (1 << 20) : lm ? tid / L : tid % P;
-      C* obuf = tma_stages<T, INV, V, IP>(a, slots[cs], work, a.tw, l, t);
+    if (!bad && !timed_out) {
+      ph = ctl->pos < pair_geo(pa).a0 ? 0 : 1;
+      C* obuf = pair_transform<T, INV, V, IP>(pa.ph[ph], cur, work, tid);
       fence_proxy_async();
       __syncthreads();
-      if (tid == 0) tma_issue_store(a, tile, obuf);
+      if (tid == 0) {
+        const PairGeo g = pair_geo(pa);
+        int tph;
+        const long long tile = pair_tile(pa, g, ctl->q, ctl->pos, tph);
+        tma_issue_store(pa.ph[tph], tile, obuf);
+      }
     }
-    if (prefetch) cs ^= 1;
-    cur = nxt;
+    if (tid == 0) {
+      const PairGeo g = pair_geo(pa);
+      int nq_ = ctl->q, npos = ctl->pos;
+      pair_advance(g, nq_, npos);
+      if (ctl->prefetch) ctl->cs = cs ^ 1;
+      if (nq_ < g.nq && npos == g.a0) {
+        // the plane's barrier comes next: complete and publish this CTA's stores
+        if (!ctl->bad) {
+          bulk_wait0();
+          fence_proxy_async_global();
+        }
+        npos = -1;
+      }
+      ctl->q = nq_ < g.nq ? nq_ : 1 << 30;
+      ctl->pos = npos;
+    }
+    __syncthreads();
   }
-  if (tid == 0 && !bad) bulk_wait0();
+  if (tid == 0 && !ctl->bad) bulk_wait0();
 }
 
 // ─────────────────────────────── host side ───────────────────────────────
