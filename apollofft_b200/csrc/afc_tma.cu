@@ -607,7 +607,7 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
     mbar_init(&bars[1], 1);
     fence_proxy_async();
     ctl->q = g.nq > 0 ? 0 : 1 << 30;
-    ctl->pos = 0;
+    ctl->pos = g.a0 == 0 ? -1 : 0;  // no phase-0 tile here: the plane starts at its barrier
     ctl->cs = 0;
     ctl->par[0] = ctl->par[1] = 0;
     ctl->bad = 0;
