@@ -84,6 +84,8 @@ struct TmaPlan {
   // contiguous in-place tiles only: real input lanes (widened in the first
   // stage) / real output lanes (real parts stored by the last stage)
   bool real_in = false, real_out = false;
+  // twiddle entries kept resident in shared memory by persistent CTAs (0: read from global)
+  int tw_res = 0;
 };
 bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, const LaneMap& om, const void* in,
               void* out, bool dbl, int lanes_pref, TmaPlan& tp, bool real_in = false, bool real_out = false);

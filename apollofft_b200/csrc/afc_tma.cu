@@ -43,6 +43,7 @@ template <class T> struct TmaArgs {
   int real_out;     // contiguous in-place mode: output lanes are the real parts
   int nbx, bn;      // boxes along the transformed axis, rows per box
   unsigned tw_bytes;  // > 0: one tile per CTA, the twiddle table is copied into the idle second slot
+  int tw_res;         // > 0: persistent CTAs keep the first tw_res twiddles resident in shared memory
   long long tpp, lpp; // contiguous mode, tpp > 0: tiles never straddle planes of lpp lanes (tpp tiles per
                       // plane, the last one of a plane shorter); tpp = 0: tile q covers lanes [q L, q L + L)
   T scale;
@@ -410,7 +411,8 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
   slots[0] = reinterpret_cast<C*>(smraw);
   slots[1] = slots[0] + a.slot_elems;
   C* work = IP ? nullptr : slots[1] + a.slot_elems;
-  C* end = IP ? slots[1] + a.slot_elems : work + (long long)L * ld;
+  C* twsm = IP ? slots[1] + a.slot_elems : work + (long long)L * ld;  // resident twiddles (a.tw_res)
+  C* end = twsm + a.tw_res;
   unsigned long long* bars =
       reinterpret_cast<unsigned long long*>(reinterpret_cast<uintptr_t>(end + 1) & ~(uintptr_t)7);
   const bool lm = a.mode == 1;
@@ -427,13 +429,15 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     fence_proxy_async();
+    // a CTA with a single tile never prefetches into the second slot: the
+    // twiddle table is staged there with the tile (stage twiddles then come
+    // from shared memory instead of L1 misses to L2)
+    tma_issue_load(a, tile, slots[0], &bars[0], a.tw_bytes ? slots[1] : nullptr);
   }
+  // a persistent CTA copies the table once into its own region
+  for (int i = tid; i < a.tw_res; i += blockDim.x) twsm[i] = a.tw[i];
   __syncthreads();
-  // a CTA with a single tile never prefetches into the second slot: the
-  // twiddle table is staged there with the tile (stage twiddles then come from
-  // shared memory instead of L1 misses to L2)
-  if (tid == 0) tma_issue_load(a, tile, slots[0], &bars[0], a.tw_bytes ? slots[1] : nullptr);
-  const C* twb = a.tw_bytes ? slots[1] : a.tw;
+  const C* twb = a.tw_res ? twsm : a.tw_bytes ? slots[1] : a.tw;
   for (int it = 0;; ++it) {
     const int cb = it & 1;
     const long long nxt = tile + gridDim.x;
@@ -566,7 +570,8 @@ __device__ __forceinline__ void pair_advance(const PairGeo& g, int& q, int& pos)
 
 template <class T, bool INV, int V, bool IP>
 __device__ __forceinline__ typename CT<T>::type* pair_transform(const TmaArgs<T>& a, typename CT<T>::type* slot,
-                                                                typename CT<T>::type* work, int tid) {
+                                                                typename CT<T>::type* work,
+                                                                const typename CT<T>::type* tw, int tid) {
   const bool lm = a.mode == 1;
   const int L = a.L, P = a.P;
   // a phase with fewer threads than the CTA leaves the rest idle (no
@@ -574,7 +579,7 @@ __device__ __forceinline__ typename CT<T>::type* pair_transform(const TmaArgs<T>
   const bool act = tid < L * P;
   const int l = !act ? 0 : lm ? tid % L : tid / P;
   const int t = !act ? (1 << 20) : lm ? tid / L : tid % P;
-  return tma_stages<T, INV, V, IP>(a, slot, work, a.tw, l, t);
+  return tma_stages<T, INV, V, IP>(a, slot, work, tw, l, t);
 }
 
 template <class T, bool INV, int V, bool IP>
@@ -590,7 +595,9 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
   int wl = pa.ph[0].L * pa.ph[0].ld;
   if (pa.ph[1].L * pa.ph[1].ld > wl) wl = pa.ph[1].L * pa.ph[1].ld;
   C* const work = IP ? nullptr : slot1 + pa.slot_elems;
-  C* end = IP ? slot1 + pa.slot_elems : work + wl;
+  C* const tw0 = IP ? slot1 + pa.slot_elems : work + wl;  // resident twiddles of each phase (tw_res)
+  C* const tw1 = tw0 + pa.ph[0].tw_res;
+  C* end = tw1 + pa.ph[1].tw_res;
   unsigned long long* const bars =
       reinterpret_cast<unsigned long long*>(reinterpret_cast<uintptr_t>(end + 1) & ~(uintptr_t)7);
   volatile PairCtl* const ctl = reinterpret_cast<volatile PairCtl*>(bars + 2);
@@ -618,6 +625,8 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
       tma_issue_load(pa.ph[ph], tile, slot0, &bars[0]);
     }
   }
+  for (int i = tid; i < pa.ph[0].tw_res; i += blockDim.x) tw0[i] = pa.ph[0].tw[i];
+  for (int i = tid; i < pa.ph[1].tw_res; i += blockDim.x) tw1[i] = pa.ph[1].tw[i];
   __syncthreads();
   for (;;) {
     // every thread reads the item; thread 0 wrote it before the last barrier
@@ -682,7 +691,8 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
     }
     if (!bad && !timed_out) {
       ph = ctl->pos < pair_geo(pa).a0 ? 0 : 1;
-      C* obuf = pair_transform<T, INV, V, IP>(pa.ph[ph], cur, work, tid);
+      C* obuf = pair_transform<T, INV, V, IP>(pa.ph[ph], cur, work, pa.ph[ph].tw_res ? (ph ? tw1 : tw0) : pa.ph[ph].tw,
+                                              tid);
       fence_proxy_async();
       __syncthreads();
       if (tid == 0) {
@@ -751,7 +761,35 @@ static bool make_map(CUtensorMap* m, const void* base, bool dbl, long long es, l
 static int g_tma_sm = 0;
 
 size_t tma_smem_bytes(const TmaPlan& tp, size_t csz) {
-  return 2 * (size_t)tp.slot_elems * csz + (tp.inplace ? 0 : (size_t)tp.L * tp.ld * csz) + 64;
+  return 2 * (size_t)tp.slot_elems * csz + (tp.inplace ? 0 : (size_t)tp.L * tp.ld * csz) + (size_t)tp.tw_res * csz + 64;
+}
+
+// Twiddle entries the stages read (r-major, twoff + (R - 1) Ns per stage).
+static long long twiddle_count(const StageList& sl) {
+  long long twc = 0;
+  for (int s = 0; s < sl.nst; ++s)
+    if (sl.st[s].Ns > 1) twc = std::max<long long>(twc, sl.st[s].twoff + (long long)(sl.st[s].R - 1) * sl.st[s].Ns);
+  return twc;
+}
+
+// CTAs per SM the register budget of a kernel build allows (its launch bounds).
+static int build_ctas_per_sm(int variant, bool dbl) {
+  if (variant == 2) return 3;
+  if (variant == 3 || ((variant == 1 || variant == 4) && !dbl)) return 2;
+  return 1;
+}
+
+// Keeps the twiddle table resident in shared memory when that costs no CTA
+// per SM (228 KB per SM, 1 KB reserved per CTA).
+static void plan_resident_twiddles(const StageList& sl, bool dbl, TmaPlan& tp, size_t extra = 0) {
+  const size_t csz = dbl ? 16 : 8;
+  tp.tw_res = 0;
+  const long long twc = twiddle_count(sl);
+  if (twc <= 0) return;
+  const size_t base = tma_smem_bytes(tp, csz) + extra;
+  const int ctas = build_ctas_per_sm(tp.variant, dbl);
+  if ((size_t)ctas * (base + (size_t)twc * csz + 1024) <= 233472 && base + (size_t)twc * csz <= 220 * 1024)
+    tp.tw_res = (int)twc;
 }
 
 // Decides whether an axis pass can run on the TMA kernel and with which tiles.
@@ -856,6 +894,7 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
     tp.slot_elems = (int)se;
   }
   if (tma_smem_bytes(tp, csz) > 220 * 1024) return false;
+  plan_resident_twiddles(sl, dbl, tp);
   tp.ntiles = tp.mode == 0 ? (lanes + tp.L - 1) / tp.L : (lanes / im.es) * tp.kb;
   tp.outer = tp.mode == 1 ? lanes / im.es : 0;
   return true;
@@ -890,6 +929,7 @@ template <class T> static bool fill_tma_args(const LaunchDesc& d, const TmaPlan&
   a.bn = tp.bn;
   a.scale = (T)d.scale;
   a.err = err;
+  a.tw_res = tp.tw_res;
   return true;
 }
 
@@ -921,12 +961,12 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
   if (grid >= tp.ntiles) {
     // one tile per CTA: stage the twiddle table (r-major, twoff + (R - 1) Ns
     // entries per stage) in the second slot when it fits and can be bulk-copied
-    long long twc = 0;
-    for (int s = 0; s < d.sl.nst; ++s)
-      if (d.sl.st[s].Ns > 1) twc = std::max<long long>(twc, d.sl.st[s].twoff + (long long)(d.sl.st[s].R - 1) * d.sl.st[s].Ns);
+    const long long twc = twiddle_count(d.sl);
     const long long twb = twc * (long long)sizeof(C);
-    if (twc > 0 && twb % 16 == 0 && twc <= tp.slot_elems && (reinterpret_cast<uintptr_t>(d.tw) & 15) == 0)
+    if (twc > 0 && twb % 16 == 0 && twc <= tp.slot_elems && (reinterpret_cast<uintptr_t>(d.tw) & 15) == 0) {
       a.tw_bytes = (unsigned)twb;
+      a.tw_res = 0;
+    }
   }
   if (grid > tp.ntiles) grid = tp.ntiles;
   k<<<(unsigned)grid, tp.L * tp.P, smem, st>>>(a);
@@ -988,6 +1028,16 @@ bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes,
   pp.smem = 2 * (size_t)pp.slot_elems * csz +
             (a.inplace ? 0 : (size_t)std::max(a.L * a.ld, b.L * b.ld) * csz) + 64;
   if (pp.smem > 220 * 1024) return false;
+  // both phases' twiddles resident when that costs no CTA per SM
+  {
+    const long long tw = (long long)pp.ph[0].tw_res + pp.ph[1].tw_res;
+    const int ctas = build_ctas_per_sm(a.variant, dbl);
+    if (tw > 0 && (size_t)ctas * (pp.smem + (size_t)tw * csz + 1024) <= 233472) {
+      pp.smem += (size_t)tw * csz;
+    } else {
+      pp.ph[0].tw_res = pp.ph[1].tw_res = 0;
+    }
+  }
   pp.planes = planes;
   const void* k = pair_kernel_ptr(dbl, inv, a.variant, a.inplace);
   if (kernel_smem_grant(k, pp.smem) != cudaSuccess) return false;
