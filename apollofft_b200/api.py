@@ -185,8 +185,7 @@ class _PlanBase:
         x = np.asarray(input)
         if x.shape != self.shape:
             raise ValueError(f"shape mismatch: expected {self.shape}, got {x.shape}")
-        return _real_forward(x, self._rank, "fft", self.profile if x.dtype != np.float64 else "high_accuracy"
-                             if self.profile == "high_accuracy" else self.profile)
+        return _real_forward(x, self._rank, "fft", self.profile)
 
     def ifft(self, input):
         X = np.asarray(input)

@@ -994,11 +994,13 @@ static const void* pair_kernel_ptr(bool dbl, bool inv, int variant, bool ip) {
 // planes in flight held to 56 MiB of L2.
 bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes, long long plane_bytes, bool dbl,
                    bool inv, TmaPairPlan& pp) {
-  static const int on = [] {
-    const char* e = getenv("AFC_PAIR");
-    return e && *e ? atoi(e) : 1;
-  }();
-  if (!on || planes < 1) return false;
+  // Opt-in (AFC_PAIR=1, read per plan execution): measured on B200 at
+  // 256^3 complex128 the pair launch keeps the intermediate in L2 (DRAM bytes
+  // halved) but takes 287 us against 2 x 95 us for the separate passes, whose
+  // tile transform is already as slow as their DRAM traffic (shared-memory
+  // and latency bound), so halving the traffic cannot pay yet.
+  const char* env = getenv("AFC_PAIR");
+  if (!(env && *env && atoi(env) != 0) || planes < 1) return false;
   for (int ph = 0; ph < 2; ++ph) {
     const LaunchDesc& d = ph ? d1 : d0;
     TmaPlan& tp = pp.ph[ph];

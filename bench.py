@@ -343,12 +343,24 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--shape", default=None, help="override the 3D shape, e.g. 128,256,256 (profiling cases)")
-    ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--precision", default=None, choices=["f64", "f32", "tc_bf16", "tc_fp16"])
+    ap.add_argument("--profile-case", default=None, choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="run one small case of a configuration --reps times and exit (for profiler captures)")
+    ap.add_argument("--reps", type=int, default=1, help="--profile-case: repetitions")
+    ap.add_argument("--rows", type=int, default=8192, help="--profile-case c4: rows of 4096")
+    ap.add_argument("--mode", type=int, default=2, help="--profile-case c3: batch mode")
+    ap.add_argument("--batch", type=int, default=2, help="--profile-case c5: images of 2048^2")
     ap.add_argument("--quick", action="store_true", help="headline only: no other configurations, e2e or CPU legs")
     ap.add_argument("--workload", default="c2",
                     choices=["c1", "c2", "c3", "c4", "c5", "calib", "stft", "czt", "nufft", "nufft3d", "hilbert"],
                     help="c2 (default) is the headline; the others print their own lines")
     args = ap.parse_args()
+    if args.profile_case:
+        return profile_case(args)
+    if args.precision is None:
+        args.precision = "f64"
+    if args.precision not in ("f64", "f32"):
+        ap.error("the headline runs f64 or f32")
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "calib":
@@ -508,6 +520,67 @@ def main():
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+    return 0
+
+
+def profile_case(a):
+    """One small single-GPU case of a measured configuration, run --reps times
+    on seeded device data (inputs larger than the 126 MB L2 where the workload
+    allows), for profiler captures, e.g.
+
+        ncu --set full --clock-control none -k regex:tc_fft_kernel -c 1 -o prof \
+            python bench.py --profile-case c4 --rows 8192 --precision tc_fp16
+
+    c1  64 x 4096 complex128 forward + inverse
+    c2  3D C2C forward + inverse of --shape (default 128,256,256) at --precision f64|f32
+    c3  the 4096-length uneven complex64 batch, --mode 0 (graph) | 1 (per length) | 2 (persistent)
+    c4  --rows x 4096 complex64 forward at --precision f32 | tc_bf16 | tc_fp16
+    c5  --batch x 2048 x 2048 real f32 R2C (full spectrum) forward + adjoint
+    """
+    import torch
+    import apollofft_b200 as afc
+    from apollofft_b200 import workloads as W
+
+    g = torch.Generator(device="cuda").manual_seed(7)
+    if a.profile_case == "c1":
+        x = torch.from_numpy(W.c1_input()).cuda()
+        p = afc.CudaPlan([4096], precision="f64", batch=64)
+        y = torch.empty_like(x)
+        for _ in range(a.reps):
+            p.execute(x, out=y)
+            p.execute(y, out=x, inverse=True)
+    elif a.profile_case == "c2":
+        prec = a.precision or "f64"
+        shape = [int(v) for v in (a.shape or "128,256,256").split(",")]
+        dt = torch.complex128 if prec == "f64" else torch.complex64
+        x = torch.randn(shape, dtype=dt, device="cuda", generator=g)
+        p = afc.CudaPlan(shape, precision=prec)
+        y = torch.empty_like(x)
+        for _ in range(a.reps):
+            p.execute(x, out=y)
+            p.execute(y, out=x, inverse=True)
+    elif a.profile_case == "c3":
+        lens = W.c3_lengths()
+        x = torch.from_numpy(W.c3_values(lens)).cuda()
+        bp = afc.BatchPlan(lens, precision="f32")
+        y = torch.empty_like(x)
+        for _ in range(a.reps):
+            bp.execute(x, out=y, mode=a.mode)
+    elif a.profile_case == "c4":
+        prec = a.precision or "f32"
+        x = torch.randn(a.rows, 4096, dtype=torch.complex64, device="cuda", generator=g)
+        p = afc.CudaPlan([4096], precision=prec, batch=a.rows)
+        y = torch.empty_like(x)
+        for _ in range(a.reps):
+            p.execute(x, out=y)
+    else:
+        from apollofft_b200 import autograd as AG
+        img = torch.randn(a.batch, 2048, 2048, dtype=torch.float32, device="cuda", generator=g, requires_grad=True)
+        for _ in range(a.reps):
+            X = AG.rfft2(img, half=False)
+            (X.abs() ** 2).sum().backward()
+    torch.cuda.synchronize()
+    print("ok")
     return 0
 
 

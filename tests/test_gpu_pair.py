@@ -1,6 +1,7 @@
-"""The plane-by-plane pass pair: the last two axes of a C2C plan run in one
-persistent launch whose second-axis tiles of an x-plane wait for that plane's
-first-axis tiles (per-plane counters), so the intermediate stays in L2.
+"""The plane-by-plane pass pair (opt-in, AFC_PAIR=1): the last two axes of a
+C2C plan run in one launch in which a thread-block cluster owns an x-plane,
+transforms its first-axis tiles, meets at the cluster barrier and transforms
+its second-axis tiles, so the intermediate stays in L2.
 
 Results must match the oracle's FftPlan2D/3D (crates/apollo-fft/src/
 application/execution/plan/fft/dimension_{2,3}d.rs: forward last axis first,
@@ -15,6 +16,12 @@ from conftest import rel_l2
 
 pytestmark = pytest.mark.gpu
 TOL = {"f64": 1e-12, "f32": 1e-5}
+
+
+@pytest.fixture(autouse=True)
+def pair_on(monkeypatch):
+    """The pass pair is opt-in (AFC_PAIR=1, read by the library per execution)."""
+    monkeypatch.setenv("AFC_PAIR", "1")
 
 
 def cplx(rng, shape):
@@ -73,3 +80,15 @@ def test_pair_repeated_calls_are_identical(afc, cuda):
         y = p.execute(x)
         assert torch.equal(y, first)
         p.execute(y, inverse=True)
+
+
+def test_default_runs_the_separate_passes(afc, cuda, monkeypatch):
+    monkeypatch.delenv("AFC_PAIR", raising=False)
+    x = torch.zeros((4, 256, 256), dtype=torch.complex128, device=cuda)
+    p = afc.CudaPlan([4, 256, 256], precision="f64")
+    p.execute(x)
+    torch.cuda.synchronize()
+    n0 = afc.kernel_launch_count()
+    p.execute(x)
+    torch.cuda.synchronize()
+    assert afc.kernel_launch_count() - n0 == 3
