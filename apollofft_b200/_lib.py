@@ -111,6 +111,9 @@ SIGNATURES = {
     "afc_nufft3d_type1": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),
     "afc_nufft3d_type2": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),
     "afc_nufft3d_plan_destroy": (_i32, [_vp]),
+    "afc_nudft1d_type1": (_i32, [_vp, _vp, _i64, _i64, _dbl, _vp, _i32, _vp]),
+    "afc_nudft1d_type2": (_i32, [_vp, _i64, _vp, _i64, _dbl, _vp, _i32, _vp]),
+    "afc_nudft3d_type1": (_i32, [_vp, _vp, _i64, _i64, _i64, _i64, _dbl, _dbl, _dbl, _vp, _i32, _vp]),
 }
 
 _lib = None

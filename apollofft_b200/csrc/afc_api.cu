@@ -2346,6 +2346,69 @@ afc_status afc_nufft1d_type2(afc_nufft_plan plan, const void* coeffs, const doub
   return AFC_OK;
 }
 
+// Domain checks of UniformDomain1D::new / UniformGrid3D::new
+// (apollo-nufft/src/domain/metadata/grid.rs:36-48,76-101).
+static afc_status check_domain(const char* nname, int64_t n, const char* dname, double d) {
+  if (n <= 0) return fail(AFC_ERR_VALIDATION, "validation failed for `%s`: `%lld` violates `must be > 0`", nname, (long long)n);
+  if (!std::isfinite(d) || d <= 0.0)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `%s`: `%g` violates `must be finite and > 0`", dname, d);
+  return AFC_OK;
+}
+
+static afc_status direct_device(int device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(AFC_ERR_BACKEND_UNAVAILABLE, "backend unavailable: cuda (no device)");
+  if (device < 0 || device >= ndev)
+    return fail(AFC_ERR_VALIDATION, "validation failed for `device`: `%d` violates `< %d`", device, ndev);
+  return AFC_OK;
+}
+
+afc_status afc_nudft1d_type1(const double* positions, const void* values, int64_t npts, int64_t n, double dx,
+                             void* out, int device, void* stream) {
+  afc_status s = check_domain("n", n, "dx", dx);
+  if (s != AFC_OK) return s;
+  if (npts < 0) return fail(AFC_ERR_VALIDATION, "validation failed for `npts`: `%lld` violates `>= 0`", (long long)npts);
+  if (!out || (npts > 0 && (!positions || !values)))
+    return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  if ((s = direct_device(device)) != AFC_OK) return s;
+  DeviceGuard g(device);
+  AFC_CUDA(nudft1_type1_dev(positions, values, npts, n, (double)n * dx, out, static_cast<cudaStream_t>(stream)),
+           "direct type-1 NUDFT");
+  return AFC_OK;
+}
+
+afc_status afc_nudft1d_type2(const void* coeffs, int64_t n, const double* positions, int64_t npts, double dx,
+                             void* out, int device, void* stream) {
+  afc_status s = check_domain("n", n, "dx", dx);
+  if (s != AFC_OK) return s;
+  if (npts < 0) return fail(AFC_ERR_VALIDATION, "validation failed for `npts`: `%lld` violates `>= 0`", (long long)npts);
+  if (!coeffs || (npts > 0 && (!positions || !out)))
+    return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  if ((s = direct_device(device)) != AFC_OK) return s;
+  DeviceGuard g(device);
+  AFC_CUDA(nudft1_type2_dev(coeffs, n, positions, npts, (double)n * dx, out, static_cast<cudaStream_t>(stream)),
+           "direct type-2 NUDFT");
+  return AFC_OK;
+}
+
+afc_status afc_nudft3d_type1(const double* positions, const void* values, int64_t npts, int64_t nx, int64_t ny,
+                             int64_t nz, double dx, double dy, double dz, void* out, int device, void* stream) {
+  afc_status s = AFC_OK;
+  if ((s = check_domain("nx", nx, "dx", dx)) != AFC_OK) return s;
+  if ((s = check_domain("ny", ny, "dy", dy)) != AFC_OK) return s;
+  if ((s = check_domain("nz", nz, "dz", dz)) != AFC_OK) return s;
+  if (npts < 0) return fail(AFC_ERR_VALIDATION, "validation failed for `npts`: `%lld` violates `>= 0`", (long long)npts);
+  if (!out || (npts > 0 && (!positions || !values)))
+    return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  if ((s = direct_device(device)) != AFC_OK) return s;
+  DeviceGuard g(device);
+  AFC_CUDA(nudft3_type1_dev(positions, values, npts, nx, ny, nz, (double)nx * dx, (double)ny * dy, (double)nz * dz, out,
+                            static_cast<cudaStream_t>(stream)),
+           "direct 3D type-1 NUDFT");
+  return AFC_OK;
+}
+
 afc_status afc_nufft_plan_destroy(afc_nufft_plan plan) {
   if (!plan) return AFC_OK;
   DeviceGuard g(plan->device);

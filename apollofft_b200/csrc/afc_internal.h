@@ -162,6 +162,13 @@ cudaError_t nufft3_modes_dev(const NuLaunch3& L, const double* dcx, const double
                              const void* src, void* dst, bool to_grid, cudaStream_t st);
 cudaError_t nufft_place_coeffs_dev(const void* coeffs, const double* deconv, long long n, long long m, void* grid,
                                    cudaStream_t st);
+// exact direct non-uniform DFTs (afc_nufft.cu), complex128
+cudaError_t nudft1_type1_dev(const double* pos, const void* val, long long npts, long long n, double len, void* out,
+                             cudaStream_t st);
+cudaError_t nudft1_type2_dev(const void* coeffs, long long n, const double* pos, long long npts, double len, void* out,
+                             cudaStream_t st);
+cudaError_t nudft3_type1_dev(const double* pos, const void* val, long long npts, long long nx, long long ny,
+                             long long nz, double lx, double ly, double lz, void* out, cudaStream_t st);
 cudaError_t launch_wait_probe(unsigned* err, int polls, cudaStream_t st);
 cudaError_t launch_tc_selftest(const float* A, const float* B, float* D, unsigned* err, bool fp16, cudaStream_t st);
 size_t tc_fft_smem(int n);

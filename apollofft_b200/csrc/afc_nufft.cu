@@ -660,4 +660,141 @@ cudaError_t nufft3_tiled_dev(const NuLaunch3& L, const NuTileLaunch& TL, bool sp
   return cudaGetLastError();
 }
 
+// ───────────────────── exact direct non-uniform DFTs ─────────────────────
+// apollo-nufft's exact direct sums (transform/dimension_1d.rs:428-472,
+// dimension_3d.rs:677-712): every output is the full sum over the inputs with
+// the phase (2 pi / L) k x, k the FFT-signed index (k <= n/2 stays, else
+// k - n; kaiser_bessel.rs:152-158), evaluated in FP64 like the reference.
+// One thread per output; the inputs stream through shared memory in chunks of
+// the block size, so each is read from global memory once per block.
+
+constexpr int kDirectThreads = 256;
+constexpr double kTwoPi = 6.283185307179586476925286766559;  // 2 pi
+
+__device__ __forceinline__ long long direct_signed(long long k, long long n) { return k <= n / 2 ? k : k - n; }
+
+// out[k] = sum_j v_j exp(-i (2 pi / L) k_s x_j), k < n
+__global__ void __launch_bounds__(kDirectThreads) nudft1_type1(const double* __restrict__ pos,
+                                                               const double2* __restrict__ val, long long npts,
+                                                               long long n, double two_pi_over_l, double2* out) {
+  __shared__ double sx[kDirectThreads];
+  __shared__ double2 sv[kDirectThreads];
+  const long long k = (long long)blockIdx.x * kDirectThreads + threadIdx.x;
+  const double ks = (double)direct_signed(k < n ? k : 0, n);
+  double re = 0.0, im = 0.0;
+  for (long long j0 = 0; j0 < npts; j0 += kDirectThreads) {
+    const long long j = j0 + threadIdx.x;
+    __syncthreads();
+    if (j < npts) {
+      sx[threadIdx.x] = pos[j];
+      sv[threadIdx.x] = val[j];
+    }
+    __syncthreads();
+    const int cnt = (int)(npts - j0 < kDirectThreads ? npts - j0 : kDirectThreads);
+    for (int i = 0; i < cnt; ++i) {
+      const double angle = -two_pi_over_l * ks * sx[i];
+      double sn, cs;
+      sincos(angle, &sn, &cs);
+      const double2 v = sv[i];
+      re += v.x * cs - v.y * sn;
+      im += v.x * sn + v.y * cs;
+    }
+  }
+  if (k < n) out[k] = make_double2(re, im);
+}
+
+// out[j] = sum_k c_k exp(+i (2 pi / L) k_s x_j), j < npts
+__global__ void __launch_bounds__(kDirectThreads) nudft1_type2(const double2* __restrict__ coeffs, long long n,
+                                                               const double* __restrict__ pos, long long npts,
+                                                               double two_pi_over_l, double2* out) {
+  __shared__ double2 sc[kDirectThreads];
+  const long long j = (long long)blockIdx.x * kDirectThreads + threadIdx.x;
+  const double x = j < npts ? pos[j] : 0.0;
+  double re = 0.0, im = 0.0;
+  for (long long k0 = 0; k0 < n; k0 += kDirectThreads) {
+    __syncthreads();
+    if (k0 + threadIdx.x < n) sc[threadIdx.x] = coeffs[k0 + threadIdx.x];
+    __syncthreads();
+    const int cnt = (int)(n - k0 < kDirectThreads ? n - k0 : kDirectThreads);
+    for (int i = 0; i < cnt; ++i) {
+      const double angle = two_pi_over_l * (double)direct_signed(k0 + i, n) * x;
+      double sn, cs;
+      sincos(angle, &sn, &cs);
+      const double2 c = sc[i];
+      re += c.x * cs - c.y * sn;
+      im += c.x * sn + c.y * cs;
+    }
+  }
+  if (j < npts) out[j] = make_double2(re, im);
+}
+
+// out[kx, ky, kz] = sum_j v_j exp(-i (wx kx_s x_j + wy ky_s y_j + wz kz_s z_j))
+__global__ void __launch_bounds__(kDirectThreads) nudft3_type1(const double* __restrict__ pos,
+                                                               const double2* __restrict__ val, long long npts,
+                                                               long long nx, long long ny, long long nz, double wx,
+                                                               double wy, double wz, double2* out) {
+  __shared__ double sp[3 * kDirectThreads];
+  __shared__ double2 sv[kDirectThreads];
+  const long long total = nx * ny * nz;
+  const long long m = (long long)blockIdx.x * kDirectThreads + threadIdx.x;
+  const long long mm = m < total ? m : 0;
+  const double kx = (double)direct_signed(mm / (ny * nz), nx);
+  const double ky = (double)direct_signed((mm / nz) % ny, ny);
+  const double kz = (double)direct_signed(mm % nz, nz);
+  double re = 0.0, im = 0.0;
+  for (long long j0 = 0; j0 < npts; j0 += kDirectThreads) {
+    const long long j = j0 + threadIdx.x;
+    __syncthreads();
+    if (j < npts) {
+      sp[3 * threadIdx.x] = pos[3 * j];
+      sp[3 * threadIdx.x + 1] = pos[3 * j + 1];
+      sp[3 * threadIdx.x + 2] = pos[3 * j + 2];
+      sv[threadIdx.x] = val[j];
+    }
+    __syncthreads();
+    const int cnt = (int)(npts - j0 < kDirectThreads ? npts - j0 : kDirectThreads);
+    for (int i = 0; i < cnt; ++i) {
+      const double angle = -(wx * kx * sp[3 * i] + wy * ky * sp[3 * i + 1] + wz * kz * sp[3 * i + 2]);
+      double sn, cs;
+      sincos(angle, &sn, &cs);
+      const double2 v = sv[i];
+      re += v.x * cs - v.y * sn;
+      im += v.x * sn + v.y * cs;
+    }
+  }
+  if (m < total) out[m] = make_double2(re, im);
+}
+
+cudaError_t nudft1_type1_dev(const double* pos, const void* val, long long npts, long long n, double len, void* out,
+                             cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const unsigned grid = (unsigned)((n + kDirectThreads - 1) / kDirectThreads);
+  nudft1_type1<<<grid, kDirectThreads, 0, st>>>(pos, static_cast<const double2*>(val), npts, n, kTwoPi / len,
+                                                static_cast<double2*>(out));
+  count_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t nudft1_type2_dev(const void* coeffs, long long n, const double* pos, long long npts, double len, void* out,
+                             cudaStream_t st) {
+  if (npts <= 0) return cudaSuccess;
+  const unsigned grid = (unsigned)((npts + kDirectThreads - 1) / kDirectThreads);
+  nudft1_type2<<<grid, kDirectThreads, 0, st>>>(static_cast<const double2*>(coeffs), n, pos, npts, kTwoPi / len,
+                                                static_cast<double2*>(out));
+  count_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t nudft3_type1_dev(const double* pos, const void* val, long long npts, long long nx, long long ny,
+                             long long nz, double lx, double ly, double lz, void* out, cudaStream_t st) {
+  const long long total = nx * ny * nz;
+  if (total <= 0) return cudaSuccess;
+  const unsigned grid = (unsigned)((total + kDirectThreads - 1) / kDirectThreads);
+  nudft3_type1<<<grid, kDirectThreads, 0, st>>>(pos, static_cast<const double2*>(val), npts, nx, ny, nz,
+                                                kTwoPi / lx, kTwoPi / ly, kTwoPi / lz,
+                                                static_cast<double2*>(out));
+  count_launch(1);
+  return cudaGetLastError();
+}
+
 }  // namespace afc

@@ -323,6 +323,29 @@ AFC_API afc_status afc_nufft3d_plan_destroy(afc_nufft3d_plan plan);
 AFC_API afc_status afc_execute_1d_no_alloc(afc_plan plan, const void* in, void* out, afc_direction direction,
                                            void* stream);
 
+/* ── exact direct non-uniform DFTs ─────────────────────────────────────────── */
+
+/* Replace apollo-nufft's exact direct sums behind apollo-python's
+ * nufft_type1_1d / nufft_type2_1d / nufft_type1_3d
+ * (crates/apollo-nufft/src/application/execution/transform/dimension_1d.rs:428-472,
+ * dimension_3d.rs:677-712; bindings crates/apollo-python/src/lib.rs:753-850):
+ * every output is the full O(inputs) sum, phase (2 pi / L) k x with k the
+ * FFT-signed index (k <= n/2 stays, else k - n) and L = n dx per axis, in
+ * FP64.  Device pointers: positions float64 (3D: npts x 3, row major), values,
+ * coefficients and outputs complex128.  Domain checks as UniformDomain1D::new /
+ * UniformGrid3D::new (n > 0, spacing finite and > 0).  Runs on `device`, on
+ * the caller's stream.
+ * type1: out[k] = sum_j v_j exp(-i 2 pi k x_j / L), k < n.
+ * type2: out[j] = sum_k c_k exp(+i 2 pi k x_j / L), j < npts.
+ * 3D type1: out[kx, ky, kz] (C order) = sum_j v_j exp(-i 2 pi (kx x_j / Lx + ky y_j / Ly + kz z_j / Lz)). */
+AFC_API afc_status afc_nudft1d_type1(const double* positions, const void* values, int64_t npts, int64_t n, double dx,
+                                     void* out, int device, void* stream);
+AFC_API afc_status afc_nudft1d_type2(const void* coeffs, int64_t n, const double* positions, int64_t npts, double dx,
+                                     void* out, int device, void* stream);
+AFC_API afc_status afc_nudft3d_type1(const double* positions, const void* values, int64_t npts, int64_t nx,
+                                     int64_t ny, int64_t nz, double dx, double dy, double dz, void* out, int device,
+                                     void* stream);
+
 #ifdef __cplusplus
 }
 #endif
