@@ -86,6 +86,8 @@ struct TmaPlan {
   bool real_in = false, real_out = false;
   // twiddle entries kept resident in shared memory by persistent CTAs (0: read from global)
   int tw_res = 0;
+  // tile slots of the load ring (2 or 3): slots - 1 tile loads in flight per CTA
+  int nslot = 2;
 };
 bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, const LaneMap& om, const void* in,
               void* out, bool dbl, int lanes_pref, TmaPlan& tp, bool real_in = false, bool real_out = false);

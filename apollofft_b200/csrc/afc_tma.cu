@@ -44,6 +44,7 @@ template <class T> struct TmaArgs {
   int nbx, bn;      // boxes along the transformed axis, rows per box
   unsigned tw_bytes;  // > 0: one tile per CTA, the twiddle table is copied into the idle second slot
   int tw_res;         // > 0: persistent CTAs keep the first tw_res twiddles resident in shared memory
+  int nslot;          // tile slots in the ring (2 or 3): nslot - 1 tile loads in flight
   long long tpp, lpp; // contiguous mode, tpp > 0: tiles never straddle planes of lpp lanes (tpp tiles per
                       // plane, the last one of a plane shorter); tpp = 0: tile q covers lanes [q L, q L + L)
   T scale;
@@ -407,11 +408,13 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
   using C = typename CT<T>::type;
   extern __shared__ __align__(128) unsigned char smraw[];
   const int L = a.L, P = a.P, ld = a.ld;
-  C* slots[2];
-  slots[0] = reinterpret_cast<C*>(smraw);
-  slots[1] = slots[0] + a.slot_elems;
-  C* work = IP ? nullptr : slots[1] + a.slot_elems;
-  C* twsm = IP ? slots[1] + a.slot_elems : work + (long long)L * ld;  // resident twiddles (a.tw_res)
+  // a ring of ns tile slots: while one tile is transformed, the loads of the
+  // next ns - 1 tiles are in flight
+  const int ns = a.nslot;
+  C* slots[3];
+  for (int k = 0; k < 3; ++k) slots[k] = reinterpret_cast<C*>(smraw) + (long long)k * a.slot_elems;
+  C* work = IP ? nullptr : slots[0] + (long long)ns * a.slot_elems;
+  C* twsm = IP ? slots[0] + (long long)ns * a.slot_elems : work + (long long)L * ld;  // resident twiddles (a.tw_res)
   C* end = twsm + a.tw_res;
   unsigned long long* bars =
       reinterpret_cast<unsigned long long*>(reinterpret_cast<uintptr_t>(end + 1) & ~(uintptr_t)7);
@@ -425,42 +428,45 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
     if (tid == 0) atomicExch(a.err, 1u);
     return;
   }
+  const long long G = gridDim.x;
   if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    for (int k = 0; k < ns; ++k) mbar_init(&bars[k], 1);
     fence_proxy_async();
-    // a CTA with a single tile never prefetches into the second slot: the
-    // twiddle table is staged there with the tile (stage twiddles then come
-    // from shared memory instead of L1 misses to L2)
+    // a CTA with a single tile never prefetches: the twiddle table is staged
+    // in the idle second slot with the tile (stage twiddles then come from
+    // shared memory instead of L1 misses to L2)
     tma_issue_load(a, tile, slots[0], &bars[0], a.tw_bytes ? slots[1] : nullptr);
+    for (int d = 1; d < ns - 1; ++d)
+      if (tile + d * G < a.ntiles) tma_issue_load(a, tile + d * G, slots[d], &bars[d]);
   }
   // a persistent CTA copies the table once into its own region
   for (int i = tid; i < a.tw_res; i += blockDim.x) twsm[i] = a.tw[i];
   __syncthreads();
   const C* twb = a.tw_res ? twsm : a.tw_bytes ? slots[1] : a.tw;
   for (int it = 0;; ++it) {
-    const int cb = it & 1;
-    const long long nxt = tile + gridDim.x;
+    const int cs = it % ns;
+    const long long pf = tile + (long long)(ns - 1) * G;  // the tile whose load is issued now
     if (tid == 0) {
-      bulk_wait_read0();  // the previous tile's store has finished reading its buffer
-      if (nxt < a.ntiles) tma_issue_load(a, nxt, slots[cb ^ 1], &bars[cb ^ 1]);
+      bulk_wait_read0();  // the previous tile's store has finished reading its buffer (slot (it - 1) % ns)
+      if (pf < a.ntiles) tma_issue_load(a, pf, slots[(it + ns - 1) % ns], &bars[(it + ns - 1) % ns]);
     }
-    const bool ok = mbar_wait(&bars[cb], (unsigned)((it >> 1) & 1));
+    const bool ok = mbar_wait(&bars[cs], (unsigned)((it / ns) & 1));
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         atomicExch(a.err, 1u);
-        // let the prefetch already in flight land before the CTA leaves (bounded)
-        if (nxt < a.ntiles) mbar_wait(&bars[cb ^ 1], (unsigned)(((it + 1) >> 1) & 1));
+        // let the loads already in flight land before the CTA leaves (bounded)
+        for (int d = 1; d < ns; ++d)
+          if (tile + d * G < a.ntiles) mbar_wait(&bars[(it + d) % ns], (unsigned)(((it + d) / ns) & 1));
         bulk_wait0();
       }
       return;
     }
-    C* cur = slots[cb];
+    C* cur = slots[cs];
     C* obuf = tma_stages<T, INV, V, IP>(a, cur, work, twb, l, t);
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) tma_issue_store(a, tile, obuf);
-    tile = nxt;
+    tile += G;
     if (tile >= a.ntiles) break;
   }
   if (tid == 0) bulk_wait0();
@@ -761,7 +767,8 @@ static bool make_map(CUtensorMap* m, const void* base, bool dbl, long long es, l
 static int g_tma_sm = 0;
 
 size_t tma_smem_bytes(const TmaPlan& tp, size_t csz) {
-  return 2 * (size_t)tp.slot_elems * csz + (tp.inplace ? 0 : (size_t)tp.L * tp.ld * csz) + (size_t)tp.tw_res * csz + 64;
+  return (size_t)tp.nslot * tp.slot_elems * csz + (tp.inplace ? 0 : (size_t)tp.L * tp.ld * csz) +
+         (size_t)tp.tw_res * csz + 64;
 }
 
 // Twiddle entries the stages read (r-major, twoff + (R - 1) Ns per stage).
@@ -894,6 +901,20 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
     tp.slot_elems = (int)se;
   }
   if (tma_smem_bytes(tp, csz) > 220 * 1024) return false;
+  // a third slot (two tile loads in flight per CTA) when it costs no CTA per
+  // SM: the passes whose CTAs hold few bytes in flight are bandwidth x latency
+  // bound with two
+  {
+    TmaPlan t3 = tp;
+    t3.nslot = 3;
+    const size_t b3 = tma_smem_bytes(t3, csz);
+    const int ctas = build_ctas_per_sm(tp.variant, dbl);
+    static const int slots_env = [] {
+      const char* e = getenv("AFC_TMA_SLOTS");
+      return e && *e ? atoi(e) : 3;
+    }();
+    if (slots_env >= 3 && (size_t)ctas * (b3 + 1024) <= 233472 && b3 <= 220 * 1024) tp.nslot = 3;
+  }
   plan_resident_twiddles(sl, dbl, tp);
   tp.ntiles = tp.mode == 0 ? (lanes + tp.L - 1) / tp.L : (lanes / im.es) * tp.kb;
   tp.outer = tp.mode == 1 ? lanes / im.es : 0;
@@ -930,6 +951,7 @@ template <class T> static bool fill_tma_args(const LaunchDesc& d, const TmaPlan&
   a.scale = (T)d.scale;
   a.err = err;
   a.tw_res = tp.tw_res;
+  a.nslot = tp.nslot;
   return true;
 }
 
