@@ -787,10 +787,14 @@ static int build_ctas_per_sm(int variant, bool dbl) {
 }
 
 // Keeps the twiddle table resident in shared memory when that costs no CTA
-// per SM (228 KB per SM, 1 KB reserved per CTA).
+// per SM (228 KB per SM, 1 KB reserved per CTA), for the odd-radix builds
+// only: measured on B200, 243 x 250 x 343 complex128 went from 1.32 to 1.25 ms
+// per forward + inverse, while the power-of-two passes, whose shared memory is
+// already the busiest unit, got slower (16384 x 4096 complex64: 333 -> 355 us).
 static void plan_resident_twiddles(const StageList& sl, bool dbl, TmaPlan& tp, size_t extra = 0) {
   const size_t csz = dbl ? 16 : 8;
   tp.tw_res = 0;
+  if (tp.variant != 0 && tp.variant != 3) return;
   const long long twc = twiddle_count(sl);
   if (twc <= 0) return;
   const size_t base = tma_smem_bytes(tp, csz) + extra;
@@ -909,9 +913,12 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
     t3.nslot = 3;
     const size_t b3 = tma_smem_bytes(t3, csz);
     const int ctas = build_ctas_per_sm(tp.variant, dbl);
+    // measured on B200: no pass got faster with the third slot (16384 x 4096
+    // complex64 went from 355 to 386 us, its smem displacing the resident
+    // twiddles), so two slots stay the default; AFC_TMA_SLOTS=3 opts in
     static const int slots_env = [] {
       const char* e = getenv("AFC_TMA_SLOTS");
-      return e && *e ? atoi(e) : 3;
+      return e && *e ? atoi(e) : 2;
     }();
     if (slots_env >= 3 && (size_t)ctas * (b3 + 1024) <= 233472 && b3 <= 220 * 1024) tp.nslot = 3;
   }
