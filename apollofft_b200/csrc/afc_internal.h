@@ -88,9 +88,6 @@ struct TmaPlan {
   int tw_res = 0;
   // tile slots of the load ring (2 or 3): slots - 1 tile loads in flight per CTA
   int nslot = 2;
-  // in-place builds: the last stage stores each thread's outputs straight to
-  // global memory (coalesced in both lane layouts) instead of a TMA store
-  bool direct = false;
 };
 bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, const LaneMap& om, const void* in,
               void* out, bool dbl, int lanes_pref, TmaPlan& tp, bool real_in = false, bool real_out = false);

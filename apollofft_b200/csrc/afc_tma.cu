@@ -45,8 +45,6 @@ template <class T> struct TmaArgs {
   unsigned tw_bytes;  // > 0: one tile per CTA, the twiddle table is copied into the idle second slot
   int tw_res;         // > 0: persistent CTAs keep the first tw_res twiddles resident in shared memory
   int nslot;          // tile slots in the ring (2 or 3): nslot - 1 tile loads in flight
-  int direct;         // in-place builds: the last stage stores straight to global memory (no TMA store)
-  long long es;       // strided mode: element stride of a lane (lanes per outer index)
   long long tpp, lpp; // contiguous mode, tpp > 0: tiles never straddle planes of lpp lanes (tpp tiles per
                       // plane, the last one of a plane shorter); tpp = 0: tile q covers lanes [q L, q L + L)
   T scale;
@@ -182,14 +180,10 @@ __device__ __forceinline__ void tma_stage(TView<C> src, TView<C> dst, int l, int
 // the barrier.  rsrc / rdst (contiguous lanes only): when set, the stage reads
 // real input lanes (widened to complex) from rsrc, or writes the real parts of
 // its output to rdst, both with lane stride n.
-// gdst / grdst (last stage only): the stage stores its outputs straight to
-// global memory, element i of this thread's lane at gdst[i * ges] (complex) or
-// grdst[i * ges] (real parts), instead of into the shared tile.
 template <int R, bool INV, int NB2, class C, class S>
 __device__ __forceinline__ void tma_stage_inplace(TView<C> src, TView<C> dst, int l, int n, int Ns,
                                                   const C* __restrict__ tw, int t, int P, bool scale_out, S sc,
-                                                  const S* rsrc = nullptr, S* rdst = nullptr, C* gdst = nullptr,
-                                                  S* grdst = nullptr, int ges = 1) {
+                                                  const S* rsrc = nullptr, S* rdst = nullptr) {
   constexpr int NB = (R <= 8 && NB2) ? 2 : 1;
   const int nb = n / R;
   C v[NB][R];
@@ -228,13 +222,7 @@ __device__ __forceinline__ void tma_stage_inplace(TView<C> src, TView<C> dst, in
       const int o = (j - k) * R + k;
       C* q;
       int qs;
-      if (gdst) {
-#pragma unroll
-        for (int r = 0; r < R; ++r) gdst[(long long)(o + r * Ns) * ges] = scale_out ? cscale(v[b][r], sc) : v[b][r];
-      } else if (grdst) {
-#pragma unroll
-        for (int r = 0; r < R; ++r) grdst[(long long)(o + r * Ns) * ges] = scale_out ? v[b][r].x * sc : v[b][r].x;
-      } else if (rdst) {
+      if (rdst) {
 #pragma unroll
         for (int r = 0; r < R; ++r) rdst[(long long)l * n + o + r * Ns] = scale_out ? v[b][r].x * sc : v[b][r].x;
       } else if (sizeof(S) == 4 && dst.run(l, o, Ns, R, q, qs)) {
@@ -272,26 +260,6 @@ __device__ __forceinline__ void tma_issue_load(const TmaArgs<T>& a, long long ti
   if (extra) bulk_load(tw_dst, a.tw, extra, bar);
 }
 
-// The global destination of this thread's lane of `tile` for a direct last
-// stage: element 0 of the lane and the element stride.  Lanes beyond the data
-// (a partial last tile) get none and leave their result in the shared tile.
-template <class T>
-__device__ __forceinline__ void* lane_out(const TmaArgs<T>& a, long long tile, int l, int& ges) {
-  ges = 1;
-  if (a.mode == 0) {
-    long long q0;
-    int nl;
-    tile_lanes(a, tile, q0, nl);
-    if (l >= nl) return nullptr;
-    if (a.real_out) return reinterpret_cast<T*>(a.out) + (q0 + l) * a.sl.n;
-    return a.out + (q0 + l) * a.sl.n;
-  }
-  const long long o = tile / a.kb, col = (tile % a.kb) * a.L + l;
-  if (col >= a.es) return nullptr;
-  ges = (int)a.es;
-  return a.out + o * a.sl.n * a.es + col;
-}
-
 template <class T>
 __device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long tile, const typename CT<T>::type* buf) {
   using C = typename CT<T>::type;
@@ -319,8 +287,7 @@ __device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long t
 template <class T, bool INV, int V, bool IP>
 __device__ __forceinline__ typename CT<T>::type* tma_stages(const TmaArgs<T>& a, typename CT<T>::type* cur,
                                                             typename CT<T>::type* work,
-                                                            const typename CT<T>::type* twb, int l, int t,
-                                                            void* gout = nullptr, int ges = 1) {
+                                                            const typename CT<T>::type* twb, int l, int t) {
   constexpr bool P2 = V == 1 || V == 2 || V == 4;
   constexpr bool S7 = V == 3;
   using C = typename CT<T>::type;
@@ -341,10 +308,7 @@ __device__ __forceinline__ typename CT<T>::type* tma_stages(const TmaArgs<T>& a,
     const C* twi = twb + sd.twoff;
     const T* rsrc = (s == 0 && a.real_in) ? reinterpret_cast<const T*>(cur) : nullptr;
     T* rdst = (last && a.real_out) ? reinterpret_cast<T*>(cur) : nullptr;
-#define AFC_TI(R)                                                                                        \
-  tma_stage_inplace<R, INV, (V == 4 ? 1 : 0)>(                                                          \
-      src, dst, l, n, sd.Ns, twi, t, P, last, a.scale, rsrc, rdst,                                     \
-      (last && !a.real_out) ? static_cast<C*>(gout) : nullptr, (last && a.real_out) ? static_cast<T*>(gout) : nullptr, ges)
+#define AFC_TI(R) tma_stage_inplace<R, INV, (V == 4 ? 1 : 0)>(src, dst, l, n, sd.Ns, twi, t, P, last, a.scale, rsrc, rdst)
     if constexpr (P2) {
       switch (sd.R) {
         case 2: AFC_TI(2); break;
@@ -498,15 +462,10 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
       return;
     }
     C* cur = slots[cs];
-    int ges = 1;
-    const bool direct = IP && a.direct;
-    void* gout = direct ? lane_out(a, tile, l, ges) : nullptr;
-    C* obuf = tma_stages<T, INV, V, IP>(a, cur, work, twb, l, t, gout, ges);
-    if (!direct) {
-      fence_proxy_async();
-      __syncthreads();
-      if (tid == 0) tma_issue_store(a, tile, obuf);
-    }
+    C* obuf = tma_stages<T, INV, V, IP>(a, cur, work, twb, l, t);
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) tma_issue_store(a, tile, obuf);
     tile += G;
     if (tile >= a.ntiles) break;
   }
@@ -618,8 +577,7 @@ __device__ __forceinline__ void pair_advance(const PairGeo& g, int& q, int& pos)
 template <class T, bool INV, int V, bool IP>
 __device__ __forceinline__ typename CT<T>::type* pair_transform(const TmaArgs<T>& a, typename CT<T>::type* slot,
                                                                 typename CT<T>::type* work,
-                                                                const typename CT<T>::type* tw, int tid,
-                                                                long long tile) {
+                                                                const typename CT<T>::type* tw, int tid) {
   const bool lm = a.mode == 1;
   const int L = a.L, P = a.P;
   // a phase with fewer threads than the CTA leaves the rest idle (no
@@ -627,11 +585,7 @@ __device__ __forceinline__ typename CT<T>::type* pair_transform(const TmaArgs<T>
   const bool act = tid < L * P;
   const int l = !act ? 0 : lm ? tid % L : tid / P;
   const int t = !act ? (1 << 20) : lm ? tid / L : tid % P;
-  int ges = 1;
-  const bool direct = IP && a.direct;
-  void* gout = (direct && act) ? lane_out(a, tile, l, ges) : nullptr;
-  typename CT<T>::type* obuf = tma_stages<T, INV, V, IP>(a, slot, work, tw, l, t, gout, ges);
-  return direct ? nullptr : obuf;  // nullptr: stored straight to global memory
+  return tma_stages<T, INV, V, IP>(a, slot, work, tw, l, t);
 }
 
 template <class T, bool INV, int V, bool IP>
@@ -688,9 +642,6 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
     if (ctl->pos < 0) {
       // the barrier between a plane's phases: this CTA's phase-0 stores are
       // complete and visible before any CTA of the cluster loads phase-1 tiles
-      // (direct stores: every thread orders its global writes before the
-      // tensor loads of the other CTAs)
-      fence_proxy_async_global();
       cluster_sync_all();
       if (tid == 0) {
         const PairGeo g = pair_geo(pa);
@@ -745,15 +696,16 @@ __global__ void __launch_bounds__(V == 2 ? 128 : 256,
       }
     }
     if (!bad && !timed_out) {
-      int tph;
-      const long long tile = pair_tile(pa, pair_geo(pa), ctl->q, ctl->pos, tph);
-      ph = tph;
+      ph = ctl->pos < pair_geo(pa).a0 ? 0 : 1;
       C* obuf = pair_transform<T, INV, V, IP>(pa.ph[ph], cur, work, pa.ph[ph].tw_res ? (ph ? tw1 : tw0) : pa.ph[ph].tw,
-                                              tid, tile);
-      if (obuf) {  // the tile left its result in shared memory: one TMA store
-        fence_proxy_async();
-        __syncthreads();
-        if (tid == 0) tma_issue_store(pa.ph[ph], tile, obuf);
+                                              tid);
+      fence_proxy_async();
+      __syncthreads();
+      if (tid == 0) {
+        const PairGeo g = pair_geo(pa);
+        int tph;
+        const long long tile = pair_tile(pa, g, ctl->q, ctl->pos, tph);
+        tma_issue_store(pa.ph[tph], tile, obuf);
       }
     }
     if (tid == 0) {
@@ -933,10 +885,6 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
   // in place only for power-of-two plans: odd-radix butterflies held across
   // the barrier cost spills
   tp.inplace = fits_inplace(P, false);
-  static const int direct_env = [] {
-    const char* e = getenv("AFC_TMA_DIRECT");
-    return e && *e ? atoi(e) : 1;
-  }();
   if (!tp.inplace && !dbl && fits_inplace(P, true)) {
     tp.inplace = true;
     tp.variant = 4;
@@ -944,7 +892,6 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
   if (real && !tp.inplace) return false;
   tp.real_in = real_in;
   tp.real_out = real_out;
-  tp.direct = tp.inplace && direct_env != 0;
   const int align = dbl ? 8 : 16;  // 128-byte aligned slots
   long long rows = tp.mode == 1 ? (long long)tp.nbx * tp.bn : n;
   long long se = (long long)tp.L * std::max<long long>(ld, rows);
@@ -1012,8 +959,6 @@ template <class T> static bool fill_tma_args(const LaunchDesc& d, const TmaPlan&
   a.err = err;
   a.tw_res = tp.tw_res;
   a.nslot = tp.nslot;
-  a.direct = tp.direct ? 1 : 0;
-  a.es = d.im.es;
   return true;
 }
 
