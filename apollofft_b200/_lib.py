@@ -97,6 +97,7 @@ SIGNATURES = {
     "afc_stft_inverse": (_i32, [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _sz, _vp]),
     "afc_czt_plan_create": (_i32, [ctypes.POINTER(_vp), _i64, _i64, _dbl, _dbl, _dbl, _dbl, _i32, _i32]),
     "afc_czt_execute": (_i32, [_vp, _vp, _vp, _i64, _vp]),
+    "afc_czt_inverse": (_i32, [_vp, _vp, _vp, _i64, _vp]),
     "afc_czt_conv_len": (_i32, [_vp, _pi64]),
     "afc_czt_plan_destroy": (_i32, [_vp]),
     "afc_hilbert_plan_create": (_i32, [ctypes.POINTER(_vp), _i64, _i32, _i32]),

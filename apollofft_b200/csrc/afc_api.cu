@@ -12,6 +12,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <functional>
+#include <limits>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -1107,12 +1108,18 @@ struct afc_czt_plan_s {
   int64_t n = 0, m = 0, L = 0;
   bool dbl = true;
   int device = 0;
-  afc::LenPlan lp;                 // the length-L convolution in one CTA
+  afc::LenPlan lp;                 // the length-L convolution in one CTA (when it fits)
+  std::unique_ptr<afc::AxisPlan> big;  // else the multi-pass plan of length L
   void* chirp_n = nullptr;         // A^-j W^(j^2/2), j < n
   void* chirp_k = nullptr;         // W^(k^2/2), k < m
   void* spec = nullptr;            // FFT of the chirp kernel, scaled by 1/L
+  // square plans: the inverse's Vandermonde nodes W^k and A^k (complex128),
+  // and whether the nodes are distinct enough to invert
+  void* nodes = nullptr;
+  void* apow = nullptr;
+  bool invertible = false;
   ~afc_czt_plan_s() {
-    void* ptrs[] = {lp.tw, chirp_n, chirp_k, spec};
+    void* ptrs[] = {lp.tw, chirp_n, chirp_k, spec, nodes, apow};
     for (void* p : ptrs)
       if (p) cudaFree(p);
   }
@@ -1963,10 +1970,27 @@ afc_status afc_stft_forward(afc_plan plan, const void* signal, int64_t signal_le
     return fail(AFC_ERR_SHAPE_MISMATCH, "shape mismatch: expected %lld output elements (%lld frames x %lld), got %lld",
                 (long long)(frames * n), (long long)frames, (long long)n, (long long)out_elems);
   const AxisPlan& ap = *plan->axes[0];
-  if (ap.algo != ALGO_SMEM)
-    return fail(AFC_ERR_UNSUPPORTED, "fused STFT frames need a single-CTA frame length (got %lld)", (long long)n);
   const size_t csz = plan->dbl ? 16 : 8;
   DeviceGuard g(plan->device);
+  if (ap.algo != ALGO_SMEM) {
+    // frames beyond one CTA: gather the windowed frames into the output, then
+    // the multi-pass plan in place (its workspace stream-ordered)
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    AFC_CUDA(stft_gather_dev(signal, window, signal_len, n, hop, frames, out, plan->dbl, st), "stft frames");
+    AxisIO io;
+    io.in = out;
+    io.out = out;
+    io.lanes = frames;
+    io.im = io.om = LaneMap{1, 1, n, 0, 0, 1, nullptr};
+    const size_t ab = axis_ws_bytes(ap, frames, csz);
+    void* w = nullptr;
+    if (ab) AFC_CUDA(cudaMallocAsync(&w, ab, st), "stft workspace");
+    cudaError_t e = exec_axis(ap, plan->dbl, false, io, w, st);
+    cudaError_t ef = w ? cudaFreeAsync(w, st) : cudaSuccess;
+    if (e != cudaSuccess) return cuda_fail(e, "stft forward");
+    AFC_CUDA(ef, "stft workspace");
+    return AFC_OK;
+  }
   LaunchDesc d;
   fill_common(d, ap.lp);
   d.lanes = frames;
@@ -2020,10 +2044,12 @@ afc_status afc_stft_inverse(afc_plan plan, const void* spectrum, int64_t spectru
     return fail(AFC_ERR_VALIDATION, "validation failed for `workspace_bytes`: `%zu` violates `>= %zu`", workspace_bytes,
                 (size_t)frames * (size_t)n * rsz);
   const AxisPlan& ap = *plan->axes[0];
-  if (ap.algo != ALGO_SMEM)
-    return fail(AFC_ERR_UNSUPPORTED, "inverse STFT frames need a single-CTA frame length (got %lld)", (long long)n);
   DeviceGuard g(plan->device);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // frames beyond one CTA run the multi-pass plan, its workspace stream-ordered
+  const size_t ab = axis_ws_bytes(ap, frames, plan->dbl ? 16 : 8);
+  void* w = nullptr;
+  if (ab) AFC_CUDA(cudaMallocAsync(&w, ab, st), "stft workspace");
   // 1. every frame: normalized inverse FFT, real part, into the workspace
   AxisIO io;
   io.in = spectrum;
@@ -2034,12 +2060,19 @@ afc_status afc_stft_inverse(afc_plan plan, const void* spectrum, int64_t spectru
   io.in_op = IN_C;
   io.out_op = OUT_RE;
   io.scale = 1.0 / (double)n;
-  cudaError_t e = exec_axis(ap, plan->dbl, true, io, nullptr, st);
+  cudaError_t e = exec_axis(ap, plan->dbl, true, io, w, st);
+  cudaError_t ef = w ? cudaFreeAsync(w, st) : cudaSuccess;
   if (e != cudaSuccess) return cuda_fail(e, "stft inverse frames");
+  AFC_CUDA(ef, "stft workspace");
   // 2. windowed overlap-add, normalized by the summed squared window
   e = stft_ola_dev(workspace, window, frames, n, hop, signal_len, out, plan->dbl, st);
   if (e != cudaSuccess) return cuda_fail(e, "stft overlap-add");
   return AFC_OK;
+}
+
+// num-complex's product (a.re b.re - a.im b.im, a.re b.im + a.im b.re)
+static std::complex<double> cmul_ref(std::complex<double> a, std::complex<double> b) {
+  return {a.real() * b.real() - a.imag() * b.imag(), a.real() * b.imag() + a.imag() * b.real()};
 }
 
 // num-complex powf (polar form): |z|^e exp(i arg(z) e), as the reference's
@@ -2069,8 +2102,6 @@ afc_status afc_czt_plan_create(afc_czt_plan* out, int64_t n, int64_t m, double a
   const size_t csz = dbl ? 16 : 8;
   int64_t L = 1;
   while (L < n + m - 1) L <<= 1;
-  if (!plannable(L, csz))
-    return fail(AFC_ERR_UNSUPPORTED, "CZT convolution length %lld exceeds one CTA (n + m - 1 too large)", (long long)L);
   DeviceGuard g(device);
   std::unique_ptr<afc_czt_plan_s> p(new afc_czt_plan_s());
   p->n = n;
@@ -2098,16 +2129,50 @@ afc_status afc_czt_plan_create(afc_czt_plan* out, int64_t n, int64_t m, double a
   AFC_CUDA(upload(cn, &p->chirp_n), "CZT chirp");
   AFC_CUDA(upload(ck, &p->chirp_k), "CZT chirp");
   AFC_CUDA(upload(ker, &p->spec), "CZT kernel");
+  // square plans: the inverse's nodes z_k = W^k and A^k by the reference's
+  // recurrences (czt_inverse_nodes, kernel/bluestein.rs:167-175; the A^n
+  // scaling of czt_bjork_pereyra_inverse_into, :215-220), and its collision
+  // test |z_k - z_(k-j-1)| < 1024 eps over every pair the solve divides by
+  if (n == m && (size_t)n * 32 <= kSmemMax) {
+    std::vector<std::complex<double>> z(n), ap(n);
+    std::complex<double> wk(1.0, 0.0), ak(1.0, 0.0);
+    for (int64_t k = 0; k < n; ++k) {
+      z[k] = wk;
+      ap[k] = ak;
+      wk = cmul_ref(wk, W);
+      ak = cmul_ref(ak, A);
+    }
+    bool ok = true;
+    for (int64_t d = 1; d < n && ok; ++d)
+      for (int64_t k = d; k < n; ++k)
+        if (std::hypot(z[k].real() - z[k - d].real(), z[k].imag() - z[k - d].imag()) <
+            std::numeric_limits<double>::epsilon() * 1024.0) {
+          ok = false;
+          break;
+        }
+    p->invertible = ok;
+    AFC_CUDA(dev_alloc(&p->nodes, (size_t)n * 16), "CZT nodes");
+    AFC_CUDA(cudaMemcpy(p->nodes, z.data(), (size_t)n * 16, cudaMemcpyHostToDevice), "CZT nodes");
+    AFC_CUDA(dev_alloc(&p->apow, (size_t)n * 16), "CZT nodes");
+    AFC_CUDA(cudaMemcpy(p->apow, ap.data(), (size_t)n * 16, cudaMemcpyHostToDevice), "CZT nodes");
+  }
   cudaStream_t st;
   AFC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
-  afc_status s = build_lenplan(L, dbl, p->lp, st);
-  if (s == AFC_OK) {
-    AxisPlan mp;
-    mp.n = L;
-    mp.algo = ALGO_SMEM;
-    mp.lp = p->lp;
-    s = fft_table(mp, dbl, p->spec, st);
-    mp.lp.tw = nullptr;  // owned by the CZT plan
+  afc_status s = AFC_OK;
+  if (plannable(L, csz)) {  // one convolution tile per lane
+    s = build_lenplan(L, dbl, p->lp, st);
+    if (s == AFC_OK) {
+      AxisPlan mp;
+      mp.n = L;
+      mp.algo = ALGO_SMEM;
+      mp.lp = p->lp;
+      s = fft_table(mp, dbl, p->spec, st);
+      mp.lp.tw = nullptr;  // owned by the CZT plan
+    }
+  } else {  // the convolution through the library's multi-pass plan of length L
+    p->big.reset(new AxisPlan());
+    s = build_axis(L, dbl, *p->big, st);
+    if (s == AFC_OK) s = fft_table(*p->big, dbl, p->spec, st);
   }
   cudaStreamSynchronize(st);
   cudaStreamDestroy(st);
@@ -2122,6 +2187,34 @@ afc_status afc_czt_execute(afc_czt_plan plan, const void* in, void* out, int64_t
   if (batch < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `batch`: `%lld` violates `> 0`", (long long)batch);
   const size_t csz = plan->dbl ? 16 : 8;
   DeviceGuard g(plan->device);
+  if (plan->big) {
+    // premultiply into a zero-padded workspace, forward FFT of length L,
+    // product with the kernel spectrum (scaled 1/L), unnormalized inverse,
+    // postmultiply of the first m bins (kernel/bluestein.rs:83-130); the
+    // workspace is stream-ordered, so the call allocates nothing the host waits for
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t L = plan->L;
+    const size_t wb = ((size_t)batch * L * csz + 255) / 256 * 256;
+    const size_t ab = axis_ws_bytes(*plan->big, batch, csz);
+    void* w = nullptr;
+    AFC_CUDA(cudaMallocAsync(&w, wb + ab, st), "CZT workspace");
+    AxisIO io;
+    io.in = w;
+    io.out = w;
+    io.lanes = batch;
+    io.im = io.om = LaneMap{1, 1, L, 0, 0, 1, nullptr};
+    io.scale = 1.0;
+    void* aws = static_cast<char*>(w) + wb;
+    cudaError_t e = chirp_rows_dev(in, plan->n, plan->n, plan->chirp_n, w, L, L, batch, plan->dbl, st);
+    if (e == cudaSuccess) e = exec_axis(*plan->big, plan->dbl, false, io, aws, st);
+    if (e == cudaSuccess) e = chirp_rows_dev(w, L, L, plan->spec, w, L, L, batch, plan->dbl, st);
+    if (e == cudaSuccess) e = exec_axis(*plan->big, plan->dbl, true, io, aws, st);
+    if (e == cudaSuccess) e = chirp_rows_dev(w, L, plan->m, plan->chirp_k, out, plan->m, plan->m, batch, plan->dbl, st);
+    cudaError_t ef = cudaFreeAsync(w, st);
+    if (e != cudaSuccess) return cuda_fail(e, "czt execute");
+    AFC_CUDA(ef, "CZT workspace");
+    return AFC_OK;
+  }
   LaunchDesc d;
   fill_common(d, plan->lp);
   d.lanes = batch;
@@ -2228,6 +2321,25 @@ afc_status afc_hilbert_plan_destroy(afc_hilbert_plan plan) {
   if (!plan) return AFC_OK;
   DeviceGuard g(plan->device);
   delete plan;
+  return AFC_OK;
+}
+
+afc_status afc_czt_inverse(afc_czt_plan plan, const void* spectrum, void* out, int64_t batch, void* stream) {
+  if (!plan) return fail(AFC_ERR_VALIDATION, "validation failed for `plan`: `null` violates `must be non-null`");
+  if (!spectrum || !out) return fail(AFC_ERR_VALIDATION, "validation failed for `buffer`: `null` violates `must be non-null`");
+  if (batch < 1) return fail(AFC_ERR_VALIDATION, "validation failed for `batch`: `%lld` violates `> 0`", (long long)batch);
+  // the reference's errors (plan/czt/dimension_1d.rs:250-293, kernel/bluestein.rs:193-205)
+  if (plan->n != plan->m)
+    return fail(AFC_ERR_VALIDATION, "not invertible: inverse is only defined for square (M == N) CZT plans");
+  if (!plan->nodes)
+    return fail(AFC_ERR_UNSUPPORTED, "the device inverse CZT holds the length in shared memory: n <= %zu (got %lld)",
+                kSmemMax / 32, (long long)plan->n);
+  if (!plan->invertible)
+    return fail(AFC_ERR_VALIDATION, "not invertible: Vandermonde nodes z_k collide; W is a root of unity of order <= N");
+  DeviceGuard g(plan->device);
+  AFC_CUDA(czt_inverse_dev(spectrum, out, plan->nodes, plan->apow, plan->n, batch, plan->dbl,
+                           static_cast<cudaStream_t>(stream)),
+           "czt inverse");
   return AFC_OK;
 }
 

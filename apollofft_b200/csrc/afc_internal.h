@@ -1,6 +1,7 @@
 // afc_internal.h -- host <-> kernel interface inside libapollofft_cuda.so.
 #pragma once
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstddef>
 #include "afc_engine.cuh"
 
@@ -192,6 +193,14 @@ int batch_blocks_per_sm(size_t smem, bool dbl, bool inv);
 cudaError_t launch_tile(const LaunchDesc& d, bool dbl, bool inv, cudaStream_t st);
 cudaError_t launch_conv(const LaunchDesc& d, bool dbl, cudaStream_t st);
 
+// caller kernels of multi-pass transforms (afc_callers.cu)
+cudaError_t stft_gather_dev(const void* sig, const void* win, long long nsig, long long flen, long long hop,
+                            long long frames, void* out, bool dbl, cudaStream_t st);
+cudaError_t chirp_rows_dev(const void* src, long long ss, long long valid, const void* table, void* dst, long long ds,
+                           long long nout, long long batch, bool dbl, cudaStream_t st);
+size_t czt_inverse_smem(long long n);
+cudaError_t czt_inverse_dev(const void* spec, void* out, const void* nodes, const void* apow, long long n,
+                            long long batch, bool dbl, cudaStream_t st);
 cudaError_t stft_ola_dev(const void* frames, const void* window, long long nframes, long long flen, long long hop,
                          long long nsig, void* out, bool dbl, cudaStream_t st);
 cudaError_t gen_row_spectrum_dev(void* dst, const void* src, long long N1, long long N2, bool dbl, cudaStream_t st);

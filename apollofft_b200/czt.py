@@ -4,7 +4,10 @@
 (crates/apollo-czt/src/application/execution/plan/czt/dimension_1d.rs:60-120):
 X_k = sum_j x_j a^-j w^(j k) for k < m, evaluated with Bluestein's identity over
 a convolution of length next_pow2(n + m - 1).  The premultiply, both FFTs, the
-kernel product and the postmultiply run in one kernel launch on device data.
+kernel product and the postmultiply run in one kernel launch on device data
+when the convolution fits one CTA, else around the multi-pass plan.
+`inverse(X)` is the reference's exact inverse of a square plan (CztPlan::inverse:
+Björck-Pereyra solve on the nodes W^k), one CTA per lane in FP64.
 """
 from __future__ import annotations
 
@@ -65,6 +68,27 @@ class CztPlan:
         require_device(out, self.device, "output")
         st = stream if stream is not None else torch.cuda.current_stream(x.device).cuda_stream
         L.check(L.lib().afc_czt_execute(self._h, x.data_ptr(), out.data_ptr(), batch, st), "czt execute")
+        return out
+
+    def inverse(self, X, out=None, stream=None):
+        """X: complex torch tensor on the device with last dimension n (= m);
+        returns the signal whose forward transform is X."""
+        import torch
+        cdt = torch.complex128 if self.precision == "f64" else torch.complex64
+        if X.dtype != cdt or not X.is_contiguous() or X.shape[-1] != self.m or not X.is_cuda:
+            raise ValueError(f"expected a contiguous {cdt} tensor with last dimension {self.m}")
+        require_device(X, self.device, "spectrum")
+        batch = X.numel() // self.m
+        if out is None:
+            out = torch.empty(tuple(X.shape[:-1]) + (self.n,), dtype=cdt, device=X.device)
+        if out.dtype != cdt or not out.is_contiguous() or out.numel() != batch * self.n or not out.is_cuda:
+            raise ValueError("output buffer does not match the plan")
+        require_device(out, self.device, "output")
+        st = stream if stream is not None else torch.cuda.current_stream(X.device).cuda_stream
+        status = L.lib().afc_czt_inverse(self._h, X.data_ptr(), out.data_ptr(), batch, st)
+        if status == L.AFC_ERR_VALIDATION:
+            raise CztError(L.last_error())
+        L.check(status, "czt inverse")
         return out
 
     def close(self):

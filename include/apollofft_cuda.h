@@ -235,15 +235,26 @@ AFC_API afc_status afc_stft_inverse(afc_plan plan, const void* spectrum, int64_t
  * kernel/bluestein.rs:83-130), which run the premultiply, the two
  * FftPlan1D slice transforms and the postmultiply on host buffers; same chirp
  * tables (num-complex powf, polar form) and the same convolution length
- * L = next_pow2(n + m - 1), which must fit one CTA (AFC_ERR_UNSUPPORTED
- * otherwise).  n, m > 0 and finite non-zero A, W (CztError::EmptyLength /
- * InvalidParameters -> AFC_ERR_VALIDATION).  Execute: `batch` contiguous lanes
- * of n complex inputs -> `batch` lanes of m complex outputs (F32: complex64,
- * F64: complex128), device pointers, on `stream`. */
+ * L = next_pow2(n + m - 1).  When L does not fit one CTA the same steps run
+ * around the library's multi-pass plan of length L (five launches, workspace
+ * stream-ordered on `stream`).  n, m > 0 and finite non-zero A, W
+ * (CztError::EmptyLength / InvalidParameters -> AFC_ERR_VALIDATION).  Execute:
+ * `batch` contiguous lanes of n complex inputs -> `batch` lanes of m complex
+ * outputs (F32: complex64, F64: complex128), device pointers, on `stream`.
+ *
+ * afc_czt_inverse replaces CztPlan::inverse (plan/czt/dimension_1d.rs:250-293,
+ * czt_bjork_pereyra_inverse_into in kernel/bluestein.rs:167-223): the exact
+ * inverse of a square plan by the Björck-Pereyra solve of the Vandermonde
+ * system on z_k = W^k, then x_k = y_k A^k, in FP64 (complex64 plans convert
+ * on load and store), one CTA per lane.  Errors as the reference's
+ * CztError::NotInvertible (AFC_ERR_VALIDATION): m != n, or two nodes closer
+ * than 1024 eps (W a root of unity of order <= n); n beyond one CTA's shared
+ * memory (n > 7040) is AFC_ERR_UNSUPPORTED.  `batch` lanes of n in, n out. */
 typedef struct afc_czt_plan_s* afc_czt_plan;
 AFC_API afc_status afc_czt_plan_create(afc_czt_plan* out, int64_t n, int64_t m, double a_re, double a_im,
                                        double w_re, double w_im, afc_precision precision, int device);
 AFC_API afc_status afc_czt_execute(afc_czt_plan plan, const void* in, void* out, int64_t batch, void* stream);
+AFC_API afc_status afc_czt_inverse(afc_czt_plan plan, const void* spectrum, void* out, int64_t batch, void* stream);
 AFC_API afc_status afc_czt_conv_len(afc_czt_plan plan, int64_t* conv_len);
 AFC_API afc_status afc_czt_plan_destroy(afc_czt_plan plan);
 

@@ -89,5 +89,83 @@ def test_czt_two_calls_and_validation(afc, cuda):
         CztPlan(4, 4, 0.0, 1.0)
     with pytest.raises(CztError):
         CztPlan(4, 4, 1.0, float("nan"))
-    with pytest.raises(afc.AfcError):
-        CztPlan(100000, 100000)  # convolution beyond one CTA
+
+
+@pytest.mark.parametrize("n,m,prec", [(3000, 3000, "f64"), (5000, 1200, "f64"), (8000, 8000, "f32")])
+def test_czt_beyond_one_cta(afc, oracle, cuda, n, m, prec):
+    """Convolution lengths beyond one CTA (8192 in f64, 16384 in f32) run the
+    same steps around the multi-pass plan of length L."""
+    from apollofft_b200.czt import CztPlan
+    a, w = cmath.exp(0.2j), cmath.exp(-2j * cmath.pi * 0.7 / m)
+    rng = np.random.default_rng(n + m)
+    x = rng.uniform(-1, 1, (2, n)) + 1j * rng.uniform(-1, 1, (2, n))
+    plan = CztPlan(n, m, a, w, precision=prec)
+    L = plan.convolution_len()
+    assert L == 1 << int(np.ceil(np.log2(n + m - 1)))
+    dt = np.complex128 if prec == "f64" else np.complex64
+    y = plan.forward(torch.from_numpy(x.astype(dt)).cuda()).cpu().numpy()
+    ref = czt_reference(x.astype(dt).astype(np.complex128), m, a, w, oracle)
+    assert rel_l2(y, ref) < (1e-12 if prec == "f64" else 1e-5)
+    # a few bins against the direct sum
+    ks = [0, 1, m // 3, m - 1]
+    j = np.arange(n)
+    for k in ks:
+        d = x.astype(dt).astype(np.complex128) @ np.array([cpowf(a, -jj) * cpowf(w, jj * k) for jj in j])
+        assert np.max(np.abs(y[:, k] - d)) / np.max(np.abs(d)) < (1e-9 if prec == "f64" else 1e-3)
+
+
+def bjorck_pereyra(y, a, w):
+    """apollo-czt's czt_bjork_pereyra_inverse_into (kernel/bluestein.rs:181-223) in numpy loops."""
+    n = len(y)
+    z = []
+    wk = 1 + 0j
+    for _ in range(n):
+        z.append(wk)
+        wk *= w
+    c = np.array(y, dtype=np.complex128)
+    for j in range(n - 1):
+        for k in range(n - 1, j, -1):
+            c[k] = (c[k] - c[k - 1]) / (z[k] - z[k - j - 1])
+    for j in range(n - 2, -1, -1):
+        for k in range(j, n - 1):
+            c[k] -= z[j] * c[k + 1]
+    ap = 1 + 0j
+    for k in range(n):
+        c[k] *= ap
+        ap *= a
+    return c
+
+
+@pytest.mark.parametrize("n,a,w", [
+    (16, 1.0, cmath.exp(-2j * cmath.pi / 16)),                  # the DFT (czt/dimension_1d.rs:965-983)
+    (6, cmath.exp(0.5j), cmath.exp(-2j * cmath.pi / 6)),        # general A (:986-1003)
+    (5, 1.0, cmath.rect(1.1, -0.9)),                            # non-unit W (:1006-1021)
+    (48, cmath.exp(0.2j), cmath.exp(-2j * cmath.pi / 48)),
+])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_czt_inverse(afc, cuda, n, a, w, prec):
+    from apollofft_b200.czt import CztPlan
+    rng = np.random.default_rng(n)
+    x = rng.uniform(-1, 1, (3, n)) + 1j * rng.uniform(-1, 1, (3, n))
+    plan = CztPlan(n, n, a, w, precision=prec)
+    dt = np.complex128 if prec == "f64" else np.complex64
+    X = plan.forward(torch.from_numpy(x.astype(dt)).cuda())
+    back = plan.inverse(X).cpu().numpy()
+    Xh = X.cpu().numpy().astype(np.complex128)
+    ref = np.stack([bjorck_pereyra(Xh[i], a, w) for i in range(3)])
+    # against the reference's solve on the same spectrum, and the round trip at
+    # the reference's own bounds (1e-10 DFT, 1e-9 general A, 1e-8 non-unit W)
+    assert rel_l2(back, ref) < (1e-12 if prec == "f64" else 1e-5)
+    bound = 1e-10 if abs(abs(w) - 1) < 1e-12 and a == 1.0 else 1e-8
+    if prec == "f64":
+        assert np.max(np.abs(back - x)) < max(bound, 1e-8 * n)
+
+
+def test_czt_inverse_errors(afc, cuda):
+    from apollofft_b200.czt import CztError, CztPlan
+    X = torch.zeros(8, dtype=torch.complex128, device="cuda")
+    with pytest.raises(CztError, match="square"):
+        CztPlan(8, 6, 1.0, cmath.exp(-0.3j)).inverse(torch.zeros(6, dtype=torch.complex128, device="cuda"))
+    # W of order 4 <= n: the nodes W^k collide
+    with pytest.raises(CztError, match="collide"):
+        CztPlan(8, 8, 1.0, cmath.exp(-2j * cmath.pi / 4)).inverse(X)

@@ -43,7 +43,9 @@ def test_hann_window_is_symmetric():  # apollo-stft stft/dimension_1d/tests.rs:1
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("frame_len,hop,n_sig", [(512, 128, 8192), (256, 256, 1000), (1024, 300, 20000),
-                                                 (64, 1, 64), (16, 5, 333), (4096, 1024, 50000), (243, 81, 5000)])
+                                                 (64, 1, 64), (16, 5, 333), (4096, 1024, 50000), (243, 81, 5000),
+                                                 # frames beyond one CTA: four-step and large-prime Bluestein plans
+                                                 (16384, 4096, 100000), (10007, 2500, 60000)])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_stft_forward_vs_oracle(afc, oracle, cuda, frame_len, hop, n_sig, prec):
     from apollofft_b200.stft import StftPlan
@@ -98,7 +100,7 @@ def istft_ref(spec, window, frame_len, hop, n_sig, oracle):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("frame_len,hop,n_sig", [(8, 4, 12), (512, 128, 8192), (256, 200, 1000), (1024, 256, 20001),
-                                                 (243, 81, 5000)])
+                                                 (243, 81, 5000), (16384, 4096, 100001)])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_stft_inverse_vs_reference_and_roundtrip(afc, oracle, cuda, frame_len, hop, n_sig, prec):
     from apollofft_b200.stft import StftPlan
