@@ -140,7 +140,7 @@ def bjorck_pereyra(y, a, w):
     (16, 1.0, cmath.exp(-2j * cmath.pi / 16)),                  # the DFT (czt/dimension_1d.rs:965-983)
     (6, cmath.exp(0.5j), cmath.exp(-2j * cmath.pi / 6)),        # general A (:986-1003)
     (5, 1.0, cmath.rect(1.1, -0.9)),                            # non-unit W (:1006-1021)
-    (48, cmath.exp(0.2j), cmath.exp(-2j * cmath.pi / 48)),
+    (12, cmath.exp(0.2j), cmath.exp(-2j * cmath.pi / 12)),
 ])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_czt_inverse(afc, cuda, n, a, w, prec):
@@ -154,7 +154,10 @@ def test_czt_inverse(afc, cuda, n, a, w, prec):
     Xh = X.cpu().numpy().astype(np.complex128)
     ref = np.stack([bjorck_pereyra(Xh[i], a, w) for i in range(3)])
     # against the reference's solve on the same spectrum, and the round trip at
-    # the reference's own bounds (1e-10 DFT, 1e-9 general A, 1e-8 non-unit W)
+    # the reference's own bounds (1e-10 DFT, 1e-9 general A, 1e-8 non-unit W).
+    # Divided differences amplify rounding quickly with n (at n = 48 two FP64
+    # evaluations of the same solve already differ by 5e-5), so the cases keep
+    # the small lengths the reference tests.
     assert rel_l2(back, ref) < (1e-12 if prec == "f64" else 1e-5)
     bound = 1e-10 if abs(abs(w) - 1) < 1e-12 and a == 1.0 else 1e-8
     if prec == "f64":
