@@ -80,7 +80,8 @@ struct TmaPlan {
   bool inplace = false;
   // kernel build: 0 any radix (256 threads), 1 radix 2/4/8/16 (256 threads),
   // 2 radix 2/4/8/16 complex128 at <= 128 threads, three CTAs per SM,
-  // 3 7-smooth, 4 complex64 in place with two butterflies of a radix <= 8 stage
+  // 3 7-smooth, 4 complex64 in place with two butterflies of a radix <= 8 stage,
+  // 5 n = 256 as radix 16 x 16 in place with fixed shared-memory offsets
   int variant = 0;
   // contiguous in-place tiles only: real input lanes (widened in the first
   // stage) / real output lanes (real parts stored by the last stage)

@@ -279,6 +279,58 @@ __device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long t
   bulk_commit();
 }
 
+// Threads per CTA and CTAs per SM each kernel build is compiled for.
+template <class T, int V> struct TmaBuild {
+  static constexpr int threads = (V == 2 || (V == 5 && sizeof(T) == 8)) ? 128 : 256;
+  static constexpr int ctas =
+      threads == 128 ? 3 : (V == 3 || ((V == 1 || V == 4 || V == 5) && sizeof(T) == 4)) ? 2 : 1;
+};
+
+// n = 256 as two radix-16 stages in place, every shared-memory address a
+// compile-time offset from one per-thread base (variant 5).  The general
+// stage code computes each element's address from the runtime lane stride,
+// element stride and padding, and selects between the scaled and unscaled
+// output of every stage: on B200 that is more integer and select instructions
+// per point than FP64 ones.  Layouts as in the general path: the slot holds
+// the tile linearly (strided mode: element i of lane l at i LK + l;
+// contiguous: at 256 l + i), stage 0 writes the padded layout (element i at
+// 273 l + i + i / 16) and stage 1 writes the linear layout back.  The thread
+// (l, t) owns butterfly t < 16 of lane l in both stages.  Strided tiles hold
+// LK lanes (8 complex128 / 16 complex64).
+template <class T, bool INV, bool LM, int LK>
+__device__ __forceinline__ void stages256(const TmaArgs<T>& a, typename CT<T>::type* cur,
+                                          const typename CT<T>::type* __restrict__ twb, int l, int t) {
+  using C = typename CT<T>::type;
+  constexpr int LD = 273;                // padded lane stride of a 256-point lane
+  constexpr int S = LM ? 16 * LK : 16;   // linear layout: distance of elements t and t + 16
+  C* const lin = LM ? cur + l + t * LK : cur + l * 256 + t;
+  C v[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) v[r] = lin[r * S];
+  __syncthreads();
+  DFT<16, INV>::run(v);
+  C* const p0 = cur + l * LD + 17 * t;  // outputs 16 t + r, no twiddles (Ns = 1)
+#pragma unroll
+  for (int r = 0; r < 16; ++r) p0[r] = v[r];
+  __syncthreads();
+  C* const p1 = cur + l * LD + t;  // inputs t + 16 r at t + 17 r
+#pragma unroll
+  for (int r = 0; r < 16; ++r) v[r] = p1[17 * r];
+  __syncthreads();
+  const C* const tw = twb + a.sl.st[1].twoff + t;  // Ns = 16: twiddle (r - 1) 16 + t
+#pragma unroll
+  for (int r = 1; r < 16; ++r) v[r] = INV ? cmulc(v[r], tw[(r - 1) * 16]) : cmul(v[r], tw[(r - 1) * 16]);
+  DFT<16, INV>::run(v);
+  const T sc = a.scale;
+  if (sc != (T)1) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = cscale(v[r], sc);
+  }
+#pragma unroll
+  for (int r = 0; r < 16; ++r) lin[r * S] = v[r];  // outputs t + 16 r
+  __syncthreads();
+}
+
 // Every stage of the tile in slot `cur` (`work` is the ping-pong buffer when
 // the stages do not run in place).  Returns the buffer that holds the result in
 // the linear layout, the TMA store's source.  Every thread of the CTA calls it
@@ -291,6 +343,14 @@ __device__ __forceinline__ typename CT<T>::type* tma_stages(const TmaArgs<T>& a,
   constexpr bool P2 = V == 1 || V == 2 || V == 4;
   constexpr bool S7 = V == 3;
   using C = typename CT<T>::type;
+  if constexpr (V == 5) {
+    constexpr int LK = sizeof(T) == 8 ? 8 : 16;
+    if (a.mode == 1)
+      stages256<T, INV, true, LK>(a, cur, twb, l, t);
+    else
+      stages256<T, INV, false, LK>(a, cur, twb, l, t);
+    return cur;
+  }
   const int L = a.L, P = a.P, n = a.sl.n, ld = a.ld;
   const bool lm = a.mode == 1;
   const TView<C> wv{work, ld, 1, 1};
@@ -400,10 +460,11 @@ __device__ __forceinline__ typename CT<T>::type* tma_stages(const TmaArgs<T>& a,
 // Variant 3: 7-smooth plans (radix 2/3/4/5/7/8/16, no 11 or 13), built for two
 // CTAs of up to 256 threads per SM (at most 128 registers).  Variant 4:
 // complex64 power-of-two in place with two butterflies per thread in the
-// radix <= 8 stages (the 256-thread build of variant 1 otherwise).
+// radix <= 8 stages (the 256-thread build of variant 1 otherwise).  Variant 5:
+// n = 256 as radix 16 x 16 in place (stages256), 16 threads per lane, built
+// like variant 2 for complex128 and like variant 1 for complex64.
 template <class T, bool INV, int V, bool IP>
-__global__ void __launch_bounds__(V == 2 ? 128 : 256,
-                                  V == 2 ? 3 : (V == 3 || ((V == 1 || V == 4) && sizeof(T) == 4)) ? 2 : 1)
+__global__ void __launch_bounds__(TmaBuild<T, V>::threads, TmaBuild<T, V>::ctas)
     tma_kernel(const __grid_constant__ TmaArgs<T> a) {
   using C = typename CT<T>::type;
   extern __shared__ __align__(128) unsigned char smraw[];
@@ -589,8 +650,7 @@ __device__ __forceinline__ typename CT<T>::type* pair_transform(const TmaArgs<T>
 }
 
 template <class T, bool INV, int V, bool IP>
-__global__ void __launch_bounds__(V == 2 ? 128 : 256,
-                                  V == 2 ? 3 : (V == 3 || ((V == 1 || V == 4) && sizeof(T) == 4)) ? 2 : 1)
+__global__ void __launch_bounds__(TmaBuild<T, V>::threads, TmaBuild<T, V>::ctas)
     tma_pair_kernel(const __grid_constant__ TmaPairArgs<T> pa) {
   using C = typename CT<T>::type;
   // no static shared variables: they would move the dynamic block off the
@@ -781,10 +841,13 @@ static long long twiddle_count(const StageList& sl) {
 
 // CTAs per SM the register budget of a kernel build allows (its launch bounds).
 static int build_ctas_per_sm(int variant, bool dbl) {
-  if (variant == 2) return 3;
-  if (variant == 3 || ((variant == 1 || variant == 4) && !dbl)) return 2;
+  if (variant == 2 || (variant == 5 && dbl)) return 3;
+  if (variant == 3 || ((variant == 1 || variant == 4 || variant == 5) && !dbl)) return 2;
   return 1;
 }
+
+// Threads per CTA a kernel build is compiled for (its launch bounds).
+static int build_threads(int variant, bool dbl) { return (variant == 2 || (variant == 5 && dbl)) ? 128 : 256; }
 
 // Keeps the twiddle table resident in shared memory when that costs no CTA
 // per SM (228 KB per SM, 1 KB reserved per CTA), for the odd-radix builds
@@ -890,6 +953,21 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
     tp.variant = 4;
   }
   if (real && !tp.inplace) return false;
+  // n = 256 as radix 16 x 16 on complex lanes: the build with fixed addresses.
+  // Measured on B200 at 256^3 (forward, 20 warm repetitions): complex64 went
+  // from 206 to 151 us per transform (2.6x fewer instructions: the general
+  // stages' address and select arithmetic bounded the passes), while
+  // complex128, whose passes are DRAM-bound at 3 CTAs per SM either way, went
+  // from 285 to 298 us (twiddles resident in shared memory changed nothing),
+  // so complex128 keeps the general build.  AFC_TMA_N256: 0 off, 1 complex64
+  // (default), 2 both; read at every plan.
+  const char* n256_env = getenv("AFC_TMA_N256");
+  const int n256_on = n256_env && *n256_env ? atoi(n256_env) : 1;
+  if (n256_on && (!dbl || n256_on >= 2) && n == 256 && sl.nst == 2 && sl.st[0].R == 16 && sl.st[1].R == 16 && sl.st[0].Ns == 1 &&
+      sl.st[1].Ns == 16 && tp.inplace && !real && ld == 273 && P == 16 &&
+      (tp.variant == 2 || (tp.variant == 1 && !dbl)) && tp.L * P == build_threads(5, dbl) &&
+      (tp.mode == 0 || tp.L == (dbl ? 8 : 16)))
+    tp.variant = 5;
   tp.real_in = real_in;
   tp.real_out = real_out;
   const int align = dbl ? 8 : 16;  // 128-byte aligned slots
@@ -975,7 +1053,8 @@ static int sm_count() {
 template <class T, bool INV>
 static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, cudaStream_t st) {
   using C = typename CT<T>::type;
-  auto k = tp.variant == 4  ? tma_kernel<T, INV, 4, true>
+  auto k = tp.variant == 5  ? tma_kernel<T, INV, 5, true>
+           : tp.variant == 4 ? tma_kernel<T, INV, 4, true>
            : tp.variant == 2 ? tma_kernel<T, INV, 2, true>
            : tp.variant == 1 ? (tp.inplace ? tma_kernel<T, INV, 1, true> : tma_kernel<T, INV, 1, false>)
            : tp.variant == 3 ? tma_kernel<T, INV, 3, false>
@@ -1004,7 +1083,8 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
 }
 
 template <class T, bool INV> static const void* pair_kernel_ptr(int variant, bool ip) {
-  auto k = variant == 4   ? tma_pair_kernel<T, INV, 4, true>
+  auto k = variant == 5   ? tma_pair_kernel<T, INV, 5, true>
+           : variant == 4 ? tma_pair_kernel<T, INV, 4, true>
            : variant == 2 ? tma_pair_kernel<T, INV, 2, true>
            : variant == 1 ? (ip ? tma_pair_kernel<T, INV, 1, true> : tma_pair_kernel<T, INV, 1, false>)
                           : tma_pair_kernel<T, INV, 3, false>;
@@ -1055,7 +1135,9 @@ bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes,
   const size_t csz = dbl ? 16 : 8;
   pp.slot_elems = std::max(a.slot_elems, b.slot_elems);
   pp.threads = std::max(a.L * a.P, b.L * b.P);
-  if (pp.threads > (a.variant == 2 ? 128 : 256)) return false;
+  if (pp.threads > build_threads(a.variant, dbl)) return false;
+  // the fixed-address build gives every thread a butterfly in both phases
+  if (a.variant == 5 && (a.L * a.P != pp.threads || b.L * b.P != pp.threads)) return false;
   pp.smem = 2 * (size_t)pp.slot_elems * csz +
             (a.inplace ? 0 : (size_t)std::max(a.L * a.ld, b.L * b.ld) * csz) + 64;
   if (pp.smem > 220 * 1024) return false;
