@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libapollofft_cuda.so")
-SOURCES = ["afc_kernels.cu", "afc_tma.cu", "afc_tc.cu", "afc_nufft.cu", "afc_callers.cu", "afc_api.cu"]
+SOURCES = ["afc_kernels.cu", "afc_tma.cu", "afc_plane.cu", "afc_tc.cu", "afc_nufft.cu", "afc_callers.cu", "afc_api.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

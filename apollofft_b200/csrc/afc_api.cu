@@ -1254,6 +1254,38 @@ static bool try_pair(const afc_plan_s& p, int a0, int a1, const AxisIO& io0, con
   return true;
 }
 
+// The two plane-local passes as one launch of the cluster plane kernel when
+// both axes have 256 points (radix 16 x 16) and the passes are plain complex
+// lanes: rows (the last axis) then columns, whichever order run_plan chose
+// (the two orders differ by rounding only).  Reads the first pass's input,
+// writes the second pass's output; false when the kernel cannot take them.
+static bool try_plane(const afc_plan_s& p, const AxisIO& io0, const AxisIO& io1, bool inv, cudaStream_t st,
+                      cudaError_t& e) {
+  if (p.kind != AFC_KIND_C2C || p.rank < 2 || p.tc || tl_rec) return false;
+  const AxisPlan& az = *p.axes[p.rank - 1];
+  const AxisPlan& ay = *p.axes[p.rank - 2];
+  for (const AxisPlan* ap : {&az, &ay}) {
+    const StageList& sl = ap->lp.sl;
+    if (ap->algo != ALGO_SMEM || ap->n != 256 || sl.nst != 2 || sl.st[0].R != 16 || sl.st[1].R != 16 ||
+        sl.st[0].Ns != 1 || sl.st[1].Ns != 16 || !ap->lp.tw)
+      return false;
+  }
+  for (const AxisIO* io : {&io0, &io1})
+    if (io->in_op != IN_C || io->out_op != OUT_C) return false;
+  // the second pass transforms the first pass's output in place
+  if (io1.in != io0.out || io1.out != io0.out) return false;
+  const long long planes = p.batch * (p.rank == 3 ? p.dims[0] : 1);
+  PlanePlan pp;
+  if (!plane_plan(planes, p.dbl, inv, io0.in, io1.out, pp)) return false;
+  unsigned* err = device_err_word();
+  if (!err) return false;
+  const size_t csz = p.dbl ? 16 : 8;
+  const char* twz = static_cast<const char*>(az.lp.tw) + (size_t)az.lp.sl.st[1].twoff * csz;
+  const char* twy = static_cast<const char*>(ay.lp.tw) + (size_t)ay.lp.sl.st[1].twoff * csz;
+  e = launch_plane(pp, io0.in, io1.out, twz, twy, io0.scale * io1.scale, err, p.dbl, inv, st);
+  return true;
+}
+
 // Runs one transform of the plan.  scale is applied on the last pass;
 // pair_w is the Hermitian weight used by the R2C_HALF adjoints.
 static cudaError_t run_plan(const afc_plan_s& p, const void* in, void* out, bool inv, double scale, double pair_w,
@@ -1347,7 +1379,7 @@ static cudaError_t run_plan(const afc_plan_s& p, const void* in, void* out, bool
     // y then z inverse) when both fit the TMA kernels
     if (k + 1 < order.size() && a >= r - 2 && order[k + 1] >= r - 2) {
       cudaError_t pe = cudaSuccess;
-      if (try_pair(p, a, order[k + 1], io, ios[k + 1], inv, st, pe)) {
+      if (try_plane(p, io, ios[k + 1], inv, st, pe) || try_pair(p, a, order[k + 1], io, ios[k + 1], inv, st, pe)) {
         if (pe != cudaSuccess) return pe;
         ++k;
         continue;

@@ -1,5 +1,6 @@
 // afc_internal.h -- host <-> kernel interface inside libapollofft_cuda.so.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cstddef>
@@ -95,6 +96,25 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
               void* out, bool dbl, int lanes_pref, TmaPlan& tp, bool real_in = false, bool real_out = false);
 size_t tma_smem_bytes(const TmaPlan& tp, size_t csz);
 cudaError_t launch_tma(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, bool dbl, bool inv, cudaStream_t st);
+
+// Tensor map of lanes viewed as [2 es scalars, n, outer] with box [2 L, bn, 1]
+// (afc_tma.cu); false when the driver cannot encode it.
+bool tma_lane_map(CUtensorMap* m, const void* base, bool dbl, long long es, long long n, long long outer, int L, int bn);
+
+// The last two axes of a C2C transform with 256 x 256 planes in one launch
+// (afc_plane.cu, plane_kernel): a thread-block cluster owns a plane, its CTAs
+// transform their rows, exchange columns through distributed shared memory and
+// transform the columns.
+struct PlanePlan {
+  int cfg = 0;        // kernel build (cluster size, plane buffers, CTAs per SM)
+  int cs = 0;         // CTAs per cluster
+  int nclusters = 0;  // clusters launched (persistent over the planes)
+  size_t smem = 0;
+  long long planes = 0;
+};
+bool plane_plan(long long planes, bool dbl, bool inv, const void* in, const void* out, PlanePlan& pp);
+cudaError_t launch_plane(const PlanePlan& pp, const void* in, void* out, const void* twz, const void* twy,
+                         double scale, unsigned* err, bool dbl, bool inv, cudaStream_t st);
 
 // Two axis passes over the same x-planes in one launch (afc_tma.cu,
 // tma_pair_kernel): a thread-block cluster per plane transforms the plane's

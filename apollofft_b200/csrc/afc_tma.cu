@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include <cstdlib>
 #include <cstring>
+#include "afc_async.cuh"
 #include "afc_engine.cuh"
 #include "afc_internal.h"
 
@@ -66,31 +67,6 @@ __device__ __forceinline__ void tile_lanes(const TmaArgs<T>& a, long long tile, 
   nl = (int)(rem < a.L ? rem : a.L);
 }
 
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait: about 2^21 polls (each try_wait itself suspends for a while),
-// a few seconds at most; false on timeout.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity, int limit = 1 << 21) {
-  for (int i = 0; i < limit; ++i)
-    if (mbar_try_wait(b, parity)) return true;
-  return false;
-}
-
 // Exercises the timeout path of the bounded wait: one thread waits on a
 // barrier that nothing arrives on, gives up after `polls` polls and records the
 // timeout in the error word, exactly as the transform kernels do.
@@ -102,35 +78,6 @@ __global__ void wait_probe_kernel(unsigned* err, int polls) {
     if (!mbar_wait(&bar, 0, polls)) atomicExch(err, 1u);
   }
 }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
-
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
-                                            unsigned long long* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int c0, int c1, int c2, const void* src) {
-  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];\n" ::"l"(map), "r"(c0),
-               "r"(c1), "r"(c2), "r"(smem_u32(src))
-               : "memory");
-}
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src)), "r"(bytes)
-               : "memory");
-}
-
 template <class C> struct TView {
   C* p;
   int ls, is, pad;
@@ -282,8 +229,12 @@ __device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long t
 // Threads per CTA and CTAs per SM each kernel build is compiled for.
 template <class T, int V> struct TmaBuild {
   static constexpr int threads = (V == 2 || (V == 5 && sizeof(T) == 8)) ? 128 : 256;
-  static constexpr int ctas =
-      threads == 128 ? 3 : (V == 3 || ((V == 1 || V == 4 || V == 5) && sizeof(T) == 4)) ? 2 : 1;
+  // complex64 4096-point build: three CTAs per SM (80 registers; measured on
+  // B200 16384 x 4096 forward 255 -> 242 us against two); the complex64
+  // 256-point build gained nothing from a third CTA (256^3: 151 -> 154 us)
+  static constexpr int ctas = threads == 128 || (V == 6 && sizeof(T) == 4)
+                                  ? 3
+                                  : (V == 3 || ((V == 1 || V == 4 || V == 5) && sizeof(T) == 4)) ? 2 : 1;
 };
 
 // n = 256 as two radix-16 stages in place, every shared-memory address a
@@ -331,6 +282,56 @@ __device__ __forceinline__ void stages256(const TmaArgs<T>& a, typename CT<T>::t
   __syncthreads();
 }
 
+// n = 4096 as three radix-16 stages in place on one contiguous lane per tile
+// (variant 6), addresses fixed as in stages256: thread t < 256 owns butterfly
+// t of every stage.  Stage 0 reads the linear lane (t + 256 r) and writes the
+// padded layout (element i at i + i / 16) at 16 t + r; stage 1 (Ns = 16) reads
+// t + 256 r and writes 16 (t - k) + k + 16 r with k = t mod 16; stage 2
+// (Ns = 256) reads t + 256 r and writes the linear lane at t + 256 r.
+template <class T, bool INV>
+__device__ __forceinline__ void stages4096(const TmaArgs<T>& a, typename CT<T>::type* cur,
+                                           const typename CT<T>::type* __restrict__ twb, int t) {
+  using C = typename CT<T>::type;
+  C v[16];
+  C* const lin = cur + t;
+#pragma unroll
+  for (int r = 0; r < 16; ++r) v[r] = lin[256 * r];
+  __syncthreads();
+  DFT<16, INV>::run(v);
+  C* const p0 = cur + 17 * t;
+#pragma unroll
+  for (int r = 0; r < 16; ++r) p0[r] = v[r];
+  __syncthreads();
+  C* const pin = cur + t + (t >> 4);  // padded t + 256 r: t + t / 16 + 272 r
+#pragma unroll
+  for (int r = 0; r < 16; ++r) v[r] = pin[272 * r];
+  __syncthreads();
+  const int k = t & 15;
+  const C* const tw1 = twb + a.sl.st[1].twoff + k;
+#pragma unroll
+  for (int r = 1; r < 16; ++r) v[r] = INV ? cmulc(v[r], tw1[(r - 1) * 16]) : cmul(v[r], tw1[(r - 1) * 16]);
+  DFT<16, INV>::run(v);
+  C* const p1 = cur + 272 * (t >> 4) + k;  // padded 256 (t / 16) + k + 16 r
+#pragma unroll
+  for (int r = 0; r < 16; ++r) p1[17 * r] = v[r];
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 16; ++r) v[r] = pin[272 * r];
+  __syncthreads();
+  const C* const tw2 = twb + a.sl.st[2].twoff + t;
+#pragma unroll
+  for (int r = 1; r < 16; ++r) v[r] = INV ? cmulc(v[r], tw2[(r - 1) * 256]) : cmul(v[r], tw2[(r - 1) * 256]);
+  DFT<16, INV>::run(v);
+  const T sc = a.scale;
+  if (sc != (T)1) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = cscale(v[r], sc);
+  }
+#pragma unroll
+  for (int r = 0; r < 16; ++r) lin[256 * r] = v[r];
+  __syncthreads();
+}
+
 // Every stage of the tile in slot `cur` (`work` is the ping-pong buffer when
 // the stages do not run in place).  Returns the buffer that holds the result in
 // the linear layout, the TMA store's source.  Every thread of the CTA calls it
@@ -349,6 +350,10 @@ __device__ __forceinline__ typename CT<T>::type* tma_stages(const TmaArgs<T>& a,
       stages256<T, INV, true, LK>(a, cur, twb, l, t);
     else
       stages256<T, INV, false, LK>(a, cur, twb, l, t);
+    return cur;
+  }
+  if constexpr (V == 6) {
+    stages4096<T, INV>(a, cur, twb, t);
     return cur;
   }
   const int L = a.L, P = a.P, n = a.sl.n, ld = a.ld;
@@ -555,33 +560,6 @@ template <class T> struct TmaPairArgs {
   int n0, n1;         // tiles per plane of each phase
   int slot_elems;     // per slot: the larger of the two phases
 };
-
-__device__ __forceinline__ unsigned cluster_rank() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ unsigned cluster_nrank() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ unsigned cluster_id() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%clusterid.x;\n" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ unsigned cluster_count() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%nclusterid.x;\n" : "=r"(r));
-  return r;
-}
-// Every thread of every CTA of the cluster: writes before are visible to
-// reads after in the other CTAs (release / acquire at cluster scope).
-__device__ __forceinline__ void cluster_sync_all() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
-}
-__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
 
 // This CTA's work items: per plane q of the cluster (p = cluster + q * clusters),
 // its phase-0 tiles r, r + CS, ... < n0, one barrier, its phase-1 tiles
@@ -824,6 +802,11 @@ static bool make_map(CUtensorMap* m, const void* base, bool dbl, long long es, l
   return r == CUDA_SUCCESS;
 }
 
+bool tma_lane_map(CUtensorMap* m, const void* base, bool dbl, long long es, long long n, long long outer, int L,
+                  int bn) {
+  return make_map(m, base, dbl, es, n, outer, L, bn);
+}
+
 static int g_tma_sm = 0;
 
 size_t tma_smem_bytes(const TmaPlan& tp, size_t csz) {
@@ -841,7 +824,7 @@ static long long twiddle_count(const StageList& sl) {
 
 // CTAs per SM the register budget of a kernel build allows (its launch bounds).
 static int build_ctas_per_sm(int variant, bool dbl) {
-  if (variant == 2 || (variant == 5 && dbl)) return 3;
+  if (variant == 2 || (variant == 5 && dbl) || (variant == 6 && !dbl)) return 3;
   if (variant == 3 || ((variant == 1 || variant == 4 || variant == 5) && !dbl)) return 2;
   return 1;
 }
@@ -968,6 +951,16 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
       (tp.variant == 2 || (tp.variant == 1 && !dbl)) && tp.L * P == build_threads(5, dbl) &&
       (tp.mode == 0 || tp.L == (dbl ? 8 : 16)))
     tp.variant = 5;
+  // n = 4096 as radix 16 x 16 x 16 on one contiguous complex lane per tile:
+  // the fixed-address build.  Measured on B200: 16384 x 4096 complex64
+  // forward from 350 to 255 us, 64 x 4096 complex128 forward + inverse from
+  // 20.8 to 17.9 us.  AFC_TMA_N4096: 0 off, 1 complex64 only, 2 both (default).
+  const char* n4096_env = getenv("AFC_TMA_N4096");
+  const int n4096_on = n4096_env && *n4096_env ? atoi(n4096_env) : 2;
+  if (n4096_on && (!dbl || n4096_on >= 2) && n == 4096 && sl.nst == 3 && sl.st[0].R == 16 && sl.st[1].R == 16 &&
+      sl.st[2].R == 16 && sl.st[0].Ns == 1 && sl.st[1].Ns == 16 && sl.st[2].Ns == 256 && tp.inplace && !real &&
+      ld == 4353 && P == 256 && tp.mode == 0 && tp.L == 1 && tp.variant == 1)
+    tp.variant = 6;
   tp.real_in = real_in;
   tp.real_out = real_out;
   const int align = dbl ? 8 : 16;  // 128-byte aligned slots
@@ -1053,7 +1046,8 @@ static int sm_count() {
 template <class T, bool INV>
 static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, cudaStream_t st) {
   using C = typename CT<T>::type;
-  auto k = tp.variant == 5  ? tma_kernel<T, INV, 5, true>
+  auto k = tp.variant == 6  ? tma_kernel<T, INV, 6, true>
+           : tp.variant == 5 ? tma_kernel<T, INV, 5, true>
            : tp.variant == 4 ? tma_kernel<T, INV, 4, true>
            : tp.variant == 2 ? tma_kernel<T, INV, 2, true>
            : tp.variant == 1 ? (tp.inplace ? tma_kernel<T, INV, 1, true> : tma_kernel<T, INV, 1, false>)
@@ -1083,7 +1077,8 @@ static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned
 }
 
 template <class T, bool INV> static const void* pair_kernel_ptr(int variant, bool ip) {
-  auto k = variant == 5   ? tma_pair_kernel<T, INV, 5, true>
+  auto k = variant == 6   ? tma_pair_kernel<T, INV, 6, true>
+           : variant == 5 ? tma_pair_kernel<T, INV, 5, true>
            : variant == 4 ? tma_pair_kernel<T, INV, 4, true>
            : variant == 2 ? tma_pair_kernel<T, INV, 2, true>
            : variant == 1 ? (ip ? tma_pair_kernel<T, INV, 1, true> : tma_pair_kernel<T, INV, 1, false>)

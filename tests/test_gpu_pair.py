@@ -20,8 +20,11 @@ TOL = {"f64": 1e-12, "f32": 1e-5}
 
 @pytest.fixture(autouse=True)
 def pair_on(monkeypatch):
-    """The pass pair is opt-in (AFC_PAIR=1, read by the library per execution)."""
+    """The pass pair is opt-in (AFC_PAIR=1, read by the library per execution);
+    256 x 256 planes would take the cluster plane kernel first (AFC_PLANE=0
+    keeps them on the pair)."""
     monkeypatch.setenv("AFC_PAIR", "1")
+    monkeypatch.setenv("AFC_PLANE", "0")
 
 
 def cplx(rng, shape):
