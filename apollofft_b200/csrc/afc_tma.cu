@@ -860,9 +860,12 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
   if (im.d1 != 1 || om.d1 != 1 || im.d2 != om.d2 || im.s0 != om.s0 || im.es != om.es || im.s2 != om.s2) return false;
   if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) return false;
   if (n < 2) return false;
+  // contiguous complex64 lanes of odd length: a lane starts on 8 bytes only,
+  // so tiles hold an even number of lanes and start at even lanes
+  const bool lane2 = im.es == 1 && (n * (long long)csz) % 16 != 0;
   if (im.es == 1) {  // contiguous lanes at q * n
     if (im.d2 != 1 || im.s0 != n) return false;
-    if ((n * (long long)csz) % 16) return false;
+    if (lane2 && (real || (n * (long long)csz) % 8 || (lanes & 1))) return false;
     tp.mode = 0;
     tp.L = 1;
     tp.bn = (int)n;
@@ -917,6 +920,7 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
   const int tmax = (v2_on && dbl && p2 && ip128) ? 128 : 256;
   if (tp.mode == 0) {
     int L = std::max(1, tmax / P);
+    if (lane2) L = std::max(2, L & ~1);
     tp.L = L;
   }
   while (tp.L * P > tmax) P = std::max(1, P / 2);
@@ -969,8 +973,8 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
   se = (se + align - 1) / align * align;
   tp.slot_elems = (int)se;
   // shrink the contiguous tile until it fits comfortably
-  while (tp.mode == 0 && tp.L > 1 && tma_smem_bytes(tp, csz) > 110 * 1024) {
-    tp.L--;
+  while (tp.mode == 0 && tp.L > (lane2 ? 2 : 1) && tma_smem_bytes(tp, csz) > 110 * 1024) {
+    tp.L -= lane2 ? 2 : 1;
     se = (long long)tp.L * std::max<long long>(ld, n);
     se = (se + align - 1) / align * align;
     tp.slot_elems = (int)se;
@@ -1117,6 +1121,8 @@ bool tma_pair_plan(const LaunchDesc& d0, const LaunchDesc& d1, long long planes,
     if (d.lanes % planes) return false;
     if (tp.mode == 0) {
       pp.lpp[ph] = d.lanes / planes;
+      // odd-length complex64 lanes: every tile of a plane must start at an even lane
+      if ((d.sl.n * (long long)(dbl ? 16 : 8)) % 16 && (pp.lpp[ph] & 1)) return false;
       pp.n[ph] = (int)((pp.lpp[ph] + tp.L - 1) / tp.L);
     } else {
       if (tp.outer != planes) return false;
