@@ -82,7 +82,9 @@ struct TmaPlan {
   // kernel build: 0 any radix (256 threads), 1 radix 2/4/8/16 (256 threads),
   // 2 radix 2/4/8/16 complex128 at <= 128 threads, three CTAs per SM,
   // 3 7-smooth, 4 complex64 in place with two butterflies of a radix <= 8 stage,
-  // 5 n = 256 as radix 16 x 16 in place with fixed shared-memory offsets
+  // 5 n = 256 as radix 16 x 16 in place with fixed shared-memory offsets,
+  // 6 n = 4096 as radix 16 x 16 x 16 likewise, 7 a compile-time stage list
+  // of a smooth odd length (out of place)
   int variant = 0;
   // contiguous in-place tiles only: real input lanes (widened in the first
   // stage) / real output lanes (real parts stored by the last stage)
@@ -91,6 +93,8 @@ struct TmaPlan {
   int tw_res = 0;
   // tile slots of the load ring (2 or 3): slots - 1 tile loads in flight per CTA
   int nslot = 2;
+  // variant 7: index of the compile-time stage list (afc_tma.cu, kFixed)
+  int fix = -1;
 };
 bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, const LaneMap& om, const void* in,
               void* out, bool dbl, int lanes_pref, TmaPlan& tp, bool real_in = false, bool real_out = false);

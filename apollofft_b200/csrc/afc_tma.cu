@@ -234,7 +234,7 @@ template <class T, int V> struct TmaBuild {
   // 256-point build gained nothing from a third CTA (256^3: 151 -> 154 us)
   static constexpr int ctas = threads == 128 || (V == 6 && sizeof(T) == 4)
                                   ? 3
-                                  : (V == 3 || ((V == 1 || V == 4 || V == 5) && sizeof(T) == 4)) ? 2 : 1;
+                                  : (V == 3 || V == 7 || ((V == 1 || V == 4 || V == 5) && sizeof(T) == 4)) ? 2 : 1;
 };
 
 // n = 256 as two radix-16 stages in place, every shared-memory address a
@@ -332,18 +332,93 @@ __device__ __forceinline__ void stages4096(const TmaArgs<T>& a, typename CT<T>::
   __syncthreads();
 }
 
+// A stage list fixed at compile time (variant 7): length N as radices R0 R1
+// [R2], P threads per lane, LK lanes per strided tile (0: contiguous lanes).
+// Each stage is the general out-of-place Stockham stage with every stride a
+// constant, and without the 16-element padding: the smooth odd lengths this
+// build serves (343 = 7^3, 243 = 9 9 3, 250 = 10 5 5) have odd or
+// non-power-of-two strides, so their shared-memory accesses do not need it.
+// Intermediate stages ping-pong between the slot and the work buffer in the
+// lane layout (element i of lane l at N l + i); contiguous tiles hold the
+// same layout, strided tiles hold element i of lane l at LK i + l.
+struct FixNone {};
+template <int N_, int R0_, int R1_, int R2_, int P_, int LK_> struct Fix {
+  static constexpr int N = N_, P = P_, LK = LK_;
+  static constexpr int NST = R2_ ? 3 : 2;
+  static constexpr int R(int s) { return s == 0 ? R0_ : s == 1 ? R1_ : R2_; }
+  static constexpr int NS(int s) { return s == 0 ? 1 : s == 1 ? R0_ : R0_ * R1_; }
+};
+
+template <class T, bool INV, class FX, int S>
+__device__ __forceinline__ void fixed_stage(const TmaArgs<T>& a, const typename CT<T>::type* src,
+                                            typename CT<T>::type* dst, const typename CT<T>::type* __restrict__ twb,
+                                            int l, int t) {
+  using C = typename CT<T>::type;
+  constexpr int N = FX::N, P = FX::P, R = FX::R(S), NS = FX::NS(S), NB = N / R, IT = (NB + P - 1) / P;
+  constexpr bool LM = FX::LK > 0, LAST = S == FX::NST - 1;
+  constexpr int SLS = (S == 0 && LM) ? 1 : N, SIS = (S == 0 && LM) ? FX::LK : 1;
+  constexpr int DLS = (LAST && LM) ? 1 : N, DIS = (LAST && LM) ? FX::LK : 1;
+  const C* const tw = twb + a.sl.st[S].twoff;
+  const T sc = a.scale;
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int j = t + it * P;
+    if (j < NB) {
+      C v[R];
+      const C* s = src + l * SLS + j * SIS;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = s[r * NB * SIS];
+      const int k = NS == 1 ? 0 : j % NS;
+      if (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          const C w = tw[(r - 1) * NS + k];
+          v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
+        }
+      }
+      DFT<R, INV>::run(v);
+      if (LAST && sc != (T)1) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = cscale(v[r], sc);
+      }
+      C* d = dst + l * DLS + ((j - k) * R + k) * DIS;
+#pragma unroll
+      for (int r = 0; r < R; ++r) d[r * NS * DIS] = v[r];
+    }
+  }
+}
+
+// Every stage of a fixed list; returns the buffer holding the linear result.
+template <class T, bool INV, class FX>
+__device__ __forceinline__ typename CT<T>::type* fixed_stages(const TmaArgs<T>& a, typename CT<T>::type* cur,
+                                                              typename CT<T>::type* work,
+                                                              const typename CT<T>::type* twb, int l, int t) {
+  fixed_stage<T, INV, FX, 0>(a, cur, work, twb, l, t);
+  __syncthreads();
+  fixed_stage<T, INV, FX, 1>(a, work, cur, twb, l, t);
+  __syncthreads();
+  if constexpr (FX::NST == 3) {
+    fixed_stage<T, INV, FX, 2>(a, cur, work, twb, l, t);
+    __syncthreads();
+    return work;
+  } else {
+    return cur;
+  }
+}
+
 // Every stage of the tile in slot `cur` (`work` is the ping-pong buffer when
 // the stages do not run in place).  Returns the buffer that holds the result in
 // the linear layout, the TMA store's source.  Every thread of the CTA calls it
 // (the stages hold CTA barriers); (l, t) is the thread's lane and position in
 // the lane, with t >= P for a thread that has no butterflies in this tile.
-template <class T, bool INV, int V, bool IP>
+template <class T, bool INV, int V, bool IP, class FX = FixNone>
 __device__ __forceinline__ typename CT<T>::type* tma_stages(const TmaArgs<T>& a, typename CT<T>::type* cur,
                                                             typename CT<T>::type* work,
                                                             const typename CT<T>::type* twb, int l, int t) {
   constexpr bool P2 = V == 1 || V == 2 || V == 4;
   constexpr bool S7 = V == 3;
   using C = typename CT<T>::type;
+  if constexpr (V == 7) return fixed_stages<T, INV, FX>(a, cur, work, twb, l, t);
   if constexpr (V == 5) {
     constexpr int LK = sizeof(T) == 8 ? 8 : 16;
     if (a.mode == 1)
@@ -468,7 +543,7 @@ __device__ __forceinline__ typename CT<T>::type* tma_stages(const TmaArgs<T>& a,
 // radix <= 8 stages (the 256-thread build of variant 1 otherwise).  Variant 5:
 // n = 256 as radix 16 x 16 in place (stages256), 16 threads per lane, built
 // like variant 2 for complex128 and like variant 1 for complex64.
-template <class T, bool INV, int V, bool IP>
+template <class T, bool INV, int V, bool IP, class FX = FixNone>
 __global__ void __launch_bounds__(TmaBuild<T, V>::threads, TmaBuild<T, V>::ctas)
     tma_kernel(const __grid_constant__ TmaArgs<T> a) {
   using C = typename CT<T>::type;
@@ -528,7 +603,7 @@ __global__ void __launch_bounds__(TmaBuild<T, V>::threads, TmaBuild<T, V>::ctas)
       return;
     }
     C* cur = slots[cs];
-    C* obuf = tma_stages<T, INV, V, IP>(a, cur, work, twb, l, t);
+    C* obuf = tma_stages<T, INV, V, IP, FX>(a, cur, work, twb, l, t);
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) tma_issue_store(a, tile, obuf);
@@ -825,13 +900,31 @@ static long long twiddle_count(const StageList& sl) {
 // CTAs per SM the register budget of a kernel build allows (its launch bounds).
 static int build_ctas_per_sm(int variant, bool dbl) {
   if (variant == 2 || (variant == 5 && dbl) || (variant == 6 && !dbl)) return 3;
-  if (variant == 3 || ((variant == 1 || variant == 4 || variant == 5) && !dbl)) return 2;
+  if (variant == 3 || variant == 7 || ((variant == 1 || variant == 4 || variant == 5) && !dbl)) return 2;
   return 1;
 }
 
 // Threads per CTA a kernel build is compiled for (its launch bounds).
 static int build_threads(int variant, bool dbl) { return (variant == 2 || (variant == 5 && dbl)) ? 128 : 256; }
 
+// The compile-time stage lists built (variant 7): the smooth odd axis lengths
+// of the 243 x 250 x 343 volume, with the thread and lane counts tma_plan
+// picks for them (contiguous tiles, and strided tiles of 8 complex128 / 16
+// complex64 lanes).
+#define AFC_FIXED_LIST(X)                                                                                \
+  X(true, 343, 7, 7, 7, 22, 0) X(true, 343, 7, 7, 7, 22, 8) X(true, 243, 9, 9, 3, 16, 0)              \
+  X(true, 243, 9, 9, 3, 16, 8) X(true, 250, 10, 5, 5, 16, 0) X(true, 250, 10, 5, 5, 16, 8)            \
+  X(false, 343, 7, 7, 7, 22, 0) X(false, 343, 7, 7, 7, 11, 16) X(false, 243, 9, 9, 3, 16, 0)          \
+  X(false, 243, 9, 9, 3, 16, 16) X(false, 250, 10, 5, 5, 16, 0) X(false, 250, 10, 5, 5, 16, 16)
+struct FixedEntry {
+  bool dbl;
+  int n, r0, r1, r2, P, LK;
+};
+static const FixedEntry kFixed[] = {
+#define AFC_FX_ENTRY(D, N, R0, R1, R2, P, LK) {D, N, R0, R1, R2, P, LK},
+    AFC_FIXED_LIST(AFC_FX_ENTRY)
+#undef AFC_FX_ENTRY
+};
 // Keeps the twiddle table resident in shared memory when that costs no CTA
 // per SM (228 KB per SM, 1 KB reserved per CTA), for the odd-radix builds
 // only: measured on B200, 243 x 250 x 343 complex128 went from 1.32 to 1.25 ms
@@ -840,7 +933,7 @@ static int build_threads(int variant, bool dbl) { return (variant == 2 || (varia
 static void plan_resident_twiddles(const StageList& sl, bool dbl, TmaPlan& tp, size_t extra = 0) {
   const size_t csz = dbl ? 16 : 8;
   tp.tw_res = 0;
-  if (tp.variant != 0 && tp.variant != 3) return;
+  if (tp.variant != 0 && tp.variant != 3 && tp.variant != 7) return;
   const long long twc = twiddle_count(sl);
   if (twc <= 0) return;
   const size_t base = tma_smem_bytes(tp, csz) + extra;
@@ -940,6 +1033,24 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
     tp.variant = 4;
   }
   if (real && !tp.inplace) return false;
+  // a 7-smooth out-of-place plan whose stage list, threads and tile are built
+  // at compile time (AFC_TMA_FIXED=0 keeps the general build; read at every plan)
+  {
+    const char* fx_env = getenv("AFC_TMA_FIXED");
+    const bool fx_on = !(fx_env && *fx_env && atoi(fx_env) == 0);
+    const int nent = (int)(sizeof(kFixed) / sizeof(kFixed[0]));
+    for (int i = 0; fx_on && tp.variant == 3 && !tp.inplace && !real && i < nent; ++i) {
+      const FixedEntry& e = kFixed[i];
+      const int nst = e.r2 ? 3 : 2;
+      if (e.dbl != dbl || e.n != n || sl.nst != nst || sl.st[0].R != e.r0 || sl.st[1].R != e.r1 ||
+          (nst == 3 && sl.st[2].R != e.r2) || P != e.P)
+        continue;
+      if (e.LK == 0 ? tp.mode != 0 : (tp.mode != 1 || tp.L != e.LK)) continue;
+      tp.variant = 7;
+      tp.fix = i;
+      break;
+    }
+  }
   // n = 256 as radix 16 x 16 on complex lanes: the build with fixed addresses.
   // Measured on B200 at 256^3 (forward, 20 warm repetitions): complex64 went
   // from 206 to 151 us per transform (2.6x fewer instructions: the general
@@ -1047,16 +1158,30 @@ static int sm_count() {
   return g_tma_sm;
 }
 
+template <class T, bool INV> static auto fixed_kernel(int fix) -> decltype(&tma_kernel<T, INV, 0, false>) {
+  int i = 0;
+#define AFC_FX_KERNEL(D, N, R0, R1, R2, P, LK)                                  \
+  if constexpr ((sizeof(T) == 8) == D) {                                        \
+    if (fix == i) return &tma_kernel<T, INV, 7, false, Fix<N, R0, R1, R2, P, LK>>; \
+  }                                                                             \
+  ++i;
+  AFC_FIXED_LIST(AFC_FX_KERNEL)
+#undef AFC_FX_KERNEL
+  return nullptr;
+}
+
 template <class T, bool INV>
 static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, cudaStream_t st) {
   using C = typename CT<T>::type;
-  auto k = tp.variant == 6  ? tma_kernel<T, INV, 6, true>
+  auto k = tp.variant == 7  ? fixed_kernel<T, INV>(tp.fix)
+           : tp.variant == 6 ? tma_kernel<T, INV, 6, true>
            : tp.variant == 5 ? tma_kernel<T, INV, 5, true>
            : tp.variant == 4 ? tma_kernel<T, INV, 4, true>
            : tp.variant == 2 ? tma_kernel<T, INV, 2, true>
            : tp.variant == 1 ? (tp.inplace ? tma_kernel<T, INV, 1, true> : tma_kernel<T, INV, 1, false>)
            : tp.variant == 3 ? tma_kernel<T, INV, 3, false>
                              : tma_kernel<T, INV, 0, false>;
+  if (!k) return cudaErrorInvalidValue;
   const size_t smem = tma_smem_bytes(tp, sizeof(C));
   cudaError_t e = kernel_smem_grant(reinterpret_cast<const void*>(k), smem);
   if (e != cudaSuccess) return e;

@@ -2,11 +2,15 @@
 constant) against the general build and the oracle: 256 points as radix
 16 x 16 for contiguous lanes (1D batches, the last axis of a 3D volume) and
 strided lanes (the middle and first axes), alone and inside the pass pair, and
-4096 points as radix 16 x 16 x 16 on contiguous lanes; forward and inverse
-with 1/N, in and out of place.
+4096 points as radix 16 x 16 x 16 on contiguous lanes, and the compile-time
+stage lists of the smooth odd lengths 343 = 7 7 7, 243 = 9 9 3 and
+250 = 10 5 5 on contiguous and strided lanes; forward and inverse with 1/N, in
+and out of place.
 
 AFC_TMA_N256 / AFC_TMA_N4096 (read by the library at every plan): 0 general
-build, 1 the fixed build for complex64 (default), 2 for complex128 as well.  Results against the
+build, 1 the fixed build for complex64, 2 for complex128 as well (N256 default
+1, N4096 default 2).  AFC_TMA_FIXED: 0 general build, 1 the stage lists
+(default).  Results against the
 oracle's FftPlan1D/3D (crates/apollo-fft/src/application/execution/plan/fft/
 dimension_{1,3}d.rs) at f64 <= 1e-12 and f32 <= 1e-5; both builds compute the
 same butterflies with the same twiddles in the same order, so their outputs
@@ -31,6 +35,7 @@ def cplx(rng, shape):
 def run(afc, cuda, monkeypatch, mode, shape, prec, x, inverse=False, batch=1):
     monkeypatch.setenv("AFC_TMA_N256", str(mode))
     monkeypatch.setenv("AFC_TMA_N4096", str(mode))
+    monkeypatch.setenv("AFC_TMA_FIXED", "1" if mode else "0")
     p = afc.CudaPlan(list(shape), precision=prec, batch=batch)
     return p.execute(torch.from_numpy(x).to(cuda, DT[prec]), inverse=inverse).cpu().numpy()
 
@@ -38,7 +43,9 @@ def run(afc, cuda, monkeypatch, mode, shape, prec, x, inverse=False, batch=1):
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 @pytest.mark.parametrize("shape,batch", [((256,), 37), ((256,), 1), ((3, 256, 256), 1), ((256, 256), 2),
                                          ((256, 8, 256), 1), ((256, 2, 2), 1), ((4096,), 1), ((4096,), 300),
-                                         ((3, 4096), 2), ((5, 7, 4096), 1)])
+                                         ((3, 4096), 2), ((5, 7, 4096), 1), ((343,), 50), ((243,), 33),
+                                         ((250,), 64), ((7, 9, 343), 1), ((243, 250, 34), 1),
+                                         ((250, 6, 243), 1)])
 def test_fixed_build_matches_oracle_and_general(afc, oracle, cuda, monkeypatch, prec, shape, batch):
     rng = np.random.default_rng(256 + len(shape) + batch)
     full = (batch,) + shape if batch > 1 else shape
