@@ -234,7 +234,9 @@ template <class T, int V> struct TmaBuild {
   // 256-point build gained nothing from a third CTA (256^3: 151 -> 154 us)
   static constexpr int ctas = threads == 128 || (V == 6 && sizeof(T) == 4)
                                   ? 3
-                                  : (V == 3 || V == 7 || ((V == 1 || V == 4 || V == 5) && sizeof(T) == 4)) ? 2 : 1;
+                                  : (V == 3 || V == 7 || ((V == 1 || V == 4 || V == 5 || V == 8) && sizeof(T) == 4))
+                                        ? 2
+                                        : 1;
 };
 
 // n = 256 as two radix-16 stages in place, every shared-memory address a
@@ -388,6 +390,112 @@ __device__ __forceinline__ void fixed_stage(const TmaArgs<T>& a, const typename 
   }
 }
 
+// A power-of-two stage list fixed at compile time and run in place in the
+// slot (variant 8): length N as radices R0 R1 R2 [R3], P threads per lane
+// (a thread holds N / (R P) butterflies of a stage across its barrier), LK
+// lanes per strided tile (0: contiguous lanes, whose stage 0 may read real
+// input and whose last stage may store real parts).  The padded layout
+// (element i of lane l at LD l + i + i / 16) keeps every address a
+// compile-time offset from one per-butterfly base wherever the stage's
+// input stride N / R and output stride Ns are multiples of 16 or the
+// first stage is radix 16; elsewhere the padding term is computed per element.
+template <int N_, int R0_, int R1_, int R2_, int R3_, int P_, int LK_> struct FixIP {
+  static constexpr int N = N_, P = P_, LK = LK_;
+  static constexpr int LD = (N + (N - 1) / 16 + 1) | 1;  // the plan's padded lane stride
+  static constexpr int NST = R3_ ? 4 : R2_ ? 3 : 2;
+  static constexpr int R(int s) { return s == 0 ? R0_ : s == 1 ? R1_ : s == 2 ? R2_ : R3_; }
+  static constexpr int NS(int s) { return s == 0 ? 1 : R(s - 1) * NS(s - 1); }
+};
+
+template <class T, bool INV, class FX, int S>
+__device__ __forceinline__ void fixed_stage_ip(const TmaArgs<T>& a, typename CT<T>::type* cur,
+                                               const typename CT<T>::type* __restrict__ twb, int l, int t) {
+  using C = typename CT<T>::type;
+  constexpr int N = FX::N, P = FX::P, LD = FX::LD, R = FX::R(S), NS = FX::NS(S), NB = N / R;
+  constexpr int NBT = (NB + P - 1) / P;
+  constexpr bool LM = FX::LK > 0, LAST = S == FX::NST - 1;
+  static_assert(NB % P == 0, "every thread holds the same number of butterflies");
+  C v[NBT][R];
+  // ── reads: element j + r NB ──
+#pragma unroll
+  for (int b = 0; b < NBT; ++b) {
+    const int j = t + b * P;
+    if constexpr (S == 0) {
+      if (!LM && a.real_in) {
+        const T* s = reinterpret_cast<const T*>(cur) + l * N + j;
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[b][r] = C{s[r * NB], (T)0};
+      } else {
+        const C* s = LM ? cur + l + j * FX::LK : cur + l * N + j;
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[b][r] = s[r * NB * (LM ? FX::LK : 1)];
+      }
+    } else {
+      static_assert(NB % 16 == 0, "padded reads need a stride that is a multiple of 16");
+      const C* s = cur + l * LD + j + (j >> 4);
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b][r] = s[r * (NB + NB / 16)];
+    }
+  }
+  __syncthreads();
+  const T sc = a.scale;
+#pragma unroll
+  for (int b = 0; b < NBT; ++b) {
+    const int j = t + b * P;
+    const int k = j & (NS - 1);
+    if constexpr (NS > 1) {
+      const C* const tw = twb + a.sl.st[S].twoff + k;
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const C w = tw[(r - 1) * NS];
+        v[b][r] = INV ? cmulc(v[b][r], w) : cmul(v[b][r], w);
+      }
+    }
+    DFT<R, INV>::run(v[b]);
+    const int o = (j - k) * R + k;  // outputs o + r NS
+    if constexpr (LAST) {
+      if (sc != (T)1) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[b][r] = cscale(v[b][r], sc);
+      }
+      if (!LM && a.real_out) {
+        T* d = reinterpret_cast<T*>(cur) + l * N + o;
+#pragma unroll
+        for (int r = 0; r < R; ++r) d[r * NS] = v[b][r].x;
+      } else {
+        C* d = LM ? cur + l + o * FX::LK : cur + l * N + o;
+#pragma unroll
+        for (int r = 0; r < R; ++r) d[r * NS * (LM ? FX::LK : 1)] = v[b][r];
+      }
+    } else if constexpr (NS % 16 == 0) {
+      C* d = cur + l * LD + o + (o >> 4);
+#pragma unroll
+      for (int r = 0; r < R; ++r) d[r * (NS + NS / 16)] = v[b][r];
+    } else if constexpr (NS == 1 && R == 16) {
+      C* d = cur + l * LD + 17 * j;  // o + r = 16 j + r, padded 17 j + r
+#pragma unroll
+      for (int r = 0; r < R; ++r) d[r] = v[b][r];
+    } else {
+      C* d = cur + l * LD;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int p = o + r * NS;
+        d[p + (p >> 4)] = v[b][r];
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <class T, bool INV, class FX>
+__device__ __forceinline__ void fixed_stages_ip(const TmaArgs<T>& a, typename CT<T>::type* cur,
+                                                const typename CT<T>::type* twb, int l, int t) {
+  fixed_stage_ip<T, INV, FX, 0>(a, cur, twb, l, t);
+  fixed_stage_ip<T, INV, FX, 1>(a, cur, twb, l, t);
+  if constexpr (FX::NST >= 3) fixed_stage_ip<T, INV, FX, 2>(a, cur, twb, l, t);
+  if constexpr (FX::NST >= 4) fixed_stage_ip<T, INV, FX, 3>(a, cur, twb, l, t);
+}
+
 // Every stage of a fixed list; returns the buffer holding the linear result.
 template <class T, bool INV, class FX>
 __device__ __forceinline__ typename CT<T>::type* fixed_stages(const TmaArgs<T>& a, typename CT<T>::type* cur,
@@ -419,6 +527,10 @@ __device__ __forceinline__ typename CT<T>::type* tma_stages(const TmaArgs<T>& a,
   constexpr bool S7 = V == 3;
   using C = typename CT<T>::type;
   if constexpr (V == 7) return fixed_stages<T, INV, FX>(a, cur, work, twb, l, t);
+  if constexpr (V == 8) {
+    fixed_stages_ip<T, INV, FX>(a, cur, twb, l, t);
+    return cur;
+  }
   if constexpr (V == 5) {
     constexpr int LK = sizeof(T) == 8 ? 8 : 16;
     if (a.mode == 1)
@@ -900,7 +1012,8 @@ static long long twiddle_count(const StageList& sl) {
 // CTAs per SM the register budget of a kernel build allows (its launch bounds).
 static int build_ctas_per_sm(int variant, bool dbl) {
   if (variant == 2 || (variant == 5 && dbl) || (variant == 6 && !dbl)) return 3;
-  if (variant == 3 || variant == 7 || ((variant == 1 || variant == 4 || variant == 5) && !dbl)) return 2;
+  if (variant == 3 || variant == 7 || ((variant == 1 || variant == 4 || variant == 5 || variant == 8) && !dbl))
+    return 2;
   return 1;
 }
 
@@ -918,12 +1031,21 @@ static int build_threads(int variant, bool dbl) { return (variant == 2 || (varia
   X(false, 243, 9, 9, 3, 16, 16) X(false, 250, 10, 5, 5, 16, 0) X(false, 250, 10, 5, 5, 16, 16)
 struct FixedEntry {
   bool dbl;
-  int n, r0, r1, r2, P, LK;
+  int n, r0, r1, r2, r3, P, LK;
 };
 static const FixedEntry kFixed[] = {
-#define AFC_FX_ENTRY(D, N, R0, R1, R2, P, LK) {D, N, R0, R1, R2, P, LK},
+#define AFC_FX_ENTRY(D, N, R0, R1, R2, P, LK) {D, N, R0, R1, R2, 0, P, LK},
     AFC_FIXED_LIST(AFC_FX_ENTRY)
 #undef AFC_FX_ENTRY
+};
+// The in-place power-of-two stage lists built (variant 8): 2048 points in
+// complex64 (the 2048 x 2048 images), contiguous (complex or real lanes) and
+// strided tiles of 2 lanes.
+#define AFC_FIXED_IP_LIST(X) X(false, 2048, 16, 16, 8, 0, 128, 0) X(false, 2048, 16, 16, 8, 0, 128, 2)
+static const FixedEntry kFixedIP[] = {
+#define AFC_FXI_ENTRY(D, N, R0, R1, R2, R3, P, LK) {D, N, R0, R1, R2, R3, P, LK},
+    AFC_FIXED_IP_LIST(AFC_FXI_ENTRY)
+#undef AFC_FXI_ENTRY
 };
 // Keeps the twiddle table resident in shared memory when that costs no CTA
 // per SM (228 KB per SM, 1 KB reserved per CTA), for the odd-radix builds
@@ -1050,6 +1172,19 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
       tp.fix = i;
       break;
     }
+    const int nip = (int)(sizeof(kFixedIP) / sizeof(kFixedIP[0]));
+    for (int i = 0; fx_on && (tp.variant == 1 || tp.variant == 4) && tp.inplace && i < nip; ++i) {
+      const FixedEntry& e = kFixedIP[i];
+      const int nst = e.r3 ? 4 : e.r2 ? 3 : 2;
+      if (e.dbl != dbl || e.n != n || sl.nst != nst || sl.st[0].R != e.r0 || sl.st[1].R != e.r1 ||
+          (nst >= 3 && sl.st[2].R != e.r2) || (nst >= 4 && sl.st[3].R != e.r3) || P != e.P)
+        continue;
+      if (e.LK == 0 ? tp.mode != 0 : (tp.mode != 1 || tp.L != e.LK || real)) continue;
+      if (ld != ((e.n + (e.n - 1) / 16 + 1) | 1) || tp.L * P > 256) continue;
+      tp.variant = 8;
+      tp.fix = i;
+      break;
+    }
   }
   // n = 256 as radix 16 x 16 on complex lanes: the build with fixed addresses.
   // Measured on B200 at 256^3 (forward, 20 warm repetitions): complex64 went
@@ -1169,11 +1304,23 @@ template <class T, bool INV> static auto fixed_kernel(int fix) -> decltype(&tma_
 #undef AFC_FX_KERNEL
   return nullptr;
 }
+template <class T, bool INV> static auto fixed_ip_kernel(int fix) -> decltype(&tma_kernel<T, INV, 0, false>) {
+  int i = 0;
+#define AFC_FXI_KERNEL(D, N, R0, R1, R2, R3, P, LK)                                       \
+  if constexpr ((sizeof(T) == 8) == D) {                                                  \
+    if (fix == i) return &tma_kernel<T, INV, 8, true, FixIP<N, R0, R1, R2, R3, P, LK>>; \
+  }                                                                                       \
+  ++i;
+  AFC_FIXED_IP_LIST(AFC_FXI_KERNEL)
+#undef AFC_FXI_KERNEL
+  return nullptr;
+}
 
 template <class T, bool INV>
 static cudaError_t launch_tma_t(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, cudaStream_t st) {
   using C = typename CT<T>::type;
-  auto k = tp.variant == 7  ? fixed_kernel<T, INV>(tp.fix)
+  auto k = tp.variant == 8  ? fixed_ip_kernel<T, INV>(tp.fix)
+           : tp.variant == 7 ? fixed_kernel<T, INV>(tp.fix)
            : tp.variant == 6 ? tma_kernel<T, INV, 6, true>
            : tp.variant == 5 ? tma_kernel<T, INV, 5, true>
            : tp.variant == 4 ? tma_kernel<T, INV, 4, true>

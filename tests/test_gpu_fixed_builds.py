@@ -45,7 +45,7 @@ def run(afc, cuda, monkeypatch, mode, shape, prec, x, inverse=False, batch=1):
                                          ((256, 8, 256), 1), ((256, 2, 2), 1), ((4096,), 1), ((4096,), 300),
                                          ((3, 4096), 2), ((5, 7, 4096), 1), ((343,), 50), ((243,), 33),
                                          ((250,), 64), ((7, 9, 343), 1), ((243, 250, 34), 1),
-                                         ((250, 6, 243), 1)])
+                                         ((250, 6, 243), 1), ((2048,), 37), ((2048, 10), 1), ((3, 2048, 6), 1)])
 def test_fixed_build_matches_oracle_and_general(afc, oracle, cuda, monkeypatch, prec, shape, batch):
     rng = np.random.default_rng(256 + len(shape) + batch)
     full = (batch,) + shape if batch > 1 else shape
@@ -86,3 +86,27 @@ def test_fixed_build_in_place_and_in_the_pair(afc, oracle, cuda, monkeypatch, pr
     assert rel_l2(y, ref) < TOL[prec]
     back = p2.execute(torch.from_numpy(ref).to(cuda, DT[prec]), inverse=True).cpu().numpy()
     assert rel_l2(back, oracle.fft3d(ref, inverse=True)) < TOL[prec]
+
+
+@pytest.mark.parametrize("kind", ["r2c_full", "r2c_half"])
+@pytest.mark.parametrize("shape,batch", [((2048,), 6), ((2, 2048), 3), ((2048, 2048), 1)])
+def test_fixed_real_lanes_2048(afc, cuda, monkeypatch, kind, shape, batch):
+    """Real input rows widened in the first stage and real parts stored by the
+    last stage of the in-place 2048-point build, against numpy (f32 <= 1e-5)
+    and against the general build."""
+    rng = np.random.default_rng(2048 + batch)
+    x = rng.standard_normal((batch,) + shape).astype(np.float32)
+    axes = tuple(range(1, len(shape) + 1))
+    ref = np.fft.fftn(x.astype(np.float64), axes=axes)
+    if kind == "r2c_half":
+        ref = np.fft.rfftn(x.astype(np.float64), axes=axes)
+    outs = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("AFC_TMA_FIXED", mode)
+        p = afc.CudaPlan(list(shape), precision="f32", kind=kind, batch=batch)
+        y = p.execute(torch.from_numpy(x).to(cuda))
+        back = p.execute(y, inverse=True)
+        outs[mode] = (y.cpu().numpy().reshape(ref.shape), back.cpu().numpy().reshape(x.shape))
+    assert rel_l2(outs["1"][0], ref) < 1e-5
+    assert rel_l2(outs["1"][1], x) < 1e-5
+    assert rel_l2(outs["1"][0], outs["0"][0]) < 1e-6
