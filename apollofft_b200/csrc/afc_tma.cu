@@ -358,8 +358,12 @@ __device__ __forceinline__ void fixed_stage(const TmaArgs<T>& a, const typename 
   using C = typename CT<T>::type;
   constexpr int N = FX::N, P = FX::P, R = FX::R(S), NS = FX::NS(S), NB = N / R, IT = (NB + P - 1) / P;
   constexpr bool LM = FX::LK > 0, LAST = S == FX::NST - 1;
-  constexpr int SLS = (S == 0 && LM) ? 1 : N, SIS = (S == 0 && LM) ? FX::LK : 1;
-  constexpr int DLS = (LAST && LM) ? 1 : N, DIS = (LAST && LM) ? FX::LK : 1;
+  // intermediate lanes at an odd stride: the lanes of a strided tile sit in the
+  // same wavefront (8 complex128 / 16 complex64 lanes, one element each), and an
+  // odd stride puts them in distinct banks
+  constexpr int LDU = N | 1;
+  constexpr int SLS = S == 0 ? (LM ? 1 : N) : LDU, SIS = (S == 0 && LM) ? FX::LK : 1;
+  constexpr int DLS = LAST ? (LM ? 1 : N) : LDU, DIS = (LAST && LM) ? FX::LK : 1;
   const C* const tw = twb + a.sl.st[S].twoff;
   const T sc = a.scale;
 #pragma unroll
@@ -399,9 +403,24 @@ __device__ __forceinline__ void fixed_stage(const TmaArgs<T>& a, const typename 
 // compile-time offset from one per-butterfly base wherever the stage's
 // input stride N / R and output stride Ns are multiples of 16 or the
 // first stage is radix 16; elsewhere the padding term is computed per element.
+// Padded lane stride of the in-place builds: the plan's (odd) stride for
+// contiguous tiles; for strided tiles of LK lanes, whose lanes share a
+// shared-memory wavefront (128 bytes: 16 complex64 or 8 complex128 elements,
+// LK lanes x 16 / LK or 8 / LK butterflies), the first stride at least as
+// large that is congruent to (elements per wavefront) / LK, so the lanes'
+// elements fall in distinct banks.
+__host__ __device__ constexpr int fixip_ld(int n, int lk, int csz) {
+  const int ld = (n + (n - 1) / 16 + 1) | 1;
+  const int per = 128 / csz;
+  if (lk <= 1 || lk >= per) return ld;
+  const int want = per / lk;
+  int v = ld;
+  while (v % per != want) ++v;
+  return v;
+}
+
 template <int N_, int R0_, int R1_, int R2_, int R3_, int P_, int LK_> struct FixIP {
   static constexpr int N = N_, P = P_, LK = LK_;
-  static constexpr int LD = (N + (N - 1) / 16 + 1) | 1;  // the plan's padded lane stride
   static constexpr int NST = R3_ ? 4 : R2_ ? 3 : 2;
   static constexpr int R(int s) { return s == 0 ? R0_ : s == 1 ? R1_ : s == 2 ? R2_ : R3_; }
   static constexpr int NS(int s) { return s == 0 ? 1 : R(s - 1) * NS(s - 1); }
@@ -411,7 +430,8 @@ template <class T, bool INV, class FX, int S>
 __device__ __forceinline__ void fixed_stage_ip(const TmaArgs<T>& a, typename CT<T>::type* cur,
                                                const typename CT<T>::type* __restrict__ twb, int l, int t) {
   using C = typename CT<T>::type;
-  constexpr int N = FX::N, P = FX::P, LD = FX::LD, R = FX::R(S), NS = FX::NS(S), NB = N / R;
+  constexpr int N = FX::N, P = FX::P, LD = fixip_ld(FX::N, FX::LK, (int)sizeof(C)), R = FX::R(S), NS = FX::NS(S),
+                NB = N / R;
   constexpr int NBT = (NB + P - 1) / P;
   constexpr bool LM = FX::LK > 0, LAST = S == FX::NST - 1;
   static_assert(NB % P == 0, "every thread holds the same number of butterflies");
@@ -1224,6 +1244,11 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
     se = (long long)tp.L * std::max<long long>(ld, n);
     se = (se + align - 1) / align * align;
     tp.slot_elems = (int)se;
+  }
+  if (tp.variant == 8) {  // the slot holds the tile in the build's padded layout
+    const FixedEntry& e = kFixedIP[tp.fix];
+    const long long need = ((long long)tp.L * fixip_ld(e.n, e.LK, (int)csz) + align - 1) / align * align;
+    if (need > tp.slot_elems) tp.slot_elems = (int)need;
   }
   if (tma_smem_bytes(tp, csz) > 220 * 1024) return false;
   // a third slot (two tile loads in flight per CTA) when it costs no CTA per
