@@ -1441,10 +1441,11 @@ static afc_status create_plan(afc_plan* out, int rank, const int64_t* dims, afc_
   const bool tcp = prec == AFC_PREC_TC_BF16_SPLIT || prec == AFC_PREC_TC_FP16_SPLIT;
   if (tcp) {
     const int64_t n = dims[0];
-    bool pow16 = rank == 1 && kind == AFC_KIND_C2C && n >= 16 && (n & (n - 1)) == 0 && (__builtin_ctzll(n) % 4 == 0);
-    if (!pow16 || n > 4096)
+    const bool pow2 = rank == 1 && kind == AFC_KIND_C2C && n >= 16 && (n & (n - 1)) == 0;
+    if (!pow2 || n > 4096)
       return fail(AFC_ERR_UNSUPPORTED,
-                  "tensor-core plans are rank-1 C2C with n = 16^s <= 4096 (radix-16 stages only); got rank %d, n %lld",
+                  "tensor-core plans are rank-1 C2C with n = 2^k, 16 <= n <= 4096 (radix-16 stages on the tensor "
+                  "cores, one radix-2/4/8 stage on the CUDA cores); got rank %d, n %lld",
                   rank, (long long)n);
   }
   if (kind != AFC_KIND_C2C && kind != AFC_KIND_R2C_FULL && kind != AFC_KIND_R2C_HALF)

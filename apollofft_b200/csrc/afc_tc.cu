@@ -263,6 +263,58 @@ __device__ __forceinline__ void tc_issue_load(const TcArgs& a, long long tile, f
   tcb_load(slot, a.in + q0 * a.sl.n, bytes, bar);
 }
 
+// The radix-2/4/8 stage of a power-of-two length that is not 16^s, on the
+// CUDA cores in FP32, in place in the slot like the tensor-core stages: the
+// tile's 4096 / R butterflies are 16 / R per thread (the whole stage's reads
+// finish before the barrier, its writes come after).  Same layouts as the
+// tensor-core stages: the first stage reads lane l at n l + i, later stages the
+// padded layout ld l + i + i / 16, the last stage writes n l + i.
+template <int R>
+__device__ __forceinline__ void tc_simt_stage(float2* cur, int n, int ld, int Ns, const float2* __restrict__ tws,
+                                              bool first, bool last, bool inverse, float scale, int t) {
+  constexpr int PER = 16 / R;
+  const int nb = n / R;
+  float2 v[PER][R];
+#pragma unroll
+  for (int b = 0; b < PER; ++b) {
+    const int g = t + b * 256, l = g / nb, j = g - l * nb;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = j + r * nb;
+      v[b][r] = first ? cur[l * n + i] : cur[l * ld + i + (i >> 4)];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < PER; ++b) {
+    const int g = t + b * 256, l = g / nb, j = g - l * nb;
+    const int k = j % Ns;
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const float2 w = tws[(r - 1) * Ns + k];
+        const float wy = inverse ? -w.y : w.y;
+        const float2 x = v[b][r];
+        v[b][r] = make_float2(x.x * w.x - x.y * wy, x.x * wy + x.y * w.x);
+      }
+    }
+    if (inverse)
+      DFT<R, true>::run(v[b]);
+    else
+      DFT<R, false>::run(v[b]);
+    const int o = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int pos = o + r * Ns;
+      if (last)
+        cur[l * n + pos] = make_float2(v[b][r].x * scale, v[b][r].y * scale);
+      else
+        cur[l * ld + pos + (pos >> 4)] = v[b][r];
+    }
+  }
+  __syncthreads();
+}
+
 template <bool FP16>
 __global__ void __launch_bounds__(256, 2) tc_fft_kernel(const __grid_constant__ TcArgs a) {
   // Declared 16-byte aligned on purpose: with separately compiled device code
@@ -328,6 +380,17 @@ __global__ void __launch_bounds__(256, 2) tc_fft_kernel(const __grid_constant__ 
       const int Ns = a.sl.st[s].Ns;
       const float2* tws = a.tw + a.sl.st[s].twoff;
       const bool last = s == a.sl.nst - 1;
+      if (a.sl.st[s].R != 16) {  // the one radix-2/4/8 stage of a 2^k plan, on the CUDA cores
+        const int R = a.sl.st[s].R;
+        const bool inv = a.inverse != 0;
+        if (R == 8)
+          tc_simt_stage<8>(cur, n, ld, Ns, tws, s == 0, last, inv, a.scale, t);
+        else if (R == 4)
+          tc_simt_stage<4>(cur, n, ld, Ns, tws, s == 0, last, inv, a.scale, t);
+        else
+          tc_simt_stage<2>(cur, n, ld, Ns, tws, s == 0, last, inv, a.scale, t);
+        continue;
+      }
       const int k = j % Ns;
       float v[32];
       float sc = 1.0f;
@@ -430,8 +493,9 @@ cudaError_t launch_tc_selftest(const float* A, const float* B, float* D, unsigne
   return cudaGetLastError();
 }
 
-// Tile geometry for n = 16^s <= 4096: L = 4096 / n lanes (256 butterflies per
-// stage), slots of L x max(ld, n) complex64 (ld = n + n/16 + 1, odd).
+// Tile geometry for n = 2^k, 16 <= n <= 4096: L = 4096 / n lanes (256
+// radix-16 butterflies per stage), slots of L x max(ld, n) complex64
+// (ld = n + n/16 + 1, odd).
 static void tc_geometry(int n, int& L, int& ld, int& slot) {
   L = 4096 / n;
   ld = n + (n - 1) / 16 + 1;

@@ -45,7 +45,10 @@ typedef enum {
 /* Precision profiles (precision.rs:55-85): F64 = HIGH_ACCURACY_F64 (the
  * `high_accuracy` plan), F32 = LOW_PRECISION_F32 (`low_precision`).  The two
  * tensor-core forms compute radix-16 stages as split-precision DFT-matrix
- * products with FP32 accumulation on complex64 data. */
+ * products with FP32 accumulation on complex64 data; they plan rank-1 C2C
+ * lengths n = 2^k, 16 <= n <= 4096 (the one radix-2/4/8 stage of lengths that
+ * are not 16^s runs in FP32 on the CUDA cores) and return AFC_ERR_UNSUPPORTED
+ * for anything else. */
 typedef enum {
   AFC_PREC_F32 = 0,
   AFC_PREC_F64 = 1,

@@ -2,8 +2,10 @@
 
 * one tensor-core tile D = A B^T with hi/lo operands against numpy (checks the
   UMMA descriptors and the TMEM read-back);
-* 16^s-point transforms against the exact DFT, per row: FP16 split <= 1e-5
-  relative L2 (the accuracy bar of the split forms), BF16 split measured and bounded;
+* 2^k-point transforms (16 <= n <= 4096: radix-16 stages on the tensor cores,
+  the one radix-2/4/8 stage of lengths that are not 16^s on the CUDA cores)
+  against the exact DFT, per row: FP16 split <= 1e-5 relative L2 (the accuracy
+  bar of the split forms), BF16 split measured and bounded;
 * high-dynamic-range rows (scaled by 10^k, k in [-6, 6]) keep the FP16 bar
   thanks to the per-butterfly power-of-two scaling.
 """
@@ -33,7 +35,7 @@ def row_errors(y, ref):
     return np.linalg.norm(y - ref, axis=-1) / np.linalg.norm(ref, axis=-1)
 
 
-@pytest.mark.parametrize("n", [16, 256, 4096])
+@pytest.mark.parametrize("n", [16, 32, 64, 128, 256, 512, 1024, 2048, 4096])
 @pytest.mark.parametrize("prec,tol", [("tc_fp16", 1e-5), ("tc_bf16", 1e-4)])
 def test_tc_fft_rows(afc, cuda, n, prec, tol):
     rng = np.random.default_rng(n)
@@ -58,5 +60,8 @@ def test_tc_fp16_high_dynamic_range_rows(afc, cuda):
 
 
 def test_tc_plan_rejects_other_shapes(afc, cuda):
+    for n in (1000, 8, 8192):
+        with pytest.raises(afc.AfcError):
+            afc.CudaPlan([n], precision="tc_fp16")
     with pytest.raises(afc.AfcError):
-        afc.CudaPlan([1000], precision="tc_fp16")
+        afc.CudaPlan([16, 16], precision="tc_bf16")
