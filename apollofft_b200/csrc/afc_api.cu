@@ -1728,11 +1728,19 @@ static void tune_group(BatchGroup& g, bool dbl, void* scratch, cudaStream_t st) 
     while (L > 1 && (size_t)L * per_lane > batch_smem_cap(dbl)) --L;
     d.L = L;
     d.stage_out = ap.lp.sl.nst <= 1;
-    if (launch_lanes(d, dbl, false, st) != cudaSuccess) continue;
+    // a shape the device refuses is skipped; its error is consumed here so it
+    // is not reported by a later launch
+    if (launch_lanes(d, dbl, false, st) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
     cudaEventRecord(e0, st);
     for (int r = 0; r < 3; ++r) launch_lanes(d, dbl, false, st);
     cudaEventRecord(e1, st);
-    if (cudaEventSynchronize(e1) != cudaSuccess) continue;
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     // cost per lane on the persistent kernel: a tile of L lanes occupies one CTA
@@ -2973,8 +2981,12 @@ afc_status afc_batch_plan_create(afc_batch_plan* out, const int64_t* lengths, in
   // autotune the smem-resident lengths on a scratch buffer
   if (s == AFC_OK && env_int("AFC_AUTOTUNE", 1)) {
     void* scratch = nullptr;
-    const size_t sb = (size_t)std::max<int64_t>(max_smem_len, 1) * 4 * csz + (size_t)1 << 20;
-    if (dev_alloc(&scratch, sb) == cudaSuccess) {
+    // four times the largest shared-memory group (the tuner runs up to 4x its
+    // lanes, at most 64) plus 1 MiB
+    const size_t sb = (size_t)std::max<int64_t>(max_smem_len, 1) * 4 * csz + ((size_t)1 << 20);
+    if (dev_alloc(&scratch, sb) != cudaSuccess) {
+      cudaGetLastError();  // no scratch: the lengths keep their default shapes
+    } else {
       cudaMemsetAsync(scratch, 0, sb, st);
       for (auto& grp : bp->groups) tune_group(*grp, bp->dbl, scratch, st);
       cudaStreamSynchronize(st);
@@ -3038,25 +3050,47 @@ afc_status afc_batch_execute(afc_batch_plan plan, const void* in, void* out, afc
     AFC_CUDA(plan->fence.after(st, cap), "batch ordering");
     return AFC_OK;
   }
-  // mode 0: the persistent phases as one CUDA graph, captured once per (in, out, direction)
+  // mode 0: the persistent phases as one CUDA graph, captured once per (in,
+  // out, direction).  A call without a matching graph runs the phases
+  // directly (so every kernel of the plan has run outside a capture before it
+  // is captured, and the driver has sized its local memory), then captures the
+  // graph for the next call.  A capture the driver refuses leaves the plan
+  // without a graph: the next call runs the phases directly and tries again.
+  // Inside a caller's own capture the phases are recorded into it directly.
+  if (cap) {
+    cudaError_t e = run_batch_persistent(*plan, in, out, inv, st);
+    if (e != cudaSuccess) return cuda_fail(e, "batch execute");
+    AFC_CUDA(plan->fence.after(st, cap), "batch ordering");
+    return AFC_OK;
+  }
   if (!plan->gexec || plan->g_in != in || plan->g_out != out || plan->g_dir != (int)direction) {
     if (plan->gexec) { cudaGraphExecDestroy(plan->gexec); plan->gexec = nullptr; }
+    cudaError_t e = run_batch_persistent(*plan, in, out, inv, st);
+    if (e != cudaSuccess) return cuda_fail(e, "batch execute");
+    AFC_CUDA(plan->fence.after(st, cap), "batch ordering");
     cudaStream_t cs;
-    AFC_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
-    cudaGraph_t graph = nullptr;
-    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-      cudaError_t e2 = run_batch_persistent(*plan, in, out, inv, cs);
-      e = cudaStreamEndCapture(cs, &graph);
-      if (e2 != cudaSuccess) e = e2;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess) {
+      cudaGraph_t graph = nullptr;
+      e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        const cudaError_t e2 = run_batch_persistent(*plan, in, out, inv, cs);
+        e = cudaStreamEndCapture(cs, &graph);
+        if (e2 != cudaSuccess) e = e2;
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&plan->gexec, graph, 0);
+      if (graph) cudaGraphDestroy(graph);
+      cudaStreamDestroy(cs);
+      if (e == cudaSuccess) {
+        plan->g_in = in;
+        plan->g_out = out;
+        plan->g_dir = (int)direction;
+      } else {
+        if (plan->gexec) cudaGraphExecDestroy(plan->gexec);
+        plan->gexec = nullptr;
+      }
     }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&plan->gexec, graph, 0);
-    if (graph) cudaGraphDestroy(graph);
-    cudaStreamDestroy(cs);
-    if (e != cudaSuccess) return cuda_fail(e, "batch graph capture");
-    plan->g_in = in;
-    plan->g_out = out;
-    plan->g_dir = (int)direction;
+    cudaGetLastError();  // a refused capture is not an error of this call
+    return AFC_OK;
   }
   AFC_CUDA(cudaGraphLaunch(plan->gexec, st), "batch graph launch");
   AFC_CUDA(plan->fence.after(st, cap), "batch ordering");

@@ -87,6 +87,16 @@ __device__ __forceinline__ void cluster_sync_all() {
   asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may start while the previous kernel in the stream is still
+// finishing; griddep_wait blocks until that kernel has completed and its
+// memory operations are visible (a no-op without a programmatic
+// predecessor), griddep_launch_dependents lets the next such kernel start once
+// every CTA of this one has issued it or exited.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
 
 // Distributed shared memory: the address, in the cluster's shared window, of
 // the shared-memory location `saddr` (a shared::cta address) of CTA `rank`.

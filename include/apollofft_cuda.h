@@ -177,9 +177,12 @@ typedef struct afc_batch_plan_s* afc_batch_plan;
 AFC_API afc_status afc_batch_plan_create(afc_batch_plan* out, const int64_t* lengths, int64_t count,
                                  afc_precision precision, int device);
 AFC_API afc_status afc_batch_plan_destroy(afc_batch_plan plan);
-/* mode 0: one persistent launch per phase (captured into a CUDA graph on the
- * first call per buffer pair and direction), mode 1: one plain launch per
- * distinct length, mode 2: the persistent phases without the graph.  Calls on
+/* mode 0: one persistent launch per phase; the first call per buffer pair and
+ * direction runs the phases directly and captures them into a CUDA graph that
+ * later calls replay (a capture the driver refuses only means the next call
+ * runs directly again; inside a caller's own capture the phases are recorded
+ * into it), mode 1: one plain launch per distinct length, mode 2: the
+ * persistent phases without the graph.  Calls on
  * one batch plan from several streams are ordered on the GPU (its workspace is
  * shared), so they are safe but do not overlap. */
 AFC_API afc_status afc_batch_execute(afc_batch_plan plan, const void* in, void* out, afc_direction direction,
