@@ -60,3 +60,20 @@ def test_batch_modes_agree_on_repeats(afc, cuda):
         assert rel_l2(o, outs[0]) < 1e-6
     for got, src in zip(lanes_of(outs[0], lens), lanes_of(x, lens)):
         assert rel_l2(got, np.fft.fft(src.astype(np.complex128))) < 1e-5
+
+
+def test_plan_creation_leaves_no_stale_error(afc, cuda):
+    """A batch plan whose shared-memory group is large (here 8 lanes of 16384
+    points) is tuned on a scratch buffer sized from that group; the plan's
+    first launch, straight after creation, must succeed (a failed optional
+    allocation during creation once surfaced as an out-of-memory error of the
+    next launch)."""
+    lens = np.array([16384] * 8 + [4096, 97, 1031], dtype=np.int64)
+    rng = np.random.default_rng(21)
+    x = (rng.standard_normal(lens.sum()) + 1j * rng.standard_normal(lens.sum())).astype(np.complex64)
+    xt = torch.from_numpy(x).cuda()
+    bp = afc.BatchPlan(lens, precision="f32")
+    for mode in (2, 0, 0):
+        y = bp.execute(xt, mode=mode).cpu().numpy()
+        for got, src in zip(lanes_of(y, lens), lanes_of(x, lens)):
+            assert rel_l2(got, np.fft.fft(src.astype(np.complex128))) < 1e-5
