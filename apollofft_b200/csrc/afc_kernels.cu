@@ -809,7 +809,10 @@ int kernel_ctas_per_sm(const void* kern, int threads, size_t smem) {
     if (it != g_kper.end()) return it->second;
   }
   int per = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem) != cudaSuccess || per < 1) per = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem) != cudaSuccess || per < 1) {
+    cudaGetLastError();  // an estimate only: a refused query must not surface at the next launch
+    per = 1;
+  }
   std::lock_guard<std::mutex> lk(g_kfact_mu);
   g_kper[key] = per;
   return per;
@@ -916,12 +919,17 @@ cudaError_t launch_batch(const void* descs, const BatchItem* items, int nitems, 
 int batch_blocks_per_sm(size_t smem, bool dbl, bool inv) {
   (void)inv;
   int per = 1;
+  cudaError_t e;
   if (dbl) {
-    prep_smem(batch_kernel<double>, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<double>, kBatchThreads, smem);
+    e = prep_smem(batch_kernel<double>, smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<double>, kBatchThreads, smem);
   } else {
-    prep_smem(batch_kernel<float>, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<float>, kBatchThreads, smem);
+    e = prep_smem(batch_kernel<float>, smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<float>, kBatchThreads, smem);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // an estimate only; the launch itself reports a real failure
+    per = 1;
   }
   return per < 1 ? 1 : per;
 }

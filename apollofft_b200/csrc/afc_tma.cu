@@ -227,12 +227,20 @@ __device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long t
 }
 
 // Threads per CTA and CTAs per SM each kernel build is compiled for.
-template <class T, int V> struct TmaBuild {
-  static constexpr int threads = (V == 2 || (V == 5 && sizeof(T) == 8)) ? 128 : 256;
+struct FixNone {
+  static constexpr int BUILD_THREADS = 0;
+};
+// FX::BUILD_THREADS > 0: a compile-time stage list built for that many threads
+// at one CTA per SM (wider strided tiles)
+template <class T, int V, class FX = FixNone> struct TmaBuild {
+  static constexpr int threads = FX::BUILD_THREADS ? FX::BUILD_THREADS
+                                 : (V == 2 || (V == 5 && sizeof(T) == 8)) ? 128
+                                                                           : 256;
   // complex64 4096-point build: three CTAs per SM (80 registers; measured on
   // B200 16384 x 4096 forward 255 -> 242 us against two); the complex64
   // 256-point build gained nothing from a third CTA (256^3: 151 -> 154 us)
-  static constexpr int ctas = threads == 128 || (V == 6 && sizeof(T) == 4)
+  static constexpr int ctas = FX::BUILD_THREADS ? 1
+                              : threads == 128 || (V == 6 && sizeof(T) == 4)
                                   ? 3
                                   : (V == 3 || V == 7 || ((V == 1 || V == 4 || V == 5 || V == 8) && sizeof(T) == 4))
                                         ? 2
@@ -343,8 +351,8 @@ __device__ __forceinline__ void stages4096(const TmaArgs<T>& a, typename CT<T>::
 // Intermediate stages ping-pong between the slot and the work buffer in the
 // lane layout (element i of lane l at N l + i); contiguous tiles hold the
 // same layout, strided tiles hold element i of lane l at LK i + l.
-struct FixNone {};
 template <int N_, int R0_, int R1_, int R2_, int P_, int LK_> struct Fix {
+  static constexpr int BUILD_THREADS = 0;
   static constexpr int N = N_, P = P_, LK = LK_;
   static constexpr int NST = R2_ ? 3 : 2;
   static constexpr int R(int s) { return s == 0 ? R0_ : s == 1 ? R1_ : R2_; }
@@ -420,6 +428,7 @@ __host__ __device__ constexpr int fixip_ld(int n, int lk, int csz) {
 }
 
 template <int N_, int R0_, int R1_, int R2_, int R3_, int P_, int LK_> struct FixIP {
+  static constexpr int BUILD_THREADS = LK_ * P_ > 256 ? LK_ * P_ : 0;
   static constexpr int N = N_, P = P_, LK = LK_;
   static constexpr int NST = R3_ ? 4 : R2_ ? 3 : 2;
   static constexpr int R(int s) { return s == 0 ? R0_ : s == 1 ? R1_ : s == 2 ? R2_ : R3_; }
@@ -676,7 +685,7 @@ __device__ __forceinline__ typename CT<T>::type* tma_stages(const TmaArgs<T>& a,
 // n = 256 as radix 16 x 16 in place (stages256), 16 threads per lane, built
 // like variant 2 for complex128 and like variant 1 for complex64.
 template <class T, bool INV, int V, bool IP, class FX = FixNone>
-__global__ void __launch_bounds__(TmaBuild<T, V>::threads, TmaBuild<T, V>::ctas)
+__global__ void __launch_bounds__(TmaBuild<T, V, FX>::threads, TmaBuild<T, V, FX>::ctas)
     tma_kernel(const __grid_constant__ TmaArgs<T> a) {
   using C = typename CT<T>::type;
   extern __shared__ __align__(128) unsigned char smraw[];
@@ -1070,7 +1079,8 @@ static const FixedEntry kFixed[] = {
 // The in-place power-of-two stage lists built (variant 8): 2048 points in
 // complex64 (the 2048 x 2048 images), contiguous (complex or real lanes) and
 // strided tiles of 2 lanes.
-#define AFC_FIXED_IP_LIST(X) X(false, 2048, 16, 16, 8, 0, 128, 0) X(false, 2048, 16, 16, 8, 0, 128, 2)
+#define AFC_FIXED_IP_LIST(X)                                                                            \
+  X(false, 2048, 16, 16, 8, 0, 128, 0) X(false, 2048, 16, 16, 8, 0, 128, 4) X(false, 2048, 16, 16, 8, 0, 128, 2)
 static const FixedEntry kFixedIP[] = {
 #define AFC_FXI_ENTRY(D, N, R0, R1, R2, R3, P, LK) {D, N, R0, R1, R2, R3, P, LK},
     AFC_FIXED_IP_LIST(AFC_FXI_ENTRY)
@@ -1208,8 +1218,20 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
       if (e.dbl != dbl || e.n != n || sl.nst != nst || sl.st[0].R != e.r0 || sl.st[1].R != e.r1 ||
           (nst >= 3 && sl.st[2].R != e.r2) || (nst >= 4 && sl.st[3].R != e.r3) || P != e.P)
         continue;
-      if (e.LK == 0 ? tp.mode != 0 : (tp.mode != 1 || tp.L != e.LK || real)) continue;
-      if (ld != ((e.n + (e.n - 1) / 16 + 1) | 1) || tp.L * P > 256) continue;
+      // strided tiles of 4 lanes at 512 threads (one CTA per SM, two 70 KB
+      // slots) in place of the planner's 2 lanes at two CTAs per SM: half as
+      // many 16-byte TMA rows per point.  Measured on B200, 8 x 2048^2 R2C
+      // forward 0.31 -> 0.285 ms, forward + backward 1.59 -> 1.47 ms.
+      // AFC_TMA_L4=0 keeps 2 lanes.
+      const char* l4_env = getenv("AFC_TMA_L4");
+      const bool l4_on = !(l4_env && *l4_env && atoi(l4_env) == 0);
+      const bool widen = e.LK == 4 && l4_on && tp.mode == 1 && tp.L == 2 && !real;
+      if (!widen && (e.LK == 0 ? tp.mode != 0 : (tp.mode != 1 || tp.L != e.LK || real))) continue;
+      if (ld != ((e.n + (e.n - 1) / 16 + 1) | 1) || (!widen && tp.L * P > 256)) continue;
+      if (widen) {
+        tp.L = 4;
+        tp.kb = (im.es + tp.L - 1) / tp.L;
+      }
       tp.variant = 8;
       tp.fix = i;
       break;

@@ -36,6 +36,7 @@ def run(afc, cuda, monkeypatch, mode, shape, prec, x, inverse=False, batch=1):
     monkeypatch.setenv("AFC_TMA_N256", str(mode))
     monkeypatch.setenv("AFC_TMA_N4096", str(mode))
     monkeypatch.setenv("AFC_TMA_FIXED", "1" if mode else "0")
+    monkeypatch.setenv("AFC_TMA_L4", "1" if mode else "0")
     p = afc.CudaPlan(list(shape), precision=prec, batch=batch)
     return p.execute(torch.from_numpy(x).to(cuda, DT[prec]), inverse=inverse).cpu().numpy()
 
@@ -103,6 +104,7 @@ def test_fixed_real_lanes_2048(afc, cuda, monkeypatch, kind, shape, batch):
     outs = {}
     for mode in ("0", "1"):
         monkeypatch.setenv("AFC_TMA_FIXED", mode)
+        monkeypatch.setenv("AFC_TMA_L4", mode)
         p = afc.CudaPlan(list(shape), precision="f32", kind=kind, batch=batch)
         y = p.execute(torch.from_numpy(x).to(cuda))
         back = p.execute(y, inverse=True)
