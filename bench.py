@@ -349,6 +349,9 @@ def main():
     ap.add_argument("--reps", type=int, default=1, help="--profile-case: repetitions")
     ap.add_argument("--rows", type=int, default=8192, help="--profile-case c4: rows of 4096")
     ap.add_argument("--mode", type=int, default=2, help="--profile-case c3: batch mode")
+    ap.add_argument("--c3-class", default="all",
+                    choices=["all", "pow2", "smooth", "primes_lt1024", "primes_1024_8191", "primes_ge8192"],
+                    help="--profile-case c3: one length class of the batch")
     ap.add_argument("--batch", type=int, default=2, help="--profile-case c5: images of 2048^2")
     ap.add_argument("--quick", action="store_true", help="headline only: no other configurations, e2e or CPU legs")
     ap.add_argument("--workload", default="c2",
@@ -533,7 +536,8 @@ def profile_case(a):
 
     c1  64 x 4096 complex128 forward + inverse
     c2  3D C2C forward + inverse of --shape (default 128,256,256) at --precision f64|f32
-    c3  the 4096-length uneven complex64 batch, --mode 0 (graph) | 1 (per length) | 2 (persistent)
+    c3  the 4096-length uneven complex64 batch, --mode 0 (graph) | 1 (per length) | 2 (persistent),
+        --c3-class one length class of it
     c4  --rows x 4096 complex64 forward at --precision f32 | tc_bf16 | tc_fp16
     c5  --batch x 2048 x 2048 real f32 R2C (full spectrum) forward + adjoint
     """
@@ -561,6 +565,16 @@ def profile_case(a):
             p.execute(y, out=x, inverse=True)
     elif a.profile_case == "c3":
         lens = W.c3_lengths()
+        if a.c3_class != "all":
+            def prime(v):
+                v = int(v)
+                return v > 1 and all(v % d for d in range(2, int(v ** 0.5) + 1))
+            keep = {"pow2": lambda v: v & (v - 1) == 0,
+                    "smooth": lambda v: v & (v - 1) != 0 and not prime(v),
+                    "primes_lt1024": lambda v: prime(v) and v < 1024,
+                    "primes_1024_8191": lambda v: prime(v) and 1024 <= v < 8192,
+                    "primes_ge8192": lambda v: prime(v) and v >= 8192}[a.c3_class]
+            lens = np.asarray([v for v in lens if keep(int(v))], dtype=np.int64)
         x = torch.from_numpy(W.c3_values(lens)).cuda()
         bp = afc.BatchPlan(lens, precision="f32")
         y = torch.empty_like(x)
