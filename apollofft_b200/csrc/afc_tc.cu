@@ -318,7 +318,10 @@ __device__ __forceinline__ void tc_simt_stage(float2* cur, int n, int ld, int Ns
 // SMALL: the plan has one radix-2/4/8 stage (lengths that are not 16^s); the
 // 16^s build carries no code for it (with it, 16384 x 4096 measured 506 -> 628
 // us in BF16 on B200).
-template <bool FP16, bool SMALL>
+// FIXN = 4096: n = 4096 as three radix-16 stages with every shared-memory
+// index a compile-time offset from one per-thread base (one lane per tile,
+// thread t owns butterfly t of each stage), as in the SIMT 4096-point build.
+template <bool FP16, bool SMALL, int FIXN>
 __global__ void __launch_bounds__(256, 2) tc_fft_kernel(const __grid_constant__ TcArgs a) {
   // Declared 16-byte aligned on purpose: with separately compiled device code
   // the dynamic block starts at any 16-byte boundary after the static
@@ -379,10 +382,11 @@ __global__ void __launch_bounds__(256, 2) tc_fft_kernel(const __grid_constant__ 
       break;
     }
     float2* cur = slots[cb];
-    for (int s = 0; s < a.sl.nst; ++s) {
-      const int Ns = a.sl.st[s].Ns;
+#pragma unroll
+    for (int s = 0; s < (FIXN ? 3 : a.sl.nst); ++s) {
+      const int Ns = FIXN ? (s == 0 ? 1 : s == 1 ? 16 : 256) : a.sl.st[s].Ns;
       const float2* tws = a.tw + a.sl.st[s].twoff;
-      const bool last = s == a.sl.nst - 1;
+      const bool last = FIXN ? s == 2 : s == a.sl.nst - 1;
       if constexpr (SMALL) {
         if (a.sl.st[s].R != 16) {  // the one radix-2/4/8 stage of a 2^k plan, on the CUDA cores
           const int R = a.sl.st[s].R;
@@ -402,7 +406,11 @@ __global__ void __launch_bounds__(256, 2) tc_fft_kernel(const __grid_constant__ 
 #pragma unroll
       for (int r = 0; r < 16; ++r) {
         const int i = j + r * nb;
-        float2 x = s == 0 ? cur[l * n + i] : cur[l * ld + i + (i >> 4)];
+        float2 x;
+        if constexpr (FIXN == 4096)  // element t + 256 r: linear, or padded at t + t / 16 + 272 r
+          x = s == 0 ? cur[t + 256 * r] : cur[t + (t >> 4) + 272 * r];
+        else
+          x = s == 0 ? cur[l * n + i] : cur[l * ld + i + (i >> 4)];
         if (Ns > 1 && r > 0) {
           const float2 w = tws[(long long)(r - 1) * Ns + k];
           const float wy = a.inverse ? -w.y : w.y;
@@ -457,7 +465,19 @@ __global__ void __launch_bounds__(256, 2) tc_fft_kernel(const __grid_constant__ 
       for (int r = 0; r < 16; ++r) {
         const int pos = ob + r * Ns;
         float2 y = make_float2(o[r] * inv_sc, o[16 + r] * inv_sc);
-        if (last) {
+        if constexpr (FIXN == 4096) {
+          // outputs 16 t + r (s = 0), 256 (t / 16) + t % 16 + 16 r (s = 1),
+          // t + 256 r linear (s = 2)
+          if (s == 2) {
+            y.x *= a.scale;
+            y.y *= a.scale;
+            cur[t + 256 * r] = y;
+          } else if (s == 1) {
+            cur[272 * (t >> 4) + (t & 15) + 17 * r] = y;
+          } else {
+            cur[17 * t + r] = y;
+          }
+        } else if (last) {
           y.x *= a.scale;
           y.y *= a.scale;
           cur[l * n + pos] = y;
@@ -545,8 +565,16 @@ cudaError_t launch_tc_fft(const TcLaunch& d, bool fp16, cudaStream_t st) {
   cudaFuncAttributes fa;
   bool small = false;
   for (int s2 = 0; s2 < d.sl.nst; ++s2) small = small || d.sl.st[s2].R != 16;
-  void (*k)(TcArgs) = fp16 ? (small ? tc_fft_kernel<true, true> : tc_fft_kernel<true, false>)
-                           : (small ? tc_fft_kernel<false, true> : tc_fft_kernel<false, false>);
+  // n = 4096 on the compile-time build (AFC_TC_FIX=0 keeps the general one)
+  static const int fix_env = [] {
+    const char* e = getenv("AFC_TC_FIX");
+    return e && *e ? atoi(e) : 1;
+  }();
+  const bool fix = fix_env && !small && d.sl.n == 4096 && d.sl.nst == 3;
+  void (*k)(TcArgs) = fp16 ? (fix ? tc_fft_kernel<true, false, 4096>
+                                  : small ? tc_fft_kernel<true, true, 0> : tc_fft_kernel<true, false, 0>)
+                           : (fix ? tc_fft_kernel<false, false, 4096>
+                                  : small ? tc_fft_kernel<false, true, 0> : tc_fft_kernel<false, false, 0>);
   e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k);
   if (e != cudaSuccess) return e;
