@@ -15,6 +15,11 @@ __device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count)
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
 }
+// Raises the barrier's expected transaction count without arriving (the
+// phase still needs its arrival, made later by mbar_expect_tx).
+__device__ __forceinline__ void mbar_expect_tx_only(unsigned long long* b, unsigned bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
   unsigned ok;
   asm volatile(

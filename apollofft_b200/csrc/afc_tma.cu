@@ -714,16 +714,21 @@ __global__ void __launch_bounds__(TmaBuild<T, V, FX>::threads, TmaBuild<T, V, FX
   if (tid == 0) {
     for (int k = 0; k < ns; ++k) mbar_init(&bars[k], 1);
     fence_proxy_async();
+    // a CTA with a single tile never prefetches: the twiddle table is staged
+    // in the idle second slot on the tile's barrier (stage twiddles then come
+    // from shared memory instead of L1 misses to L2).  The table belongs to
+    // the plan, so its copy starts before the wait below.
+    if (a.tw_bytes) {
+      mbar_expect_tx_only(&bars[0], a.tw_bytes);
+      bulk_load(slots[1], a.tw, a.tw_bytes, &bars[0]);
+    }
     // launched with programmatic stream serialization, this CTA may start
     // while the previous pass is finishing: thread 0, the only thread that
     // touches the previous pass's output or this pass's output (the tile
     // copies), waits for it to complete here; the other threads read only the
     // plan's twiddle table
     griddep_wait();
-    // a CTA with a single tile never prefetches: the twiddle table is staged
-    // in the idle second slot with the tile (stage twiddles then come from
-    // shared memory instead of L1 misses to L2)
-    tma_issue_load(a, tile, slots[0], &bars[0], a.tw_bytes ? slots[1] : nullptr);
+    tma_issue_load(a, tile, slots[0], &bars[0]);
     for (int d = 1; d < ns - 1; ++d)
       if (tile + d * G < a.ntiles) tma_issue_load(a, tile + d * G, slots[d], &bars[d]);
   }
