@@ -455,6 +455,10 @@ struct AxisIO {
   long long nlen = 0;    // OUT_TRUNC bins kept
   long long herm_n = 0;  // full length for IN_HERM / OUT_TRUNC pairing
   double pair_w = 1.0;
+  // the input rows along the lanes' element stride are Hermitian (the pass
+  // after a full-spectrum R2C's real-input pass): a TMA pass may transform
+  // half the columns and store the rest as their conjugate mirrors
+  bool mirror = false;
 };
 
 // Lanes per CTA: about 256 threads, at least 8 (f64) / 16 (f32) adjacent lanes
@@ -634,7 +638,8 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
       if (!tl_rec && ((io.in_op == IN_C && io.out_op == OUT_C) || rin || rout) && tma_on) {
         TmaPlan tp;
         unsigned* err = device_err_word();
-        if (err && tma_plan(ap.lp.sl, ap.lp.ld, io.lanes, io.im, io.om, io.in, io.out, dbl, tma_lanes, tp, rin, rout))
+        if (err && tma_plan(ap.lp.sl, ap.lp.ld, io.lanes, io.im, io.om, io.in, io.out, dbl, tma_lanes, tp, rin, rout,
+                                io.mirror))
           return launch_tma(d, tp, err, dbl, inv, st);
       }
       if (!tl_rec && io.in_op == IN_C && plain_out(io.out_op)) {
@@ -1327,6 +1332,12 @@ static cudaError_t run_plan(const afc_plan_s& p, const void* in, void* out, bool
         io.in = first ? src : dst;
         io.out = dst;
         if (first) io.in_op = IN_R;
+        // the second pass's input rows (along the last axis) are the spectra
+        // of real rows; AFC_R2C_MIRROR=0 transforms every column
+        if (k == 1) {
+          const char* m_env = getenv("AFC_R2C_MIRROR");
+          io.mirror = !(m_env && *m_env && atoi(m_env) == 0);
+        }
       } else {
         void* cbuf = (r > 1) ? inter : nullptr;
         io.in = first ? src : cbuf;

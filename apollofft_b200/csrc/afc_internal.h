@@ -95,9 +95,15 @@ struct TmaPlan {
   int nslot = 2;
   // variant 7: index of the compile-time stage list (afc_tma.cu, kFixed)
   int fix = -1;
+  // strided lanes whose input rows are Hermitian (the pass after a real-input
+  // pass of a full-spectrum R2C): the tiles cover columns [0, kb L) only and
+  // column c in [1, hm_cmax] is also stored, conjugated and row-reversed, as
+  // column es - c
+  int hm_cmax = 0;
 };
 bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, const LaneMap& om, const void* in,
-              void* out, bool dbl, int lanes_pref, TmaPlan& tp, bool real_in = false, bool real_out = false);
+              void* out, bool dbl, int lanes_pref, TmaPlan& tp, bool real_in = false, bool real_out = false,
+              bool mirror = false);
 size_t tma_smem_bytes(const TmaPlan& tp, size_t csz);
 cudaError_t launch_tma(const LaunchDesc& d, const TmaPlan& tp, unsigned* err, bool dbl, bool inv, cudaStream_t st);
 

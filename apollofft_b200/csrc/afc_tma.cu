@@ -50,6 +50,9 @@ template <class T> struct TmaArgs {
                       // plane, the last one of a plane shorter); tpp = 0: tile q covers lanes [q L, q L + L)
   T scale;
   unsigned* err;
+  C* hm_out;          // hm_cmax > 0: output base and column count of the mirrored columns
+  long long hm_es;
+  int hm_cmax;
 };
 
 // First lane and lane count of contiguous-mode tile `tile`.
@@ -180,6 +183,31 @@ __device__ __forceinline__ void tma_stage_inplace(TView<C> src, TView<C> dst, in
         for (int r = 0; r < R; ++r) dst.at(l, o + r * Ns) = scale_out ? cscale(v[b][r], sc) : v[b][r];
       }
     }
+  }
+}
+
+// Hermitian columns.  The rows of a full-spectrum R2C after its real-input
+// pass satisfy X[m][es - c] = conj(X[m][c]), so the transform along the rows'
+// axis of column es - c is the conjugate of column c's read backwards:
+// Y[k][es - c] = conj(Y[(n - k) mod n][c]).  A tile of columns [c0, c0 + L)
+// whose transform sits in obuf ([row][lane]) also stores columns es - c for c
+// in [1, hm_cmax]; no tile of the pass reads those columns.
+template <class T>
+__device__ __forceinline__ void hermitian_mirror(const TmaArgs<T>& a, long long tile,
+                                                 const typename CT<T>::type* obuf, int tid) {
+  using C = typename CT<T>::type;
+  const int L = a.L, n = a.sl.n, nt = blockDim.x;  // strided tiles: nt = L P, a multiple of L
+  const int c = (int)(tile % a.kb) * L + tid % L;  // each thread keeps one lane
+  if (c < 1 || c > a.hm_cmax) return;
+  const long long es = a.hm_es, wrap = (long long)n * es, step = (long long)(nt / L) * es;
+  C* const col = a.hm_out + (tile / a.kb) * wrap + es - c;  // column es - c of row 0
+  int r = tid / L;
+  long long off = (long long)(n - r) * es;  // row (n - r) mod n
+  const C* src = obuf + tid;
+#pragma unroll 4
+  for (; r < n; r += nt / L, src += nt, off -= step) {
+    const C v = *src;
+    col[off == wrap ? 0 : off] = C{v.x, -v.y};
   }
 }
 
@@ -762,6 +790,10 @@ __global__ void __launch_bounds__(TmaBuild<T, V, FX>::threads, TmaBuild<T, V, FX
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) tma_issue_store(a, tile, obuf);
+    if (a.hm_cmax > 0) {
+      hermitian_mirror(a, tile, obuf, tid);
+      __syncthreads();  // the slot (or work buffer) is refilled next iteration
+    }
     tile += G;
     if (tile >= a.ntiles) break;
   }
@@ -1110,7 +1142,7 @@ static void plan_resident_twiddles(const StageList& sl, bool dbl, TmaPlan& tp, s
 
 // Decides whether an axis pass can run on the TMA kernel and with which tiles.
 bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, const LaneMap& om, const void* in,
-              void* out, bool dbl, int lanes_pref, TmaPlan& tp, bool real_in, bool real_out) {
+              void* out, bool dbl, int lanes_pref, TmaPlan& tp, bool real_in, bool real_out, bool mirror) {
   const size_t csz = dbl ? 16 : 8;
   const long long n = sl.n;
   const bool real = real_in || real_out;
@@ -1305,6 +1337,15 @@ bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, c
     if (slots_env >= 3 && (size_t)ctas * (b3 + 1024) <= 233472 && b3 <= 220 * 1024) tp.nslot = 3;
   }
   plan_resident_twiddles(sl, dbl, tp);
+  // Hermitian input rows: tiles over columns [0, kb L) with kb L > es / 2,
+  // columns [kb L, es) stored as mirrors of columns [1, es - kb L]
+  if (mirror && tp.mode == 1 && !real) {
+    const long long kbh = im.es / 2 / tp.L + 1;
+    if (kbh < tp.kb && im.es - kbh * tp.L > 0) {
+      tp.kb = kbh;
+      tp.hm_cmax = (int)(im.es - kbh * tp.L);
+    }
+  }
   tp.ntiles = tp.mode == 0 ? (lanes + tp.L - 1) / tp.L : (lanes / im.es) * tp.kb;
   tp.outer = tp.mode == 1 ? lanes / im.es : 0;
   return true;
@@ -1341,6 +1382,9 @@ template <class T> static bool fill_tma_args(const LaunchDesc& d, const TmaPlan&
   a.err = err;
   a.tw_res = tp.tw_res;
   a.nslot = tp.nslot;
+  a.hm_out = static_cast<C*>(d.out);
+  a.hm_es = d.om.es;
+  a.hm_cmax = tp.hm_cmax;
   return true;
 }
 
