@@ -459,6 +459,11 @@ struct AxisIO {
   // after a full-spectrum R2C's real-input pass): a TMA pass may transform
   // half the columns and store the rest as their conjugate mirrors
   bool mirror = false;
+  // set when the previous pass stored only the columns this pass reads: the
+  // mirrored TMA pass is then the only correct one
+  bool need_mirror = false;
+  // contiguous real-input lanes: elements stored per lane (0: all)
+  long long store_cols = 0;
 };
 
 // Lanes per CTA: about 256 threads, at least 8 (f64) / 16 (f32) adjacent lanes
@@ -615,6 +620,21 @@ static cudaError_t exec_fourstep(const AxisPlan& ap, bool dbl, bool inv, const A
   return do_lanes(b, dbl, inv, st);
 }
 
+// Columns [0, H) that the Hermitian (mirrored) TMA pass of `io` transforms,
+// or 0 when that pass would not take the mirrored TMA path; the same planner
+// call as exec_axis makes, so the pass then takes exactly that path.
+static long long mirror_cols(const AxisPlan& ap, bool dbl, const AxisIO& io) {
+  static const int tma_on = env_int("AFC_TMA", 1), tma_lanes = env_int("AFC_TMA_LANES", 0);
+  if (!io.mirror || ap.algo != ALGO_SMEM || tl_rec || !tma_on || io.lanes <= 0) return 0;
+  if (io.in_op != IN_C || io.out_op != OUT_C) return 0;
+  unsigned* err = device_err_word();
+  TmaPlan tp;
+  if (!err || !tma_plan(ap.lp.sl, ap.lp.ld, io.lanes, io.im, io.om, io.in, io.out, dbl, tma_lanes, tp, false, false,
+                        true))
+    return 0;
+  return tp.hm_cmax > 0 ? tp.kb * tp.L : 0;
+}
+
 static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisIO& io, void* ws, cudaStream_t st) {
   const size_t csz = dbl ? 16 : 8;
   if (io.lanes <= 0) return cudaSuccess;
@@ -639,9 +659,15 @@ static cudaError_t exec_axis(const AxisPlan& ap, bool dbl, bool inv, const AxisI
         TmaPlan tp;
         unsigned* err = device_err_word();
         if (err && tma_plan(ap.lp.sl, ap.lp.ld, io.lanes, io.im, io.om, io.in, io.out, dbl, tma_lanes, tp, rin, rout,
-                                io.mirror))
+                                io.mirror)) {
+          if (io.need_mirror && tp.hm_cmax <= 0) return cudaErrorInvalidValue;
+          if (io.store_cols > 0 && io.store_cols < ap.lp.sl.n && tp.mode == 0 && rin &&
+              (io.store_cols * (long long)csz) % 16 == 0)
+            tp.store_cols = (int)io.store_cols;
           return launch_tma(d, tp, err, dbl, inv, st);
+        }
       }
+      if (io.need_mirror) return cudaErrorInvalidValue;
       if (!tl_rec && io.in_op == IN_C && plain_out(io.out_op)) {
         const bool lm = io.im.es != 1;
         int L, P;
@@ -1426,7 +1452,19 @@ static cudaError_t run_plan(const afc_plan_s& p, const void* in, void* out, bool
       if (e != cudaSuccess) return e;
       continue;
     }
-    cudaError_t e = exec_axis(ap, p.dbl, inv, io, axis_ws, st);
+    // full-spectrum R2C forward: when the next pass transforms only the
+    // columns [0, H) and mirrors the rest, the real-row pass stores only
+    // those columns (AFC_R2C_TRUNC=0 stores whole rows)
+    AxisIO io0 = io;
+    if (k == 0 && order.size() > 1 && ios[1].mirror) {
+      const char* t_env = getenv("AFC_R2C_TRUNC");
+      const long long H = mirror_cols(*p.axes[order[1]], p.dbl, ios[1]);
+      if (H > 0) {
+        ios[1].need_mirror = true;
+        if (!(t_env && *t_env && atoi(t_env) == 0)) io0.store_cols = H;
+      }
+    }
+    cudaError_t e = exec_axis(ap, p.dbl, inv, io0, axis_ws, st);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

@@ -100,6 +100,9 @@ struct TmaPlan {
   // column c in [1, hm_cmax] is also stored, conjugated and row-reversed, as
   // column es - c
   int hm_cmax = 0;
+  // contiguous lanes: elements stored per lane (0: all n); the rest of each
+  // output lane is written by a later pass (the Hermitian column pass's mirrors)
+  int store_cols = 0;
 };
 bool tma_plan(const StageList& sl, int ld, long long lanes, const LaneMap& im, const LaneMap& om, const void* in,
               void* out, bool dbl, int lanes_pref, TmaPlan& tp, bool real_in = false, bool real_out = false,

@@ -53,6 +53,7 @@ template <class T> struct TmaArgs {
   C* hm_out;          // hm_cmax > 0: output base and column count of the mirrored columns
   long long hm_es;
   int hm_cmax;
+  int out_cols;       // contiguous mode, > 0: only the first out_cols elements of each lane are stored
 };
 
 // First lane and lane count of contiguous-mode tile `tile`.
@@ -243,7 +244,13 @@ __device__ __forceinline__ void tma_issue_store(const TmaArgs<T>& a, long long t
     int lanes_here;
     tile_lanes(a, tile, q0, lanes_here);
     const size_t es = a.real_out ? sizeof(T) : sizeof(C);
-    bulk_store(reinterpret_cast<char*>(a.out) + q0 * a.sl.n * es, buf, (unsigned)((long long)lanes_here * a.sl.n * es));
+    if (a.out_cols > 0) {  // one copy per lane: its first out_cols elements
+      for (int j = 0; j < lanes_here; ++j)
+        bulk_store(reinterpret_cast<char*>(a.out) + (q0 + j) * a.sl.n * es, buf + (long long)j * a.sl.n,
+                   (unsigned)(a.out_cols * es));
+    } else {
+      bulk_store(reinterpret_cast<char*>(a.out) + q0 * a.sl.n * es, buf, (unsigned)((long long)lanes_here * a.sl.n * es));
+    }
   } else {
     const int o = (int)(tile / a.kb), kb = (int)(tile % a.kb);
     for (int b = 0; b < a.nbx; ++b) {
@@ -1385,6 +1392,7 @@ template <class T> static bool fill_tma_args(const LaunchDesc& d, const TmaPlan&
   a.hm_out = static_cast<C*>(d.out);
   a.hm_es = d.om.es;
   a.hm_cmax = tp.hm_cmax;
+  a.out_cols = tp.store_cols;
   return true;
 }
 
