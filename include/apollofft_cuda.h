@@ -59,7 +59,9 @@ typedef enum {
 /* C2C: complex -> complex.
  * R2C_FULL: the reference's "R2C": real input widened to complex, full C2C,
  *   output of the same shape (plan/fft/real_storage.rs:186-303); its inverse is
- *   a full C2C inverse followed by taking the real part ("C2R").
+ *   a full C2C inverse followed by taking the real part ("C2R").  Rank >= 2
+ *   forward: the columns past n/2 of the last axis are stored as the exact
+ *   conjugates of their partners X[(-k) mod n0][n1 - c].
  * R2C_HALF: Hermitian half spectrum, last dim n -> n/2 + 1 (new explicit API;
  *   the reference models HalfSpectrum3D in domain/metadata/shape.rs:79-95 but
  *   never wires it). */
